@@ -1,0 +1,136 @@
+/* sdpv_b200 -- B200 (sm_100a) kernels for SDPviBe's multiprecision arithmetic hot path.
+ *
+ * C ABI of libsdpv_b200.so.  Plain pointers and sizes only: every array argument is a DEVICE pointer
+ * on the current CUDA device unless its name ends in `_host`; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  Every function returns an sdpv_status.  No function allocates device
+ * memory except sdpv_ctx_create (its tables, once per limb count and device).
+ *
+ * Number formats are the reference's:
+ *   limb planes   X[k*B + e]: k-th 32-bit limb (little endian, two's complement) of entry e
+ *                 (sdpvibe/limbops.py:3-5);
+ *   MPF           m (L, n) limb planes + e (n) int64, value = m 2^e, |m| has NB = 32L-2 bits,
+ *                 zero is m = 0, e = -2^40 (sdpvibe/mpf.py:1-10, 21);
+ *   residues      (G, rows, kp) int8 hi/lo planes, r = 128 hi + lo centred in (-m/2, m/2]
+ *                 (sdpvibe/rns.py:196-214);
+ *   accumulator   (n, rows, N) int16, canonical residues in [0, m) (sdpvibe/rns.py:106-137).
+ *
+ * The reference has no C ABI: its Python calls these operations as Triton kernels or CuPy/NVRTC
+ * kernels.  Each entry point below names the reference function it replaces (file:line); the
+ * Python host layer `sdpvibe_b200` keeps the reference's Python signatures on top of them.
+ */
+#ifndef SDPV_B200_H
+#define SDPV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SDPV_OK = 0,
+  SDPV_EOVERFLOW = 1, /* a rounding step overflowed its limb budget (limbops.py:165-185) */
+  SDPV_ENOTSPD = 2,   /* non-positive pivot in a Cholesky tile (mpf.py:475-476) */
+  SDPV_ETIMEOUT = 3,  /* a bounded device wait gave up (pipeline barrier never completed) */
+  SDPV_EINVAL = 4,    /* bad argument (shape, alignment, size beyond a documented limit) */
+  SDPV_ECUDA = 5,     /* a CUDA runtime call failed */
+  SDPV_ENOMEM = 6     /* table allocation failed */
+} sdpv_status;
+
+/* Device error word bits, read (and cleared) by sdpv_get_error. */
+#define SDPV_ERRBIT_OVERFLOW 1u
+#define SDPV_ERRBIT_TIMEOUT 2u
+#define SDPV_ERRBIT_NOTSPD 4u
+
+typedef struct sdpv_ctx sdpv_ctx;
+
+int sdpv_version(void);
+
+/* Last CUDA error text of this thread (for diagnostics after SDPV_ECUDA). */
+const char* sdpv_last_error(void);
+
+/* ---------------------------------------------------------------- RNS context
+ * Moduli: primes descending from 32639 above 2^14 until M > 4*kmax*2^(2(32L-1)) and n is a multiple
+ * of 16 (kmax = 2^17); CRT width E bytes = (ceil(bits(M)/8) + 2 + 7)//8*8, W = E/4 words.
+ * Replaces RNS.__init__ (sdpvibe/rns.py:166-191) and mpmat.ctx (sdpvibe/mpmat.py:163-166).
+ * Tables live on the device that is current at creation. */
+int sdpv_ctx_create(int L, sdpv_ctx** out);
+int sdpv_ctx_destroy(sdpv_ctx* ctx);
+/* n moduli, E CRT bytes, W = E/4 words. */
+int sdpv_ctx_query(const sdpv_ctx* ctx, int* n, int* E, int* W);
+/* Copy the n moduli to host memory. */
+int sdpv_ctx_moduli(const sdpv_ctx* ctx, int32_t* mods_host);
+
+/* ---------------------------------------------------------------- limb-plane bookkeeping */
+/* out = round_half_up(X / 2^s) (ties toward +infinity) as Lout limbs, s per entry (s <= 0: exact
+ * left shift).  flag != NULL: per-entry overflow flags (0/1); flag == NULL: overflow sets the
+ * device error word.  Replaces limbops.shift_round (sdpvibe/limbops.py:31-62, 173-185). */
+int sdpv_shift_round(const int32_t* X, int Lin, int64_t B, const int64_t* s, int Lout, int32_t* out, int32_t* flag,
+                     void* stream);
+/* out = A + sgn*B mod 2^(32L), sgn = +-1.  Replaces limbops.add_same (sdpvibe/limbops.py:65-81, 188-193). */
+int sdpv_add_same(const int32_t* A, const int32_t* Bm, int L, int64_t B, int sgn, int32_t* out, void* stream);
+/* out[e] = bit length of v (v >= 0) or of ~v (v < 0).  Replaces limbops.bitlen_words
+ * (sdpvibe/limbops.py:196-218). */
+int sdpv_bitlen(const int32_t* X, int L, int64_t B, int64_t* out, void* stream);
+/* Per entry of (nb, rows, cols): both operands rounded half up to exponent max(ea,eb)+1 of their
+ * (block, column), then A + sign*B (wrapping); EO (nb, cols) receives the exponents.
+ * Replaces batched.badd(out_exp="align") (sdpvibe/batched.py:55-92). */
+int sdpv_badd_align(const int32_t* A, const int32_t* Bm, const int64_t* EA, const int64_t* EB, int L, int64_t nb,
+                    int64_t rows, int64_t cols, int sign, int32_t* out, int64_t* EO, void* stream);
+
+/* ---------------------------------------------------------------- per-entry floating point (MPF) */
+/* O = A*B entrywise (B a single entry if bscalar), renormalised to NB bits, magnitude rounded half
+ * up.  Replaces mpf.mul / mpf_mul (sdpvibe/mpf.py:58-89, 316-323). */
+int sdpv_mpf_mul(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
+                 int bscalar, int32_t* O, int64_t* eO, void* stream);
+/* O = A + sgn*B entrywise.  Replaces mpf.add / mpf_add (sdpvibe/mpf.py:92-124, 326-331). */
+int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
+                 int sgn, int32_t* O, int64_t* eO, void* stream);
+/* Normalise LI-limb integers with exponents eI to MPF with L limbs (LI <= 160).
+ * Replaces mpf.normalize / mpf_norm (sdpvibe/mpf.py:127-140, 307-313). */
+int sdpv_mpf_norm(int L, int LI, int64_t n, const int32_t* X, const int64_t* eI, int32_t* O, int64_t* eO,
+                  void* stream);
+
+/* ---------------------------------------------------------------- residue decomposition (a)
+ * Residues of X[:, :, k0:k0+kc] for moduli g0..g0+G of ctx: X (L, rows, ld) int32 limb planes;
+ * Rhi, Rlo (G, rows, kp) int8, kp = kc rounded up to 16, zero residues for kc <= k < kp.
+ * Replaces RNS.residues / _residue_kernel (sdpvibe/rns.py:66-103, 196-214). */
+int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0,
+                  int G, int8_t* Rhi, int8_t* Rlo, void* stream);
+
+/* ---------------------------------------------------------------- residue GEMM (b) and Gram (d)
+ * For each of the G moduli g0..g0+G and each of nb blocks:
+ *   acc[g0+g][b*M + i][j] <- (acc + A_gb B_gb^T) mod m, A_gb = 128 Ahi + Alo (M x KC), B likewise (N x KC)
+ * with A* (G, nb*M, KC), B* (G, nb*N, KC) int8, acc (n, nb*M, N) int16.  mode 0: all entries;
+ * mode 1 (syrk): B = A (Bhi/Blo ignored, N = M) and only entries with i >= j are updated.
+ * KC must be a multiple of 16 and <= 65536.  Replaces RNS.accumulate / _gemm_kernel
+ * (sdpvibe/rns.py:106-137, 217-224), batched._bgemm_kernel (sdpvibe/batched.py:96-127) and
+ * batched._syrk_lower_kernel (sdpvibe/batched.py:130-162). */
+int sdpv_rns_gemm(const sdpv_ctx* ctx, const int8_t* Ahi, const int8_t* Alo, const int8_t* Bhi, const int8_t* Blo,
+                  int16_t* acc, int g0, int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream);
+
+/* ---------------------------------------------------------------- CRT reconstruction (c)
+ * Exact integers of the block "all rows x columns j0..j0+w" of acc (n, rows_total, N) (modulus
+ * stride ldg entries): words (W, rows*w) int32 two's complement (entry e = i*w + jj) and bit lengths
+ * (rows*w) of v / ~v.  Valid for |value| < M/4.  Replaces RNS.crt_block with crt_pre / crt dot /
+ * crt_carry (sdpvibe/rns.py:140-159, 227-245; sdpvibe/limbops.py:85-152, 221-239). */
+int sdpv_crt_block(const sdpv_ctx* ctx, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                   int64_t rows, int32_t* words, int64_t* bitlen, void* stream);
+
+/* CRT fused with renormalisation to MPF (mf_norm semantics): for the same block, entry (r, jj) with
+ * exponent rowexp[r] + colexp[(r / rows_per_block) * N + j0 + jj] is written to O (L, rows*w) /
+ * eO (rows*w).  Replaces the crt_block + normalize pairs of mpf.gemm (sdpvibe/mpf.py:440-450) and
+ * GramAcc._crt (sdpvibe/mpf.py:595-610). */
+int sdpv_crt_norm(const sdpv_ctx* ctx, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                  int64_t rows, int64_t rows_per_block, const int64_t* rowexp, const int64_t* colexp, int L,
+                  int32_t* O, int64_t* eO, void* stream);
+
+/* ---------------------------------------------------------------- errors
+ * Read and clear the device error word (bits SDPV_ERRBIT_*) after synchronising `stream`.
+ * Replaces limbops.check_errors (sdpvibe/limbops.py:156-169). */
+int sdpv_get_error(unsigned* flags_host, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

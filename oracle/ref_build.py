@@ -179,15 +179,27 @@ def _link(res, dst):
         os.replace(dst + ".tmp", dst)
 
 
-def load_prebuilt(kind, *key):
-    """Load a prebuilt checker library (works without the reference tree, e.g. on the GPU box)."""
-    path = prebuilt_path(kind, *key)
-    if not os.path.exists(path):
-        return None
-    code = open(path.replace(".so", ".sig")).read() if os.path.exists(path.replace(".so", ".sig")) else None
-    lib = ctypes.CDLL(path)
-    return lib
+
+
+# ------------------------------------------------------------------ the reference's CPU timing baseline
+MPF_BASELINE = os.path.join(REF_OUT, "mpf_baseline")
+
+
+def build_cpu_baseline():
+    """cpu_baseline/mpf_baseline.c (GMP mpf + OpenMP, the reference's CPU comparison) compiled where it
+    lies, as the reference documents: gcc -O2 -fopenmp mpf_baseline.c -l:libgmp.so.10 -lm."""
+    src = os.path.join(REFERENCE_ROOT, "cpu_baseline", "mpf_baseline.c")
+    if not os.path.exists(src):
+        return os.path.exists(MPF_BASELINE)
+    os.makedirs(REF_OUT, exist_ok=True)
+    if os.path.exists(MPF_BASELINE) and os.path.getmtime(MPF_BASELINE) >= os.path.getmtime(src):
+        return True
+    tmp = MPF_BASELINE + ".tmp"
+    subprocess.check_call(["gcc", "-O2", "-fopenmp", src, "-o", tmp, "-l:libgmp.so.10", "-lm"])
+    os.replace(tmp, MPF_BASELINE)
+    return True
 
 
 if __name__ == "__main__":
-    print("built" if build_prebuilt() else "reference tree absent; nothing built")
+    print("kernel checkers:", "built" if build_prebuilt() else "reference tree absent")
+    print("cpu baseline:", "built" if build_cpu_baseline() else "reference tree absent")

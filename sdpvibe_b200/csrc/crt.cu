@@ -1,0 +1,233 @@
+// CRT reconstruction fused with rounding (north-star item (c)).
+//
+// For an entry with residues a_i (n moduli m_i, M = prod m_i, |value| < M/4):
+//   y_i = a_i (M/m_i)^-1 mod m_i  (centred),  k = round(sum y_i / m_i),
+//   value = sum_i y_i (M/m_i) - k M = sum_t (Z_t - k Md_t) 256^t,  Z_t = sum_i Ct[t][i] y_i
+// with Ct[t][i] the signed base-256 digits of M/m_i (sdpvibe/rns.py:140-159, 227-245;
+// sdpvibe/limbops.py:85-152).  One CTA handles 128 entries:
+//   * pre-pass (one thread per entry): y_i from the int16 accumulator, split y = 128 yh + yl into
+//     two K-major int8 tiles in shared memory, and k;
+//   * digit contraction on the tensor cores, 64 digits at a time: Zh = Yh Ct^T, Zl = Yl Ct^T
+//     (tcgen05.mma kind::i8, M = 128 entries, N = 64 digits, K = moduli), Ct resident in shared memory;
+//   * epilogue (the same thread, TMEM lane = entry): z = 128 Zh + Zl - k Md, carried into 32-bit words;
+//     then either the words + bit length (crt_block) or the MPF renormalisation of mpf_norm
+//     (magnitude rounded half up to NB = 32L-2 bits) written straight to the output limb planes.
+// No intermediate leaves the SM; one launch replaces crt_pre + digit GEMM + crt_carry + normalize.
+#include "common.cuh"
+#include "mpcore.cuh"
+
+namespace {
+using namespace sdpv;
+
+constexpr int kThreads = 128;
+constexpr int kDig = 64;                    // digits per MMA chunk (N)
+constexpr u32 kSlice = 128 * 128;
+
+struct CrtSmemHead {
+  u64 bar_ct, bar_mma;
+  u32 tmem_slot;
+  int abort;
+};
+
+// Dynamic shared memory: [head (1 KB)] [Yh: ktc slices] [Yl: ktc slices] [Ct: Epad/128 * ktc slices]
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    crt_kernel(const int16_t* __restrict__ acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rows_per_block,
+               const int64_t* __restrict__ rowexp, const int64_t* __restrict__ colexp, int L, int n, int E, int W,
+               int ktc, int Epad, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
+               const int32_t* __restrict__ invs, const int32_t* __restrict__ md, const uint8_t* __restrict__ ct,
+               int32_t* __restrict__ out, int64_t* __restrict__ out2, unsigned* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  CrtSmemHead& H = *reinterpret_cast<CrtSmemHead*>(base);
+  uint8_t* Yh = base + 1024;
+  uint8_t* Yl = Yh + (size_t)ktc * kSlice;
+  uint8_t* Ct = Yl + (size_t)ktc * kSlice;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const i64 B = rows * w;
+  const i64 ntiles = (B + 127) / 128;
+
+  if (tid == 0) {
+    mbar_init(&H.bar_ct, 1);
+    mbar_init(&H.bar_mma, 1);
+    H.abort = 0;
+    mbar_fence_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(&H.tmem_slot, 2 * kDig);
+    tmem_relinquish();
+  }
+  __syncthreads();
+  tc_fence_after();
+  const u32 tmem = H.tmem_slot;
+  if (tid == 0) {
+    u32 bytes = (u32)(Epad / 128) * ktc * kSlice;
+    mbar_expect_tx(&H.bar_ct, bytes);
+    for (u32 off = 0; off < bytes; off += kSlice) bulk_load(Ct + off, ct + off, kSlice, &H.bar_ct);
+  }
+  if (!mbar_wait(&H.bar_ct, 0, err)) H.abort = 1;
+
+  const u32 idesc = idesc_i8(128, kDig);
+  const int ksteps = (n + 31) / 32;
+  const int nchunk = (E + kDig - 1) / kDig;
+  u32 phase = 0;
+  u32 words[160];
+
+  for (i64 tile = blockIdx.x; tile < ntiles && !H.abort; tile += gridDim.x) {
+    // ---- pre-pass: y_i, its int8 digits, k
+    const i64 e = tile * 128 + tid;
+    const bool valid = e < B;
+    const i64 r = valid ? e / w : 0, jj = valid ? e - (e / w) * w : 0;
+    const int16_t* ap = acc + r * N + j0 + jj;
+    float ks = 0.f;
+    for (int g16 = 0; g16 < ktc * 128; g16 += 16) {
+      u32 ph[4], pl[4];
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        int g = g16 + q, y = 0;
+        if (valid && g < n) {
+          int m = mods[g];
+          float mi = minvs[g];
+          y = mod_exact((int)ap[(i64)g * ldg] * invs[g], m, mi);
+          y -= (y > (m >> 1)) ? m : 0;
+          ks += (float)y * mi;
+        }
+        int yl = ((y + 64) & 127) - 64, yh = (y - yl) >> 7;
+        if ((q & 3) == 0) ph[q >> 2] = pl[q >> 2] = 0;
+        ph[q >> 2] |= (u32)(yh & 255) << (8 * (q & 3));
+        pl[q >> 2] |= (u32)(yl & 255) << (8 * (q & 3));
+      }
+      int kt = g16 >> 7, chunk = (g16 & 127) >> 4;
+      *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+      *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+    }
+    const i64 kq = (i64)__float2int_rd(ks + 0.5f);
+    fence_proxy_async_smem();
+    __syncthreads();
+
+    // ---- digit chunks: MMA, then carry into words
+    i64 carry = 0;
+    int nw = 0;
+    for (int ch = 0; ch < nchunk; ch++) {
+      if (tid == 0) {
+        tc_fence_after();
+        const u32 ctc = smem_u32(Ct) + (u32)((ch * kDig) / 128) * ktc * kSlice + (u32)((ch * kDig) % 128) * 128;
+        for (int s = 0; s < ksteps; s++) {
+          int kt = s >> 2, ko = (s & 3) * 32;
+          u64 bd = sdesc_sw128(ctc + kt * kSlice + ko);
+          mma_i8(tmem + 0, sdesc_sw128(smem_u32(Yh) + kt * kSlice + ko), bd, idesc, s ? 1u : 0u);
+          mma_i8(tmem + kDig, sdesc_sw128(smem_u32(Yl) + kt * kSlice + ko), bd, idesc, s ? 1u : 0u);
+        }
+        mma_commit(&H.bar_mma);
+      }
+      if (!mbar_wait(&H.bar_mma, phase, err)) H.abort = 1;
+      phase ^= 1;
+      tc_fence_after();
+#pragma unroll 1
+      for (int c32 = 0; c32 < kDig; c32 += 32) {
+        u32 zh[32], zl[32];
+        tmem_ld32(tmem + ((u32)(warp * 32) << 16) + c32, zh);
+        tmem_ld32(tmem + ((u32)(warp * 32) << 16) + kDig + c32, zl);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+          int t0 = ch * kDig + c32 + j;
+          if (t0 >= E) break;
+          i64 v = carry;
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            i64 z = 128 * (i64)(int)zh[j + u] + (i64)(int)zl[j + u] - kq * (i64)md[t0 + u];
+            v += z << (8 * u);
+          }
+          words[nw++] = (u32)v;
+          carry = v >> 32;
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+    }
+
+    // ---- outputs
+    if (valid) {
+      if (MODE == 0) {
+        for (int k = 0; k < W; k++) out[(i64)k * B + e] = (int32_t)words[k];
+        u32 ext = (words[W - 1] >> 31) ? 0xffffffffu : 0u;
+        i64 bl = 0;
+        for (int k = W - 1; k >= 0; k--) {
+          u32 x = words[k] ^ ext;
+          if (x) {
+            bl = 32 * (i64)k + 32 - __clz(x);
+            break;
+          }
+        }
+        out2[e] = bl;
+      } else {
+        bool ng = words[W - 1] >> 31;
+        if (ng) neg_words(words, W);
+        int bl = bitlen_mag(words, W);
+        if (!bl) {
+          for (int k = 0; k < L; k++) out[(i64)k * B + e] = 0;
+          out2[e] = SDPV_EZ;
+        } else {
+          u32 rr[160];
+          int s = bl - (32 * L - 2);
+          mag_shift(words, W, s, rr, L);
+          if (ng) neg_words(rr, L);
+          for (int k = 0; k < L; k++) out[(i64)k * B + e] = (int32_t)rr[k];
+          out2[e] = rowexp[r] + colexp[(r / rows_per_block) * N + j0 + jj] + s;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 2 * kDig);
+}
+
+template <int MODE>
+int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rpb,
+               const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st) {
+  const CtxDev& d = c->d;
+  size_t smem = 1024 + 1024 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
+  if (smem > 227 * 1024) return SDPV_EINVAL;
+  static bool attr_set[64] = {};
+  static size_t attr_val[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63] || attr_val[dev & 63] < smem) {
+    cudaError_t e = cudaFuncSetAttribute(crt_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    attr_set[dev & 63] = true;
+    attr_val[dev & 63] = smem;
+  }
+  i64 B = rows * w;
+  i64 ntiles = (B + 127) / 128;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  i64 gx = 3 * (i64)sms;
+  if (gx > ntiles) gx = ntiles;
+  crt_kernel<MODE><<<(unsigned)gx, kThreads, smem, st>>>(acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, d.n, d.E,
+                                                          d.W, d.ktc, d.Epad, d.mods, d.minv, d.inv, d.md, d.ct, out,
+                                                          out2, device_error_word());
+  return launch_status();
+}
+
+}  // namespace
+
+extern "C" int sdpv_crt_block(const sdpv_ctx* c, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                              int64_t rows, int32_t* words, int64_t* bitlen, void* stream) {
+  if (!c || N < 0 || j0 < 0 || w < 0 || j0 + w > N || rows < 0 || c->d.W > 160) return SDPV_EINVAL;
+  if (rows == 0 || w == 0) return SDPV_OK;
+  return launch_crt<0>(c, acc, ldg, N, j0, w, rows, rows, nullptr, nullptr, c->d.L, words, bitlen,
+                       sdpv::as_stream(stream));
+}
+
+extern "C" int sdpv_crt_norm(const sdpv_ctx* c, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                             int64_t rows, int64_t rows_per_block, const int64_t* rowexp, const int64_t* colexp, int L,
+                             int32_t* O, int64_t* eO, void* stream) {
+  if (!c || N < 0 || j0 < 0 || w < 0 || j0 + w > N || rows < 0 || rows_per_block < 1 || L < 1 || L > 160 ||
+      c->d.W > 160)
+    return SDPV_EINVAL;
+  if (rows == 0 || w == 0) return SDPV_OK;
+  return launch_crt<1>(c, acc, ldg, N, j0, w, rows, rows_per_block, rowexp, colexp, L, O, eO,
+                       sdpv::as_stream(stream));
+}

@@ -1,0 +1,55 @@
+// Device error word and CUDA error bookkeeping.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+
+// One word per device that loads the library; kernels OR SDPV_ERRBIT_* into it.
+__device__ unsigned g_sdpv_error_word;
+
+namespace {
+thread_local char g_last[512] = "";
+constexpr int kMaxDev = 64;
+unsigned* g_word_ptr[kMaxDev] = {};
+std::mutex g_mu;
+}  // namespace
+
+namespace sdpv {
+
+int set_cuda_error(cudaError_t e) {
+  snprintf(g_last, sizeof(g_last), "%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
+  return SDPV_ECUDA;
+}
+
+unsigned* device_error_word() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kMaxDev) return nullptr;
+  std::lock_guard<std::mutex> g(g_mu);
+  if (!g_word_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_sdpv_error_word) != cudaSuccess) return nullptr;
+    g_word_ptr[dev] = (unsigned*)p;
+  }
+  return g_word_ptr[dev];
+}
+
+}  // namespace sdpv
+
+extern "C" const char* sdpv_last_error(void) { return g_last; }
+
+extern "C" int sdpv_get_error(unsigned* flags_host, void* stream) {
+  if (!flags_host) return SDPV_EINVAL;
+  unsigned* w = sdpv::device_error_word();
+  if (!w) return SDPV_ECUDA;
+  cudaStream_t s = sdpv::as_stream(stream);
+  unsigned v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, w, sizeof(v), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && v) e = cudaMemsetAsync(w, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return sdpv::set_cuda_error(e);
+  *flags_host = v;
+  return SDPV_OK;
+}

@@ -1,0 +1,412 @@
+"""Per-entry multiprecision floating point arrays on B200: drop-in for ``sdpvibe.mpf``.
+
+MPF: m int32 (L, *shape) limb planes (little endian, two's complement), e int64 (*shape);
+value = m * 2^e; normalised: |m| has NB = 32L-2 bits (zero: m = 0, e = EZ) (sdpvibe/mpf.py:1-10).
+
+Elementwise operations are libsdpv_b200 kernels with the reference's rounding (magnitude half up).
+``gemm`` aligns rows of op(A) / columns of op(B), forms the exact product with the residue kernels and
+renormalises each entry inside the CRT kernel (one launch for CRT + rounding).  ``GramAcc`` keeps
+Q = sum_c P_c^T P_c in residue form across chunks (lower-triangle tiles only) with one CRT at the end.
+"""
+import mpmath as mp
+import numpy as np
+import torch
+
+from . import _lib
+from .limbops import shift_round, bitlen_words
+from .mpmat import ctx, KC_MAX, RES_BUDGET
+from .rns import dev
+
+EZ = -(1 << 40)                                      # exponent of zero (sdpvibe/mpf.py:21)
+LMAX_WIDE = 160
+
+
+class MPF:
+    __slots__ = ("m", "e")
+
+    def __init__(self, m, e):
+        self.m, self.e = m, e
+
+    @property
+    def L(self):
+        return self.m.shape[0]
+
+    @property
+    def shape(self):
+        return tuple(self.e.shape)
+
+    def __getitem__(self, idx):
+        if not isinstance(idx, tuple):
+            idx = (idx,)
+        return MPF(self.m[(slice(None),) + idx].contiguous(), self.e[idx].contiguous())
+
+    @property
+    def T(self):
+        """transpose of the last two dimensions"""
+        return MPF(self.m.transpose(-1, -2).contiguous(), self.e.transpose(-1, -2).contiguous())
+
+    def reshape(self, *s):
+        return MPF(self.m.reshape(self.L, *s), self.e.reshape(*s))
+
+    def clone(self):
+        return MPF(self.m.clone(), self.e.clone())
+
+    def __neg__(self):
+        return add(zeros(self.shape, self.L), self, -1)
+
+    def __add__(self, o):
+        return add(self, o, 1)
+
+    def __sub__(self, o):
+        return add(self, o, -1)
+
+    def shift(self, k):
+        """multiply by 2^k (k: int or tensor broadcastable to shape) -- exact"""
+        e = self.e + k
+        return MPF(self.m, torch.where(self.e == EZ, EZ, e))
+
+    def to_mp(self):
+        """-> numpy object array of mpmath mpf (host; tests / scalars)"""
+        L = self.L
+        a = self.m.reshape(L, -1).t().contiguous().cpu().numpy().astype(np.uint32)
+        ex = self.e.reshape(-1).cpu().numpy()
+        out = np.empty(a.shape[0], dtype=object)
+        for i in range(a.shape[0]):
+            v = int.from_bytes(a[i].tobytes(), "little", signed=True)
+            out[i] = mp.mpf(0) if v == 0 else mp.mpf((v, int(ex[i])))
+        return out.reshape(self.shape)
+
+    def to_float(self):
+        """approximate float64 values (with exponent clamping); host numpy"""
+        if self.L > 1:
+            top = self.m[-1].double() * 2.0 ** 32 + (self.m[-2].double() % 2.0 ** 32)
+        else:
+            top = self.m[-1].double()
+        sc = (self.e + 32 * (self.L - 2)).clamp(-1100, 1100).double()
+        v = torch.where(self.e == EZ, torch.zeros_like(top), top * torch.pow(2.0, sc))
+        return v.cpu().numpy()
+
+
+def zeros(shape, L):
+    return MPF(torch.zeros((L, *shape), dtype=torch.int32, device=dev),
+               torch.full(shape, EZ, dtype=torch.int64, device=dev))
+
+
+def NBITS(L):
+    return 32 * L - 2
+
+
+def from_ints(ints, exps, L, shape):
+    """Python ints (mantissas) and exponents (flat lists) -> normalised MPF"""
+    n = len(ints)
+    nb = 4 * L
+    buf = bytearray(nb * n)
+    for i, v in enumerate(ints):
+        buf[i * nb:(i + 1) * nb] = int(v).to_bytes(nb, "little", signed=True)
+    m = torch.from_numpy(np.frombuffer(bytes(buf), dtype=np.int32).reshape(n, L).T.copy()).to(dev)
+    e = torch.tensor(exps, dtype=torch.int64, device=dev)
+    return normalize(m, e, L).reshape(*shape)
+
+
+def _dec_to_bin(t, NBb):
+    """decimal string -> (signed mantissa with <= NBb bits, binary exponent) (sdpvibe/mpf.py:238-261)"""
+    t = t.strip()
+    neg = t.startswith("-")
+    if t[0] in "+-":
+        t = t[1:]
+    e10 = 0
+    if "e" in t or "E" in t:
+        t, ex = t.replace("E", "e").split("e")
+        e10 = int(ex)
+    if "." in t:
+        ip, fp = t.split(".")
+        e10 -= len(fp)
+        t = ip + fp
+    man = int(t) if t else 0
+    if man == 0:
+        return 0, EZ
+    if e10 >= 0:
+        v = man * 10 ** e10
+        bl = v.bit_length()
+        if bl <= NBb:
+            return (-v if neg else v), 0
+        sh = bl - NBb
+        v = (v + (1 << (sh - 1))) >> sh
+        return (-v if neg else v), sh
+    den = 10 ** (-e10)
+    sh = NBb + den.bit_length() - man.bit_length() + 1
+    q = ((man << sh) + den // 2) // den
+    ex = -sh
+    while q.bit_length() > NBb:
+        q = (q + 1) >> 1
+        ex += 1
+    return (-q if neg else q), ex
+
+
+def from_strings(strs, L, shape=None):
+    NBb = NBITS(L)
+    ints, exps = [], []
+    for t in strs:
+        m, e = _dec_to_bin(t, NBb)
+        ints.append(m)
+        exps.append(e)
+    return from_ints(ints, exps, L, shape or (len(ints),))
+
+
+def strings_to_host(strs, L):
+    """decimal strings -> (limbs int32 (n, L) entry-major numpy, exps int64 numpy); CPU only"""
+    NBb = NBITS(L)
+    nb = 4 * L
+    n = len(strs)
+    buf = bytearray(nb * n)
+    exps = np.empty(n, dtype=np.int64)
+    for i, t in enumerate(strs):
+        m, e = _dec_to_bin(t, NBb)
+        buf[i * nb:(i + 1) * nb] = m.to_bytes(nb, "little", signed=True)
+        exps[i] = e
+    return np.frombuffer(bytes(buf), dtype=np.int32).reshape(n, L), exps
+
+
+def host_to_mpf(limbs, exps, L, shape):
+    m = torch.from_numpy(np.ascontiguousarray(limbs.T)).to(dev)
+    e = torch.from_numpy(exps).to(dev)
+    return normalize(m, e, L).reshape(*shape)
+
+
+def from_mp(vals, L, shape=None):
+    """iterable of mpmath numbers / strings -> MPF (rounded to NB bits, half up on magnitude)"""
+    vals = list(vals)
+    NBb = NBITS(L)
+    ints, exps = [], []
+    for v in vals:
+        v = mp.mpf(v)
+        if v == 0:
+            ints.append(0)
+            exps.append(EZ)
+            continue
+        sign, man, ex, bc = v._mpf_
+        if bc > NBb:
+            sh = bc - NBb
+            man = (man + (1 << (sh - 1))) >> sh
+            ex += sh
+        ints.append(-man if sign else man)
+        exps.append(ex)
+    return from_ints(ints, exps, L, shape or (len(vals),))
+
+
+# ------------------------------------------------------------------ elementwise kernels
+def normalize(Xw, ein, L):
+    """Xw: (LI, n) int32 wide two's complement, ein (n,) -> normalised MPF (n,) (sdpvibe/mpf.py:307-313)"""
+    LI, n = Xw.shape
+    assert LI <= LMAX_WIDE
+    Xw = Xw.contiguous()
+    ein = ein.contiguous()
+    O = torch.empty((L, n), dtype=torch.int32, device=dev)
+    eO = torch.empty((n,), dtype=torch.int64, device=dev)
+    _lib.call("sdpv_mpf_norm", L, LI, n, _lib.ptr(Xw), _lib.ptr(ein), _lib.ptr(O), _lib.ptr(eO), _lib.stream())
+    return MPF(O, eO)
+
+
+def mul(A, B):
+    """entrywise product; B may be a single entry (broadcast) (sdpvibe/mpf.py:316-323)"""
+    L = A.L
+    n = A.e.numel()
+    bs = B.e.numel() == 1
+    assert bs or B.shape == A.shape
+    Am, Ae, Bm, Be = A.m.contiguous(), A.e.contiguous(), B.m.contiguous(), B.e.contiguous()
+    O = torch.empty_like(Am)
+    eO = torch.empty_like(Ae)
+    _lib.call("sdpv_mpf_mul", L, n, _lib.ptr(Am), _lib.ptr(Ae), _lib.ptr(Bm), _lib.ptr(Be), int(bs), _lib.ptr(O),
+              _lib.ptr(eO), _lib.stream())
+    return MPF(O, eO)
+
+
+def add(A, B, sgn=1):
+    """entrywise A + sgn*B (sdpvibe/mpf.py:326-331)"""
+    assert A.shape == B.shape, (A.shape, B.shape)
+    L = A.L
+    n = A.e.numel()
+    Am, Ae, Bm, Be = A.m.contiguous(), A.e.contiguous(), B.m.contiguous(), B.e.contiguous()
+    O = torch.empty_like(Am)
+    eO = torch.empty_like(Ae)
+    _lib.call("sdpv_mpf_add", L, n, _lib.ptr(Am), _lib.ptr(Ae), _lib.ptr(Bm), _lib.ptr(Be), int(sgn), _lib.ptr(O),
+              _lib.ptr(eO), _lib.stream())
+    return MPF(O, eO)
+
+
+def scalar(v, L):
+    return from_mp([v], L, (1,))
+
+
+def eye(n, L, val=1):
+    A = zeros((n, n), L)
+    d = from_mp([val], L, (1,))
+    idx = torch.arange(n, device=dev)
+    A.m[:, idx, idx] = d.m[:, :1]
+    A.e[idx, idx] = d.e[0]
+    return A
+
+
+# ------------------------------------------------------------------ reductions (host results)
+def _top(A):
+    """per-entry e + bitlen (log2 of magnitude, roughly); EZ for zeros (sdpvibe/mpf.py:348-351)"""
+    bl = bitlen_words(A.m.reshape(A.L, -1)).view(A.shape)
+    return torch.where(A.e == EZ, torch.full_like(A.e, EZ), A.e + bl)
+
+
+def total(A):
+    """exact-ish sum of all entries -> mpmath mpf (sdpvibe/mpf.py:354-366)"""
+    L = A.L
+    n = A.e.numel()
+    if n == 0:
+        return mp.mpf(0)
+    t = int(A.e.max()) - 32
+    if t < EZ // 2:
+        return mp.mpf(0)
+    s = (t - A.e.reshape(-1))
+    W = shift_round(A.m.reshape(L, -1), s, L + 2)
+    S = (W.to(torch.int64) & 0xFFFFFFFF).sum(1)
+    top = W[-1].to(torch.int64).sum()
+    S = S.cpu().tolist()
+    top = int(top)
+    v = sum(int(S[k]) << (32 * k) for k in range(L + 1)) + (top << (32 * (L + 1)))
+    return mp.mpf((v, t)) if v else mp.mpf(0)
+
+
+def dot(A, B):
+    return total(mul(A, B))
+
+
+def max_abs(A):
+    if A.e.numel() == 0:
+        return mp.mpf(0)
+    tp = _top(A).reshape(-1)
+    t = int(tp.max())
+    if t <= EZ // 2:
+        return mp.mpf(0)
+    cand = torch.nonzero(tp >= t - 1).reshape(-1)
+    Af = A.reshape(-1)
+    vals = MPF(Af.m[:, cand], Af.e[cand]).shift(-t).to_float()
+    i = int(cand[int(np.argmax(np.abs(vals)))])
+    return abs(Af[i:i + 1].to_mp()[0])
+
+
+def trace(A):
+    n = A.shape[0]
+    idx = torch.arange(n, device=dev)
+    return total(MPF(A.m[:, idx, idx], A.e[idx, idx]))
+
+
+# ------------------------------------------------------------------ GEMM
+def _align_rows(A):
+    """A (..., R, K) -> (mantissas with a common exponent per row, row exponents (..., R))
+    (sdpvibe/mpf.py:390-398)"""
+    L = A.L
+    tp = _top(A)
+    E = tp.amax(-1) - NBITS(L)
+    E = torch.where(E < EZ // 2, torch.zeros_like(E), E)
+    s = (E[..., None] - A.e).reshape(-1)
+    s = torch.where(A.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
+    return shift_round(A.m.reshape(L, -1), s, L).view(A.m.shape), E
+
+
+def gemm(A, B, transA=False, transB=False):
+    """C = op(A) op(B) (2-d, or batched 3-d (nb, ., .)); exact products, every entry rounded once
+    (operands aligned per row of op(A) / column of op(B)) (sdpvibe/mpf.py:401-452)."""
+    if A.e.dim() == 2:
+        A1 = MPF(A.m[:, None], A.e[None])
+        B1 = MPF(B.m[:, None], B.e[None])
+        C = gemm(A1, B1, transA, transB)
+        return MPF(C.m[:, 0], C.e[0])
+    if transA:
+        A = A.T
+    if not transB:
+        B = B.T                                                     # B as (nb, N, K)
+    nb, M, K = A.shape
+    nb2, N, K2 = B.shape
+    assert K == K2 and nb == nb2, (A.shape, B.shape)
+    L = A.L
+    Am, rA = _align_rows(A)                                         # (L, nb, M, K), (nb, M)
+    Bm, cB = _align_rows(B)                                         # (L, nb, N, K), (nb, N)
+    R = ctx(L)
+    acc = torch.zeros((R.n, nb * M, N), dtype=torch.int16, device=dev)
+    if K:
+        from .mpmat import residue_product
+        residue_product(R, Am.view(L, nb * M, K), Bm.view(L, nb * N, K), acc, nb=nb)
+    Om, Oe = R.crt_norm(acc, N, 0, N, nb * M, rA.reshape(-1), cB, L, rows_per_block=M)
+    return MPF(Om.view(L, nb, M, N), Oe.view(nb, M, N))
+
+
+def symmetrize(A):
+    """(A + A^T)/2"""
+    return add(A, A.T).shift(-1)
+
+
+# ------------------------------------------------------------------ Gram accumulation (Q = sum_c P_c^T P_c)
+class GramAcc:
+    """Q = sum over chunks of P_c^T P_c, accumulated exactly in residues (lower-triangle tiles only)
+    against running column reference exponents E_j, reconstructed by one CRT
+    (sdpvibe/mpf.py:536-630).  A column that outgrows its HEAD bits of headroom forces a flush (CRT of
+    the partial sum, added in MPF).  Only the lower triangle of the result is defined."""
+    HEAD = 28
+
+    def __init__(self, N, L, E_ref=None):
+        self.N, self.L = N, L
+        self.R = ctx(L + 1)
+        self.E = E_ref.clone() if E_ref is not None else torch.full((N,), EZ, dtype=torch.int64, device=dev)
+        self.Tmax = torch.full((N,), EZ, dtype=torch.int64, device=dev)
+        self.acc = None
+        self.part = None
+        self.flushes = 0
+
+    def add(self, P):
+        """P: MPF (rows, N)."""
+        L, N, R = self.L, self.N, self.R
+        tp = _top(P).amax(0)
+        live = tp > EZ // 2
+        self.Tmax = torch.maximum(self.Tmax, tp)
+        known = self.E > EZ // 2
+        if bool((live & known & (tp > self.E + self.HEAD)).any()):
+            self._flush()
+            self.E = torch.where(live & (tp > self.E), tp, self.E)
+            known = self.E > EZ // 2
+        self.E = torch.where(live & ~known, tp, self.E)
+        PT = P.T                                                    # (N, rows) contiguous
+        rows = PT.shape[1]
+        s = ((self.E - NBITS(L))[:, None] - PT.e).reshape(-1)
+        s = torch.where(PT.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
+        X = shift_round(PT.m.reshape(L, -1), s, L + 1).view(L + 1, N, rows)
+        del PT, s
+        if self.acc is None:
+            self.acc = torch.zeros((R.n, N, N), dtype=torch.int16, device=dev)
+        if rows:
+            from .mpmat import residue_product
+            residue_product(R, X, None, self.acc, syrk=True)
+
+    def _crt(self):
+        L, N, R = self.L, self.N, self.R
+        rE = torch.where(self.E > EZ // 2, self.E - NBITS(L), torch.zeros_like(self.E))
+        Om, Oe = R.crt_norm(self.acc, N, 0, N, N, rE, rE[None, :], L)
+        return MPF(Om.view(L, N, N), Oe.view(N, N))
+
+    def _flush(self):
+        if self.acc is None:
+            return
+        q = self._crt()
+        self.part = q if self.part is None else add(self.part, q)
+        self.acc = None
+        self.flushes += 1
+
+    def next_reference(self, margin=4):
+        return torch.where(self.Tmax > EZ // 2, self.Tmax + margin, self.Tmax)
+
+    def precision_loss(self):
+        ok = (self.Tmax > EZ // 2) & (self.E > EZ // 2)
+        return int((self.E - self.Tmax)[ok].max()) if bool(ok.any()) else 0
+
+    def result(self):
+        if self.acc is None:
+            return self.part
+        q = self._crt()
+        self.acc = None
+        return q if self.part is None else add(self.part, q)

@@ -1,0 +1,107 @@
+"""Exact multiprecision products through a residue number system, on B200 tensor cores.
+
+Drop-in for ``sdpvibe.rns`` (sdpvibe/rns.py): the same moduli, residue format (int8 hi/lo planes,
+r = 128 hi + lo centred) and int16 accumulator, computed by libsdpv_b200:
+
+* ``RNS.residues``   -> sdpv_residues  (tcgen05 byte-by-table product, one HBM pass)
+* ``RNS.accumulate`` -> sdpv_rns_gemm  (TMA + tcgen05 int8 GEMM, modular reduction in the epilogue)
+* ``RNS.crt_block``  -> sdpv_crt_block (pre-pass, tcgen05 digit product and carry in one kernel)
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+
+dev = "cuda"
+
+
+class RNS:
+    """Moduli and device tables for products of L-limb integers with inner dimension <= 2^17
+    (sdpvibe/rns.py:163-191)."""
+
+    KPAD = 16
+
+    def __init__(self, L, kmax=1 << 17, G=16):
+        if kmax != 1 << 17 or G != 16:
+            raise ValueError("libsdpv_b200 contexts use kmax = 2^17 and groups of 16 moduli")
+        h = ctypes.c_void_p()
+        _lib.call("sdpv_ctx_create", int(L), ctypes.byref(h))
+        self._h = h
+        n, E, W = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.call("sdpv_ctx_query", h, ctypes.byref(n), ctypes.byref(E), ctypes.byref(W))
+        self.L, self.G, self.NB = L, G, 4 * L
+        self.n, self.E, self.W = n.value, E.value, W.value
+        arr = (ctypes.c_int32 * self.n)()
+        _lib.call("sdpv_ctx_moduli", h, ctypes.cast(arr, ctypes.c_void_p))
+        self.mods = list(arr)
+        M = 1
+        for m in self.mods:
+            M *= m
+        self.M = M
+        self.device = torch.cuda.current_device()
+        self.m32 = torch.tensor(self.mods, dtype=torch.int32, device=dev)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib._lib is not None:
+            try:
+                _lib.lib().sdpv_ctx_destroy(h)
+            except Exception:
+                pass
+
+    # ---- step 1: residues (sdpvibe/rns.py:196-214)
+    def residues(self, X, k0, kc, g0=0, G=None):
+        """X: (L, rows, K) int32 limb planes -> (Rhi, Rlo) (G, rows, kp) int8, kp = kc rounded up to 16."""
+        L, rows, K = X.shape
+        assert L == self.L
+        G = G or self.n
+        kp = -(-kc // self.KPAD) * self.KPAD
+        X = X.contiguous()
+        Rhi = torch.empty((G, rows, kp), dtype=torch.int8, device=X.device)
+        Rlo = torch.empty_like(Rhi)
+        _lib.call("sdpv_residues", self._h, _lib.ptr(X), rows, K, k0, kc, g0, G, _lib.ptr(Rhi), _lib.ptr(Rlo),
+                  _lib.stream())
+        return Rhi, Rlo
+
+    # ---- step 2: accumulate residues of A @ Bt^T (sdpvibe/rns.py:217-224)
+    def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False):
+        """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows."""
+        G, Mt, KC = Ahi.shape
+        M = Mt // nb
+        N = M if syrk else Bhi.shape[1] // nb
+        _lib.call("sdpv_rns_gemm", self._h, _lib.ptr(Ahi), _lib.ptr(Alo), _lib.ptr(Bhi if not syrk else Ahi),
+                  _lib.ptr(Blo if not syrk else Alo), _lib.ptr(acc), g0, G, nb, M, N, KC, 1 if syrk else 0,
+                  _lib.stream())
+
+    # ---- step 3: CRT of a block of entries (sdpvibe/rns.py:227-245)
+    def crt_block(self, acc, N, j0, w, rows):
+        """acc (n, rows_total, N) int16; block = all rows (< rows) x columns j0..j0+w ->
+        (words (E/4, rows*w) int32, bit lengths (rows*w,) int64, rows*w)."""
+        B = rows * w
+        Wd = torch.empty((self.W, B), dtype=torch.int32, device=acc.device)
+        bl = torch.empty((B,), dtype=torch.int64, device=acc.device)
+        _lib.call("sdpv_crt_block", self._h, _lib.ptr(acc), acc.stride(0), N, j0, w, rows, _lib.ptr(Wd),
+                  _lib.ptr(bl), _lib.stream())
+        return Wd, bl, B
+
+    def crt_norm(self, acc, N, j0, w, rows, rowexp, colexp, L, rows_per_block=None):
+        """CRT fused with MPF renormalisation: entry (r, jj) gets exponent
+        rowexp[r] + colexp[r // rows_per_block, j0 + jj]; returns (m (L, rows*w), e (rows*w,))."""
+        B = rows * w
+        O = torch.empty((L, B), dtype=torch.int32, device=acc.device)
+        eO = torch.empty((B,), dtype=torch.int64, device=acc.device)
+        _lib.call("sdpv_crt_norm", self._h, _lib.ptr(acc), acc.stride(0), N, j0, w, rows, rows_per_block or rows,
+                  _lib.ptr(rowexp.contiguous()), _lib.ptr(colexp.contiguous()), L, _lib.ptr(O), _lib.ptr(eO),
+                  _lib.stream())
+        return O, eO
+
+
+def gemm_config(M, N, K):
+    """Tile shapes of the reference's Triton kernels (sdpvibe/rns.py:38-54); kept for API
+    compatibility.  The B200 kernel always uses 128 x 128 output tiles with 128-byte K slices."""
+    return 128, 128, 128, 6

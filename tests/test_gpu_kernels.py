@@ -1,0 +1,287 @@
+"""Parity of the CUDA path (libsdpv_b200 through the C ABI) with the reference's golden vectors and
+with the CPU oracle.  Every comparison is bit-exact."""
+import random
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from oracle import mp as OM
+from conftest import golden, golden_names
+
+pytestmark = pytest.mark.gpu
+
+
+def cu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import sdpvibe_b200 as sb
+    from sdpvibe_b200 import limbops, rns, mpmat, mpf  # noqa: F401
+    assert torch.cuda.is_available()
+    return sb
+
+
+def rand_limbs(rng, L, n):
+    return rng.integers(-(1 << 31), 1 << 31, size=(L, n), dtype=np.int64).astype(np.int32)
+
+
+# ------------------------------------------------------------------ limb bookkeeping
+def test_bitlen_golden(sb):
+    from sdpvibe_b200.limbops import bitlen_words
+    g = golden("bitlen")
+    assert np.array_equal(np_(bitlen_words(cu(g["X"]))), g["out"])
+
+
+@pytest.mark.parametrize("name", golden_names("shift_round_"))
+def test_shift_round_golden(sb, name):
+    from sdpvibe_b200 import _lib
+    g = golden(name)
+    X, s = cu(g["X"]), cu(g["s"])
+    Lout = g["out"].shape[0]
+    out = torch.empty((Lout, X.shape[1]), dtype=torch.int32, device="cuda")
+    flag = torch.empty((X.shape[1],), dtype=torch.int32, device="cuda")
+    _lib.call("sdpv_shift_round", _lib.ptr(X), X.shape[0], X.shape[1], _lib.ptr(s), Lout, _lib.ptr(out),
+              _lib.ptr(flag), _lib.stream())
+    assert np.array_equal(np_(out), g["out"])
+    assert np.array_equal(np_(flag), g["flag"])
+
+
+def test_shift_round_random_large(sb):
+    from sdpvibe_b200.limbops import shift_round
+    rng = np.random.default_rng(1)
+    for Lin, Lout in ((26, 27), (27, 24), (5, 9)):
+        X = rand_limbs(rng, Lin, 200_003)
+        s = rng.integers(-70, 32 * Lin + 40, size=X.shape[1])
+        ref, _ = O.shift_round(X, s, Lout)
+        assert np.array_equal(np_(shift_round(cu(X), cu(s), Lout)), ref)
+
+
+def test_overflow_flag_device_word(sb):
+    from sdpvibe_b200.limbops import shift_round, check_errors
+    check_errors()                                       # clear
+    X = cu(O.to_limbs([(1 << 60) + 5, 3], 3))
+    shift_round(X, cu(np.array([-10, 0])), 2)            # 2^70 does not fit two limbs
+    with pytest.raises(OverflowError):
+        check_errors()
+    check_errors()                                       # cleared by the previous read
+
+
+@pytest.mark.parametrize("name", golden_names("add_same_"))
+def test_add_same_golden(sb, name):
+    from sdpvibe_b200.limbops import add_same
+    g = golden(name)
+    assert np.array_equal(np_(add_same(cu(g["A"]), cu(g["B"]), 1)), g["plus"])
+    assert np.array_equal(np_(add_same(cu(g["A"]), cu(g["B"]), -1)), g["minus"])
+
+
+@pytest.mark.parametrize("name", golden_names("badd_"))
+def test_badd_golden(sb, name):
+    from sdpvibe_b200 import _lib
+    g = golden(name)
+    L = g["A"].shape[0]
+    nb, rows, cols = 2, 3, 5
+    EA = cu(np.broadcast_to(g["ea"].reshape(nb, cols), (nb, cols)).copy())
+    EB = cu(np.broadcast_to(g["eb"].reshape(nb, cols), (nb, cols)).copy())
+    A, B = cu(g["A"]), cu(g["B"])
+    for sgn in (1, -1):
+        out = torch.empty_like(A)
+        eo = torch.empty((nb, cols), dtype=torch.int64, device="cuda")
+        _lib.call("sdpv_badd_align", _lib.ptr(A), _lib.ptr(B), _lib.ptr(EA), _lib.ptr(EB), L, nb, rows, cols, sgn,
+                  _lib.ptr(out), _lib.ptr(eo), _lib.stream())
+        assert np.array_equal(np_(out).reshape(g[f"C_{sgn}"].shape), g[f"C_{sgn}"])
+        assert np.array_equal(np_(eo), np.broadcast_to(g[f"e_{sgn}"], (nb, cols)))
+
+
+# ------------------------------------------------------------------ MPF elementwise
+@pytest.mark.parametrize("name", golden_names("mpf_elem_"))
+def test_mpf_elementwise_golden(sb, name):
+    from sdpvibe_b200.mpf import MPF, mul, add, normalize
+    g = golden(name)
+    L = g["am"].shape[0]
+    A = MPF(cu(g["am"]), cu(g["ae"]))
+    B0 = MPF(cu(g["b0m"]), cu(g["b0e"]))
+    B2 = MPF(cu(g["bm"]), cu(g["be"]))
+    S = MPF(cu(g["scm"]), cu(g["sce"]))
+    for got, key in ((mul(A, B0), "mul"), (mul(A, S), "muls"), (add(A, B2, 1), "add"), (add(A, B2, -1), "sub"),
+                     (normalize(cu(g["wide"]), cu(g["ein"]), L), "nrm")):
+        assert np.array_equal(np_(got.m), g[f"{key}_m"]), key
+        assert np.array_equal(np_(got.e), g[f"{key}_e"]), key
+
+
+def test_mpf_elementwise_random_large(sb):
+    from sdpvibe_b200.mpf import MPF, mul, add
+    rng = np.random.default_rng(7)
+    for L in (24, 26, 27):
+        n = 100_000
+        am, bm = rand_limbs(rng, L, n), rand_limbs(rng, L, n)
+        ae, be = rng.integers(-500, 500, n), rng.integers(-500, 500, n)
+        A, B = MPF(cu(am), cu(ae)), MPF(cu(bm), cu(be))
+        m, e = O.mpf_mul(am, ae, bm, be)
+        C = mul(A, B)
+        assert np.array_equal(np_(C.m), m) and np.array_equal(np_(C.e), e)
+        m, e = O.mpf_add(am, ae, bm, be, -1)
+        C = add(A, B, -1)
+        assert np.array_equal(np_(C.m), m) and np.array_equal(np_(C.e), e)
+
+
+# ------------------------------------------------------------------ residues (a)
+@pytest.mark.parametrize("name", golden_names("residues_"))
+def test_residues_golden(sb, name):
+    from sdpvibe_b200.mpmat import ctx
+    g = golden(name)
+    L = g["X"].shape[0]
+    R = ctx(L)
+    assert R.n == int(g["n"])
+    for g0, G in ((0, R.n), (R.n - 16, 16)):
+        hi, lo = R.residues(cu(g["X"]), int(g["k0"]), int(g["kc"]), g0, G)
+        assert np.array_equal(np_(hi), g[f"hi_{g0}"])
+        assert np.array_equal(np_(lo), g[f"lo_{g0}"])
+
+
+@pytest.mark.parametrize("L,rows,K,k0,kc", [(24, 37, 700, 5, 651), (27, 274, 300, 0, 300), (26, 3, 4097, 1, 4096),
+                                             (50, 9, 130, 2, 120), (64, 5, 64, 0, 64), (1, 11, 33, 0, 33)])
+def test_residues_random(sb, L, rows, K, k0, kc):
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(L * 1000 + K)
+    X = rng.integers(-(1 << 31), 1 << 31, size=(L, rows, K), dtype=np.int64).astype(np.int32)
+    X[:, 0, :8] = 0
+    X[-1, 0, 1] = -(1 << 31)
+    T = O.tables(L)
+    R = ctx(L)
+    hi, lo = R.residues(cu(X), k0, kc)
+    rh, rl = O.residues(T, X, k0, kc)
+    assert np.array_equal(np_(hi), rh) and np.array_equal(np_(lo), rl)
+
+
+# ------------------------------------------------------------------ residue GEMM (b), syrk (d)
+@pytest.mark.parametrize("name", golden_names("accumulate_"))
+def test_accumulate_golden(sb, name):
+    from sdpvibe_b200.mpmat import ctx
+    g = golden(name)
+    R = ctx(int(name.split("L")[1]))
+    acc = cu(g["acc0"]).clone()
+    R.accumulate(cu(g["Ahi"]), cu(g["Alo"]), cu(g["Bhi"]), cu(g["Blo"]), acc, 0)
+    assert np.array_equal(np_(acc), g["acc"])
+
+
+def _rand_residues(rng, T, G, rows, K):
+    m = T.m32[:G].astype(np.int64)[:, None, None]
+    r = rng.integers(0, 1 << 30, size=(G, rows, K)) % m
+    r = np.where(r > m // 2, r - m, r)
+    lo = ((r + 64) & 127) - 64
+    return ((r - lo) >> 7).astype(np.int8), lo.astype(np.int8)
+
+
+@pytest.mark.parametrize("L,nb,M,N,K,syrk", [(24, 1, 256, 256, 256, False), (26, 1, 300, 129, 1024, False),
+                                              (27, 1, 274, 274, 2000, True), (24, 3, 70, 45, 48, False),
+                                              (10, 5, 33, 33, 16, True), (26, 2, 130, 7, 4096, False)])
+def test_rns_gemm_random(sb, L, nb, M, N, K, syrk):
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(M * N + K)
+    T = O.tables(L)
+    R = ctx(L)
+    Ah, Al = _rand_residues(rng, T, T.n, nb * M, K)
+    Bh, Bl = (Ah, Al) if syrk else _rand_residues(rng, T, T.n, nb * (N if not syrk else M), K)
+    m = T.m32.astype(np.int64)[:, None, None]
+    acc0 = (rng.integers(0, 1 << 30, size=(T.n, nb * M, N)) % m).astype(np.int16)
+    acc = cu(acc0).clone()
+    R.accumulate(cu(Ah), cu(Al), cu(Bh), cu(Bl), acc, 0, nb=nb, syrk=syrk)
+    got = np_(acc)
+    for b in range(nb):
+        sl = slice(b * M, (b + 1) * M)
+        ref = O.accumulate(T, Ah[:, sl], Al[:, sl], Bh[:, b * N:(b + 1) * N] if not syrk else Ah[:, sl],
+                           Bl[:, b * N:(b + 1) * N] if not syrk else Al[:, sl], acc0[:, sl], 0, lower=syrk)
+        assert np.array_equal(got[:, sl], ref)
+
+
+# ------------------------------------------------------------------ CRT (c)
+@pytest.mark.parametrize("name", golden_names("crt_block_"))
+def test_crt_block_golden(sb, name):
+    from sdpvibe_b200.mpmat import ctx
+    g = golden(name)
+    R = ctx(int(name.split("L")[1]))
+    acc = cu(g["acc"])
+    for width in (1, 5, 11):
+        W, bl, cnt = R.crt_block(acc, acc.shape[2], int(g["start"]), width, acc.shape[1])
+        assert np.array_equal(np_(W), g[f"W_{width}"])
+        assert np.array_equal(np_(bl), g[f"bl_{width}"])
+
+
+@pytest.mark.parametrize("L", [24, 27, 34, 50])
+def test_crt_norm_random(sb, L):
+    from sdpvibe_b200.mpmat import ctx
+    rng = random.Random(L)
+    T = O.tables(L)
+    R = ctx(L)
+    rows, N = 37, 53
+    lim = T.M // 4
+    vals = [rng.randrange(-lim + 1, lim) >> rng.randrange(0, T.M.bit_length() - 3) for _ in range(rows * N)]
+    vals[:6] = [0, 1, -1, lim - 1, -lim + 1, 1 << 77]
+    acc = np.array([[v % p for v in vals] for p in T.mods], np.int16).reshape(T.n, rows, N)
+    rowexp = np.array([rng.randrange(-900, 900) for _ in range(rows)], np.int64)
+    colexp = np.array([rng.randrange(-900, 900) for _ in range(N)], np.int64)
+    Wd, bl = O.crt_block(T, acc, N, 3, 41, rows)
+    ein = (rowexp[:, None] + colexp[None, 3:44]).reshape(-1)
+    rm, re_ = O.mpf_norm(Wd, ein, L)
+    m, e = R.crt_norm(cu(acc), N, 3, 41, rows, cu(rowexp), cu(colexp), L)
+    assert np.array_equal(np_(m), rm) and np.array_equal(np_(e), re_)
+    W2, bl2, _ = R.crt_block(cu(acc), N, 3, 41, rows)
+    assert np.array_equal(np_(W2), Wd) and np.array_equal(np_(bl2), bl)
+
+
+# ------------------------------------------------------------------ composed paths
+@pytest.mark.parametrize("name", golden_names("gemm_nt_L"))
+def test_gemm_nt_golden(sb, name):
+    from sdpvibe_b200.mpmat import MP, gemm_nt
+    g = golden(name)
+    mode = str(g["mode"])
+    mode = int(mode) if mode.lstrip("-").isdigit() else mode
+    C = gemm_nt(MP(cu(g["A"]), int(g["eA"])), MP(cu(g["B"]), int(g["eB"])), out_exp=mode)
+    assert np.array_equal(np_(C.limbs), g["C"])
+    assert np.array_equal(np.broadcast_to(np_(C.exp), g["Ce"].shape), g["Ce"])
+
+
+@pytest.mark.parametrize("name", golden_names("gemm_nt_rowexp_"))
+def test_gemm_nt_rowexp_golden(sb, name):
+    from sdpvibe_b200.mpmat import MP, gemm_nt
+    g = golden(name)
+    C = gemm_nt(MP(cu(g["A"]), int(g["eA"])), MP(cu(g["B"]), 0), out_exp="col", bt_rowexp=cu(g["rowexp"]))
+    assert np.array_equal(np_(C.limbs), g["C"]) and np.array_equal(np_(C.exp), g["Ce"])
+
+
+@pytest.mark.parametrize("name", golden_names("mpf_gemm_"))
+def test_mpf_gemm_golden(sb, name):
+    from sdpvibe_b200.mpf import MPF, gemm
+    g = golden(name)
+    C = gemm(MPF(cu(g["Am"]), cu(g["Ae"])), MPF(cu(g["Bm"]), cu(g["Be"])), bool(g["tA"]), bool(g["tB"]))
+    assert np.array_equal(np_(C.m), g["Cm"]) and np.array_equal(np_(C.e), g["Ce"])
+
+
+def _lower(m, e):
+    N = e.shape[-1]
+    low = np.tril(np.ones((N, N), bool))
+    return np.where(low, m, 0), np.where(low, e, 0)
+
+
+@pytest.mark.parametrize("name", golden_names("gramacc_"))
+def test_gramacc_golden(sb, name):
+    from sdpvibe_b200.mpf import MPF, GramAcc
+    g = golden(name)
+    chunks = [MPF(cu(g[f"P{i}m"]), cu(g[f"P{i}e"])) for i in range(3) if f"P{i}m" in g]
+    N, L = chunks[0].shape[1], chunks[0].L
+    acc = GramAcc(N, L, E_ref=cu(g["Eref"]) if name == "gramacc_eref" else None)
+    for c in chunks:
+        acc.add(c)
+    Q = acc.result()
+    gm, ge = _lower(g["Qm"], g["Qe"])
+    om, oe = _lower(np_(Q.m), np_(Q.e))
+    assert np.array_equal(om, gm) and np.array_equal(oe, ge)
+    assert acc.flushes == int(g["flushes"])
