@@ -1,0 +1,355 @@
+"""Benchmark: residue-form Gram accumulation at 832 bits on one B200 (per GPU).
+
+Workload (one "step"): Q = sum_b B_b^T B_b for 400 blocks B_b of m_b x 274 (m_b ~ U[20,120], numpy
+seed 0) of 832-bit MPF entries (L = 26 limbs; mantissas of NB = 830 bits, random sign, exponents
+U[-8, 8]), streamed as 4 chunks of 100 blocks through sdpvibe_b200.mpf.GramAcc(274, 26) with one CRT
+-- the reference's GramAcc (sdpvibe/mpf.py:536-630) on its Gram configuration.
+
+Metric: residue-GEMM INT8 TOPS, counted the reference's way: n_mod (128 moduli at L+1 = 27 limbs)
+x 4 digit products x 2 ops x N(N+1)/2 x R per step, divided by the step time.  Also reported as
+mp-MAC/s.  `value` times the step with inputs resident in HBM; `e2e` times the same step through the
+public API with pinned host inputs copied in and Q copied out inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+Under torchrun each rank runs one replica (the Gram step has no cross-GPU exchange in scope);
+rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "768-bit SDP s/iter & residue-GEMM INT8 TOPS, fused vs plain, 1 B200, bit-exact"
+NBLOCKS, MLO, MHI, NCOLS, L, NCHUNK = 400, 20, 120, 274, 26, 4
+N_MOD = 128                       # moduli of the accumulator context (L + 1 = 27 limbs)
+# DRAM bytes (read + write) of one syrk launch per chunk row, from the ncu capture of
+# `kernel_bench --kernel syrk --N 274 --K 7000 --L 27` (509.1 MB read + 12.2 MB written / 7000 rows).
+SYRK_DRAM_BYTES_PER_ROW = (509.113088e6 + 12.194816e6) / 7000
+
+
+def workload_shape(seed=0):
+    rng = np.random.default_rng(seed)
+    m = rng.integers(MLO, MHI + 1, size=NBLOCKS)
+    per = NBLOCKS // NCHUNK
+    rows = [int(m[c * per:(c + 1) * per].sum()) for c in range(NCHUNK)]
+    return m, rows
+
+
+def gen_chunk(rng, rows, cols, L):
+    """Normalised MPF (rows, cols): |mantissa| has exactly 32L-2 bits, random sign, e ~ U[-8, 8]."""
+    n = rows * cols
+    mag = rng.integers(0, 1 << 32, size=(L, n), dtype=np.uint64).astype(np.uint32)
+    mag[L - 1] = (mag[L - 1] & np.uint32((1 << 29) - 1)) | np.uint32(1 << 29)
+    neg = rng.random(n) < 0.5
+    m = mag.copy()
+    m[:, neg] = ~m[:, neg]
+    carry = neg.copy()
+    for k in range(L):                                    # two's-complement negation, +1 with carry
+        v = m[k].astype(np.uint64) + carry
+        m[k] = v.astype(np.uint32)
+        carry = carry & (v > 0xffffffff)
+    e = rng.integers(-8, 9, size=n).astype(np.int64)
+    return m.view(np.int32).reshape(L, rows, cols), e.reshape(rows, cols)
+
+
+def algorithmic_ops(R, N=NCOLS):
+    return N_MOD * 4 * 2 * (N * (N + 1) // 2) * R
+
+
+def mp_macs(R, N=NCOLS):
+    return (N * (N + 1) // 2) * R
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs"), d.get("bf16_tflops"), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ CPU baseline (reference's own CPU path)
+def cpu_reference_sample(threads):
+    """Time the reference's CPU baseline (cpu_baseline/mpf_baseline.c: GMP mpf, OpenMP) on a bounded
+    sample: its 274 x 274 x 274 GEMM at 832 bits.  Returns (seconds for that GEMM, kind, sample)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mpf_baseline")
+    if not os.path.exists(exe):
+        from oracle import ref_build
+        ref_build.build_cpu_baseline()
+    if os.path.exists(exe):
+        out = subprocess.run([exe, "832", str(NCOLS), str(NCOLS), str(threads)], capture_output=True, text=True,
+                             timeout=600).stdout
+        for line in out.splitlines():
+            if line.strip().startswith("gemm"):
+                return float(line.split()[1]), "reference", (
+                    f"cpu_baseline/mpf_baseline.c gemm {NCOLS}x{NCOLS}x{NCOLS} at 832 bits (GMP mpf, {threads} "
+                    f"threads), scaled by mp-MACs to the Gram step's N(N+1)/2*R")
+    # oracle port: the C restatement of the residue path, single thread, on 2 blocks of the workload
+    import oracle as O
+    from oracle import mp as OM
+    rng = np.random.default_rng(1)
+    rows = 140
+    pm, pe = gen_chunk(rng, rows, NCOLS, L)
+    t = time.perf_counter()
+    acc = OM.GramAcc(NCOLS, L)
+    acc.add(pm, pe)
+    acc.result()
+    dt = time.perf_counter() - t
+    return dt * (NCOLS ** 3) / mp_macs(rows), "port", f"oracle GramAcc on {rows} rows x {NCOLS} (1 thread), scaled"
+
+
+def cpu_baseline(R, threads):
+    t_gemm, kind, sample = cpu_reference_sample(threads)
+    t_step = t_gemm * mp_macs(R) / NCOLS ** 3
+    return {"value": algorithmic_ops(R) / t_step / 1e12, "unit": "TOPS", "cores": threads if kind == "reference" else 1,
+            "kind": kind, "sample": sample, "s_per_step": t_step,
+            "mp_mac_per_s": mp_macs(R) / t_step}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation of the path, on rank 0 only."""
+    if rank != 0:
+        return
+    m, rows = workload_shape()
+    R = int(sum(rows))
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_sample(threads)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        t_gemm, kind, sample = cpu_reference_sample(threads)
+        vals.append(t_gemm * mp_macs(R) / NCOLS ** 3)
+    wall = time.perf_counter() - t0
+    t_step = statistics.mean(vals)
+    value = algorithmic_ops(R) / t_step / 1e12
+    cfg = workload_config(R)
+    line = {"metric": METRIC, "value": value, "unit": "TOPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mpf-832 (GMP)", "data": "synthetic", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "TOPS", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "TOPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(R):
+    return {"workload": "gram_acc: Q = sum_b B_b^T B_b, 400 blocks m_b~U[20,120] (seed 0) x 274 cols, 832-bit MPF "
+                        "(L=26, accumulator L+1=27, 128 moduli), 4 chunks, one CRT",
+            "blocks": NBLOCKS, "rows_total": R, "cols": NCOLS, "limbs": L, "chunks": NCHUNK,
+            "exponents": "U[-8,8]", "l2": "inputs (~0.86 GB) larger than L2 (126 MB); no flush",
+            "parallelism": "replicas"}
+
+
+# ------------------------------------------------------------------ B200 arm
+def measure_int8_library_peak(torch):
+    """cuBLASLt int8 GEMM (torch._int_mm) 8192^3, best of 5 -- a library reference point only."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(); torch._int_mm(a, b); e.record(); e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from sdpvibe_b200 import mpf, _trace
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    m, rows = workload_shape()
+    R = int(sum(rows))
+    rng = np.random.default_rng(100 + rank)
+    host = [gen_chunk(rng, r, NCOLS, L) for r in rows]
+    chunks = [mpf.MPF(torch.from_numpy(hm).to(dev), torch.from_numpy(he).to(dev)) for hm, he in host]
+    pinned = [(torch.from_numpy(hm).pin_memory(), torch.from_numpy(he).pin_memory()) for hm, he in host]
+    h2d = sum(a.numel() * a.element_size() + b.numel() * b.element_size() for a, b in pinned)
+    out_m = torch.empty((L, NCOLS, NCOLS), dtype=torch.int32).pin_memory()
+    out_e = torch.empty((NCOLS, NCOLS), dtype=torch.int64).pin_memory()
+    d2h = out_m.numel() * 4 + out_e.numel() * 8
+
+    def step():
+        acc = mpf.GramAcc(NCOLS, L)
+        for c in chunks:
+            acc.add(c)
+        return acc.result()
+
+    def step_e2e():
+        acc = mpf.GramAcc(NCOLS, L)
+        for hm, he in pinned:
+            acc.add(mpf.MPF(hm.to(dev, non_blocking=True), he.to(dev, non_blocking=True)))
+        Q = acc.result()
+        out_m.copy_(Q.m, non_blocking=True)
+        out_e.copy_(Q.e, non_blocking=True)
+        return Q
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, k, trace=None):
+        barrier()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        if trace is not None:
+            with trace:
+                for _ in range(k):
+                    fn()
+        else:
+            for _ in range(k):
+                fn()
+        e.record()
+        barrier()
+        ms = s.elapsed_time(e)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm"})
+    with ClockSampler(local_rank) as clk:
+        ms = timed(step, args.steps, tr)
+    for _ in range(2):
+        step_e2e()
+    ms_e2e = timed(step_e2e, args.steps)
+
+    t_step = ms / args.steps * 1e-3
+    value = world * algorithmic_ops(R) / t_step / 1e12
+    gemm_ms = tr.kernel_ms("sdpv_rns_gemm")
+    res_ms = tr.kernel_ms("sdpv_residues")
+    crt_ms = tr.kernel_ms("sdpv_crt_norm")
+    hbm, bf16, src = load_peaks()
+    if rank != 0:
+        return
+    int8_lib = measure_int8_library_peak(torch)
+    peak = 2 * bf16
+    ops_per_launch = algorithmic_ops(R) / NCHUNK
+    achieved = ops_per_launch / (statistics.mean(gemm_ms) * 1e-3) / 1e12
+    # decomposition: limb bytes read (L+1 limbs after alignment) + residue bytes written, per launch
+    res_bytes = (R / NCHUNK) * NCOLS * (4 * (L + 1) + 2 * N_MOD)
+    line = {
+        "metric": METRIC, "value": value, "unit": "TOPS", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8 (exact int8 x int8 -> int32 residue products)", "data": "synthetic",
+        "config": workload_config(R),
+        "mp_mac_per_s": world * mp_macs(R) / t_step,
+        "roofline": {"bound": "tensor", "kernel": "sdpv_rns_gemm (syrk, tcgen05 kind::i8)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": SYRK_DRAM_BYTES_PER_ROW * (R / NCHUNK),
+                     "traffic_note": "ncu dram read+write of one launch at N=274, K=7000 rows, scaled per row",
+                     "peak_source": f"2 x bf16_tflops of {src} (MEASURED_PEAKS.json): B200 dense int8 = 2 x dense bf16",
+                     "int8_cublaslt_measured_tops": int8_lib,
+                     "launch_ms_mean": statistics.mean(gemm_ms), "launches": len(gemm_ms),
+                     "ops_per_launch": ops_per_launch},
+        "roofline_decomposition": {"bound": "hbm", "kernel": "sdpv_residues", "achieved":
+                                   res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                                   "frac": res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9 / hbm,
+                                   "launch_ms_mean": statistics.mean(res_ms), "bytes_per_launch": res_bytes},
+        "crt_ms": sum(crt_ms) / args.steps,
+        "e2e": {"value": world * algorithmic_ops(R) / (ms_e2e / args.steps * 1e-3) / 1e12, "unit": "TOPS",
+                "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": tr.total_launches,
+        "launches_by_entry": dict(tr.launches),
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(R, os.cpu_count() or 1)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
