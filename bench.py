@@ -78,7 +78,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -89,7 +89,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -273,7 +273,7 @@ def run_b200(args, rank, world, local_rank):
 
     for _ in range(max(args.warmup, 3)):
         step()
-    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm"})
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
     with ClockSampler(local_rank) as clk:
         ms = timed(step, args.steps, tr)
     for _ in range(2):
@@ -313,6 +313,7 @@ def run_b200(args, rank, world, local_rank):
                                    "frac": res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9 / hbm,
                                    "launch_ms_mean": statistics.mean(res_ms), "bytes_per_launch": res_bytes},
         "crt_ms": sum(crt_ms) / args.steps,
+        "kernel_ms_per_step": {k: sum(tr.kernel_ms(k)) / args.steps for k in sorted(tr.timed)},
         "e2e": {"value": world * algorithmic_ops(R) / (ms_e2e / args.steps * 1e-3) / 1e12, "unit": "TOPS",
                 "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": tr.total_launches,
@@ -327,7 +328,7 @@ def run_b200(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

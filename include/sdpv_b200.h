@@ -91,23 +91,40 @@ int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
 int sdpv_mpf_norm(int L, int LI, int64_t n, const int32_t* X, const int64_t* eI, int32_t* O, int64_t* eO,
                   void* stream);
 
+/* ---------------------------------------------------------------- operand alignment
+ * MPF array m (L, nb, R, C) / e (nb, R, C).  top = e + bitlen(m), EZ for zero entries.
+ * axis 1: out (nb, R) = max over columns of each row; axis 0: out (nb, C) = max over rows of each column.
+ * Replaces _top(A).amax(...) (sdpvibe/mpf.py:348-351, 393, 563). */
+int sdpv_top_max(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, int axis, int64_t* out,
+                 void* stream);
+/* out = m rounded half up (ties toward +infinity) to the exponent target[b][r] (per_col = 0) or target[b][c]
+ * (per_col = 1), as Lout limbs; zero entries (e = EZ) become 0; transpose = 1 writes (Lout, nb, C, R) instead of
+ * (Lout, nb, R, C).  Overflow sets the device error word.  L <= 64.  Replaces the transposing copy plus
+ * shift_round of mpf._align_rows (sdpvibe/mpf.py:390-398) and GramAcc.add (sdpvibe/mpf.py:572-576). */
+int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, const int64_t* target,
+               int per_col, int transpose, int Lout, int32_t* out, void* stream);
+
 /* ---------------------------------------------------------------- residue decomposition (a)
  * Residues of X[:, :, k0:k0+kc] for moduli g0..g0+G of ctx: X (L, rows, ld) int32 limb planes;
- * Rhi, Rlo (G, rows, kp) int8, kp = kc rounded up to 16, zero residues for kc <= k < kp.
+ * Rhi, Rlo (G, rows, kp) int8, kp = kc rounded up to 16, zero residues for kc <= k < kp; plane_stride = bytes
+ * between the planes of consecutive moduli (0: rows*kp, contiguous; otherwise a multiple of 16 >= rows*kp --
+ * an odd multiple of 2 KB keeps the 2G concurrent plane streams on different HBM channels).
  * Replaces RNS.residues / _residue_kernel (sdpvibe/rns.py:66-103, 196-214). */
 int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0,
-                  int G, int8_t* Rhi, int8_t* Rlo, void* stream);
+                  int G, int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream);
 
 /* ---------------------------------------------------------------- residue GEMM (b) and Gram (d)
  * For each of the G moduli g0..g0+G and each of nb blocks:
  *   acc[g0+g][b*M + i][j] <- (acc + A_gb B_gb^T) mod m, A_gb = 128 Ahi + Alo (M x KC), B likewise (N x KC)
- * with A* (G, nb*M, KC), B* (G, nb*N, KC) int8, acc (n, nb*M, N) int16.  mode 0: all entries;
+ * with A* (G, nb*M, KC), B* (G, nb*N, KC) int8 whose modulus planes are a_stride / b_stride bytes apart (0: packed),
+ * acc (n, nb*M, ldc) int16 (row stride ldc >= N; a
+ * multiple of 8 lets the epilogue move 16 bytes at a time).  mode 0: all entries;
  * mode 1 (syrk): B = A (Bhi/Blo ignored, N = M) and only entries with i >= j are updated.
  * KC must be a multiple of 16 and <= 65536.  Replaces RNS.accumulate / _gemm_kernel
  * (sdpvibe/rns.py:106-137, 217-224), batched._bgemm_kernel (sdpvibe/batched.py:96-127) and
  * batched._syrk_lower_kernel (sdpvibe/batched.py:130-162). */
 int sdpv_rns_gemm(const sdpv_ctx* ctx, const int8_t* Ahi, const int8_t* Alo, const int8_t* Bhi, const int8_t* Blo,
-                  int16_t* acc, int g0, int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream);
+                  int64_t a_stride, int64_t b_stride, int16_t* acc, int64_t ldc, int g0, int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream);
 
 /* ---------------------------------------------------------------- CRT reconstruction (c)
  * Exact integers of the block "all rows x columns j0..j0+w" of acc (n, rows_total, N) (modulus
@@ -117,7 +134,7 @@ int sdpv_rns_gemm(const sdpv_ctx* ctx, const int8_t* Ahi, const int8_t* Alo, con
 int sdpv_crt_block(const sdpv_ctx* ctx, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
                    int64_t rows, int32_t* words, int64_t* bitlen, void* stream);
 
-/* CRT fused with renormalisation to MPF (mf_norm semantics): for the same block, entry (r, jj) with
+/* CRT fused with renormalisation to MPF (mpf_norm semantics): for the same block, entry (r, jj) with
  * exponent rowexp[r] + colexp[(r / rows_per_block) * N + j0 + jj] is written to O (L, rows*w) /
  * eO (rows*w).  Replaces the crt_block + normalize pairs of mpf.gemm (sdpvibe/mpf.py:440-450) and
  * GramAcc._crt (sdpvibe/mpf.py:595-610). */

@@ -34,8 +34,10 @@ _SIGS = {
     "sdpv_mpf_mul": [_I, _L, _P, _P, _P, _P, _I, _P, _P, _P],
     "sdpv_mpf_add": [_I, _L, _P, _P, _P, _P, _I, _P, _P, _P],
     "sdpv_mpf_norm": [_I, _I, _L, _P, _P, _P, _P, _P],
-    "sdpv_residues": [_P, _P, _L, _L, _L, _L, _I, _I, _P, _P, _P],
-    "sdpv_rns_gemm": [_P, _P, _P, _P, _P, _P, _I, _I, _L, _L, _L, _L, _I, _P],
+    "sdpv_top_max": [_P, _P, _I, _L, _L, _L, _I, _P, _P],
+    "sdpv_align": [_P, _P, _I, _L, _L, _L, _P, _I, _I, _I, _P, _P],
+    "sdpv_residues": [_P, _P, _L, _L, _L, _L, _I, _I, _P, _P, _L, _P],
+    "sdpv_rns_gemm": [_P, _P, _P, _P, _P, _L, _L, _P, _L, _I, _I, _L, _L, _L, _L, _I, _P],
     "sdpv_crt_block": [_P, _P, _L, _L, _L, _L, _L, _P, _P, _P],
     "sdpv_crt_norm": [_P, _P, _L, _L, _L, _L, _L, _L, _P, _P, _I, _P, _P, _P],
     "sdpv_get_error": [ctypes.POINTER(ctypes.c_uint), _P],
@@ -74,6 +76,13 @@ def ptr(t):
     if not t.is_cuda:
         raise RuntimeError("sdpvibe_b200 kernels need CUDA tensors (no CPU fallback)")
     assert t.is_contiguous(), "kernel operands must be contiguous"
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def ptr_strided(t):
+    """Device pointer of a tensor view whose strides the caller passes explicitly."""
+    if not t.is_cuda:
+        raise RuntimeError("sdpvibe_b200 kernels need CUDA tensors (no CPU fallback)")
     return ctypes.c_void_p(t.data_ptr())
 
 

@@ -1,0 +1,228 @@
+// Alignment of MPF operands to per-row / per-column reference exponents (the set-up of every exact GEMM).
+//
+// top(e) = e + bitlen(m) (EZ for zero entries, sdpvibe/mpf.py:348-351); the reference takes the max of
+// top over each row of op(A) / column of op(B) (mpf.py:390-398) or over each column of a Gram chunk
+// (mpf.py:563), and re-rounds every entry to that reference exponent with limbops.shift_round
+// (ties toward +infinity), after a transposing copy.  Here:
+//   sdpv_top_max: the reduction in one launch (rows: one warp per row; columns: column strips with a
+//                 64-bit atomic max), reading only the top limbs of normalised data;
+//   sdpv_align:   the rounding shift fused with the transpose: a 16 x 32 tile of entries is staged in
+//                 shared memory with all its limbs (coalesced along columns), then each thread rounds
+//                 its entries and writes the output limb planes coalesced along the new fast axis.
+#include "common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ i64 entry_top(const int32_t* __restrict__ m, i64 plane, i64 idx, int L, i64 e) {
+  if (e == SDPV_EZ) return SDPV_EZ;
+  u32 ext = (m[(i64)(L - 1) * plane + idx] < 0) ? 0xffffffffu : 0u;
+  for (int k = L - 1; k >= 0; k--) {
+    u32 x = (u32)m[(i64)k * plane + idx] ^ ext;
+    if (x) return e + 32 * (i64)k + 32 - __clz(x);
+  }
+  return e;
+}
+
+// Max over the contiguous axis: one warp per (b, r).
+__global__ void top_max_rows_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e, int L, i64 nrows, i64 C,
+                                    i64* __restrict__ out) {
+  i64 row = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const i64 plane = nrows * C;
+  i64 best = SDPV_EZ;
+  for (i64 c = lane; c < C; c += 32) {
+    i64 idx = row * C + c;
+    i64 t = entry_top(m, plane, idx, L, e[idx]);
+    best = t > best ? t : best;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    i64 v = __shfl_xor_sync(0xffffffffu, best, o);
+    best = v > best ? v : best;
+  }
+  if (lane == 0) out[row] = best;
+}
+
+__global__ void fill_kernel(i64* __restrict__ out, i64 n, i64 v) {
+  i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+// Max over the strided axis: blocks of 32 columns x 8 row groups; each thread takes 16 rows with all
+// loads issued before any is used, then a shared-memory reduction and one 64-bit atomic max per column.
+constexpr int kColRows = 16;
+__global__ void __launch_bounds__(kThreads) top_max_cols_kernel(const int32_t* __restrict__ m,
+                                                                const i64* __restrict__ e, int L, i64 nb, i64 R,
+                                                                i64 C, i64* __restrict__ out) {
+  __shared__ i64 red[8][32];
+  const int cx = threadIdx.x & 31, ry = threadIdx.x >> 5;
+  const i64 c = (i64)blockIdx.x * 32 + cx;
+  const i64 b = blockIdx.z;
+  const i64 r0 = ((i64)blockIdx.y * 8 + ry) * kColRows;
+  const i64 plane = nb * R * C;
+  i64 best = SDPV_EZ;
+  if (c < C) {
+    i64 ev[kColRows];
+    int32_t tw[kColRows];
+#pragma unroll
+    for (int t = 0; t < kColRows; t++) {
+      i64 r = r0 + t;
+      i64 idx = (b * R + r) * C + c;
+      ev[t] = (r < R) ? e[idx] : SDPV_EZ;
+      tw[t] = (r < R) ? m[(i64)(L - 1) * plane + idx] : 0;
+    }
+#pragma unroll
+    for (int t = 0; t < kColRows; t++) {
+      if (ev[t] == SDPV_EZ) continue;
+      i64 top;
+      u32 x = (u32)tw[t] ^ (tw[t] < 0 ? 0xffffffffu : 0u);
+      if (x) top = ev[t] + 32 * (i64)(L - 1) + 32 - __clz(x);           // normalised data: top limb decides
+      else top = entry_top(m, plane, (b * R + r0 + t) * C + c, L, ev[t]);
+      best = top > best ? top : best;
+    }
+  }
+  red[ry][cx] = best;
+  __syncthreads();
+  if (ry == 0 && c < C) {
+#pragma unroll
+    for (int y = 1; y < 8; y++) best = red[y][cx] > best ? red[y][cx] : best;
+    if (best > SDPV_EZ) atomicMax((long long*)&out[b * C + c], (long long)best);
+  }
+}
+
+// Round-half-up shift of one entry whose limbs are read through `word(i)` (i in [0, L)).
+template <class Word>
+__device__ __forceinline__ void shift_entry(Word word, int L, i64 s, int Lout, int32_t* __restrict__ out, i64 ostride,
+                                            unsigned* err) {
+  i64 q = s >> 5;
+  int r = (int)(s - 32 * q);
+  u64 ext = ((int32_t)word(L - 1) < 0) ? 0xffffffffull : 0ull;
+  auto w = [&](i64 i) -> u64 { return i < 0 ? 0ull : (i >= L ? ext : (u64)word((int)i)); };
+  i64 sb = s - 1, qb = sb >> 5;
+  int rb = (int)(sb - 32 * qb);
+  u64 carry = (sb >= 0) ? ((w(qb) >> rb) & 1ull) : 0ull;
+  u64 lo = w(q), prev = 0;
+  for (int k = 0; k <= Lout; k++) {
+    u64 hi = w(q + k + 1);
+    u64 v = ((((hi << 32) | lo) >> r) & 0xffffffffull) + carry;
+    lo = hi;
+    carry = v >> 32;
+    v &= 0xffffffffull;
+    if (k < Lout) {
+      out[(i64)k * ostride] = (int32_t)(u32)v;
+      prev = v;
+    } else if (v != ((prev >> 31) ? 0xffffffffull : 0ull)) {
+      atomicOr(err, SDPV_ERRBIT_OVERFLOW);
+    }
+  }
+}
+
+// No transpose: thread per entry (b, r, c); reference exponent per row (per_col = 0) or column.
+__global__ void align_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e, int L, i64 nb, i64 R, i64 C,
+                             const i64* __restrict__ target, int per_col, int Lout, int32_t* __restrict__ out,
+                             unsigned* err) {
+  i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const i64 n = nb * R * C;
+  if (idx >= n) return;
+  i64 b = idx / (R * C), rc = idx - b * R * C, r = rc / C, c = rc - r * C;
+  i64 ev = e[idx];
+  i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
+  shift_entry([&](int i) { return (u32)__ldg(m + (i64)i * n + idx); }, L, s, Lout, out + idx, n, err);
+}
+
+// Transpose: tiles of 16 rows x 32 columns staged with all limbs; out is (Lout, nb, C, R).
+constexpr int TR = 16, TC = 32;
+__global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e,
+                                                           int L, i64 nb, i64 R, i64 C, const i64* __restrict__ target,
+                                                           int per_col, int Lout, int32_t* __restrict__ out,
+                                                           unsigned* err) {
+  extern __shared__ u32 sm[];                       // [L][TR][TC + 1] limbs, then [TR][TC] exponents
+  i64* se = reinterpret_cast<i64*>(sm + (size_t)L * TR * (TC + 1) + ((L * TR * (TC + 1)) & 1));
+  const i64 n = nb * R * C;
+  const i64 b = blockIdx.z;
+  const i64 r0 = (i64)blockIdx.x * TR, c0 = (i64)blockIdx.y * TC;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < L * TR * TC; t += kThreads) {       // all copies in flight at once
+    int l = t / (TR * TC), rr = (t / TC) % TR, cc = t % TC;
+    i64 r = r0 + rr, c = c0 + cc;
+    bool in = r < R && c < C;
+    cp_async4(&sm[(l * TR + rr) * (TC + 1) + cc], m + (in ? (i64)l * n + (b * R + r) * C + c : 0), in ? 4u : 0u);
+  }
+  cp_async_commit();
+  for (int t = tid; t < TR * TC; t += kThreads) {
+    int rr = t / TC, cc = t % TC;
+    i64 r = r0 + rr, c = c0 + cc;
+    se[t] = (r < R && c < C) ? e[(b * R + r) * C + c] : SDPV_EZ;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // thread -> (cc, rr) with rr fastest, so output stores (fast axis = r) are coalesced
+  for (int t = tid; t < TR * TC; t += kThreads) {
+    int rr = t % TR, cc = t / TR;
+    i64 r = r0 + rr, c = c0 + cc;
+    if (r >= R || c >= C) continue;
+    i64 ev = se[rr * TC + cc];
+    i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
+    const u32* base = sm + rr * (TC + 1) + cc;
+    shift_entry([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * R + r, n, err);
+  }
+}
+
+inline unsigned blocks(i64 n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+extern "C" int sdpv_top_max(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, int axis,
+                            int64_t* out, void* stream) {
+  if (L < 1 || nb < 0 || R < 0 || C < 0 || (axis != 0 && axis != 1)) return SDPV_EINVAL;
+  cudaStream_t st = sdpv::as_stream(stream);
+  if (axis == 1) {                                  // max over columns -> (nb, R)
+    i64 nrows = nb * R;
+    if (nrows == 0) return SDPV_OK;
+    if (C == 0) {
+      fill_kernel<<<blocks(nrows), kThreads, 0, st>>>(out, nrows, SDPV_EZ);
+    } else {
+      top_max_rows_kernel<<<blocks(nrows * 32), kThreads, 0, st>>>(m, e, L, nrows, C, out);
+    }
+    return sdpv::launch_status();
+  }
+  i64 ncols = nb * C;                               // max over rows -> (nb, C)
+  if (ncols == 0) return SDPV_OK;
+  fill_kernel<<<blocks(ncols), kThreads, 0, st>>>(out, ncols, SDPV_EZ);
+  if (R > 0) {
+    i64 ry = (R + 8 * kColRows - 1) / (8 * kColRows);
+    if (ry > 65535 || nb > 65535) return SDPV_EINVAL;
+    dim3 grid((unsigned)((C + 31) / 32), (unsigned)ry, (unsigned)nb);
+    top_max_cols_kernel<<<grid, kThreads, 0, st>>>(m, e, L, nb, R, C, out);
+  }
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
+                          const int64_t* target, int per_col, int transpose, int Lout, int32_t* out, void* stream) {
+  if (L < 1 || L > 64 || Lout < 1 || nb < 0 || R < 0 || C < 0 || nb > 65535) return SDPV_EINVAL;
+  i64 n = nb * R * C;
+  if (n == 0) return SDPV_OK;
+  cudaStream_t st = sdpv::as_stream(stream);
+  unsigned* err = sdpv::device_error_word();
+  if (!transpose) {
+    align_kernel<<<blocks(n), kThreads, 0, st>>>(m, e, L, nb, R, C, target, per_col, Lout, out, err);
+  } else {
+    size_t smem = (size_t)L * TR * (TC + 1) * 4 + 8 + TR * TC * 8;
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr[dev & 63]) {
+      cudaError_t ce = cudaFuncSetAttribute(align_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            64 * TR * (TC + 1) * 4 + 8 + TR * TC * 8);
+      if (ce != cudaSuccess) return sdpv::set_cuda_error(ce);
+      attr[dev & 63] = true;
+    }
+    dim3 grid((unsigned)((R + TR - 1) / TR), (unsigned)((C + TC - 1) / TC), (unsigned)nb);
+    if (grid.y > 65535 || (R + TR - 1) / TR > 0x7fffffff) return SDPV_EINVAL;
+    align_t_kernel<<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, target, per_col, Lout, out, err);
+  }
+  return sdpv::launch_status();
+}

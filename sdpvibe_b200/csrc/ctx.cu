@@ -120,7 +120,7 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
   d.E = E;
   d.W = E / 4;
   d.npad = (n + 127) / 128 * 128;
-  d.kt = (NB + 127) / 128;
+  d.kt = (NB + 2 + 127) / 128;   // limb bytes + a constant byte + a sign byte
   d.ktc = (n + 127) / 128;
   d.npad16 = (n + 31) / 32 * 32;
   d.Epad = (E + 127) / 128 * 128;
@@ -153,6 +153,18 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
     long c2 = powmod(2, 32L * L, m);
     vc1[g] = (int32_t)c1;
     vc1m2[g] = (int32_t)(c1 - c2);
+    // Column NB multiplies a constant byte 1 (adds C1), column NB+1 the sign byte (subtracts C2):
+    // the tensor-core product then is congruent to the entry itself.
+    long extra[2] = {c1 > m / 2 ? c1 - m : c1, (c2 == 0) ? 0 : ((m - c2) > m / 2 ? (m - c2) - m : (m - c2))};
+    for (int x = 0; x < 2; x++) {
+      long t = extra[x];
+      long lo = ((t + 64) % 128 + 128) % 128 - 64;
+      long hi = (t - lo) / 128;
+      int j = NB + x, kt = j / 128, col = j % 128;
+      u32 off = sw128_off(row, col / 16) + (col % 16);
+      tab[(((size_t)grp * 2 + 0) * d.kt + kt) * 128 * 128 + off] = (uint8_t)(int8_t)lo;
+      tab[(((size_t)grp * 2 + 1) * d.kt + kt) * 128 * 128 + off] = (uint8_t)(int8_t)hi;
+    }
     Big Mi = M;
     Mi.divmod_small((u32)m);
     vinv[g] = (int32_t)invmod(Mi.mod_small((u32)m), m);

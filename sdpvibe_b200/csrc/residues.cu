@@ -3,46 +3,58 @@
 // For an entry x with bytes u_j (j < 4L, little endian, two's complement) and a modulus m:
 //   x mod m = (sum_j (u_j - 128) T_j + C1 - neg*C2) mod m,  T_j = centred 256^j mod m = 128 Thi_j + Tlo_j
 // (sdpvibe/rns.py:66-103, tables rns.py:179-184).  The byte-by-table contraction runs on the tensor
-// cores as D = T * X^T with tcgen05.mma kind::i8: A = the table (128 moduli x 4L bytes, resident in
+// cores as D = T * X^T with tcgen05.mma kind::i8; two extra K columns (a constant byte 1 against C1
+// and the sign byte against -C2) make the product congruent to x itself, so the epilogue is only an
+// exact centred reduction and the int8 digit split.  A = the table (128 moduli x 4L+2 bytes, resident in
 // shared memory for the whole persistent CTA), B = 128 entries x 4L bytes staged from the limb
 // planes, D = two int32 accumulators (Tlo, Thi) of 128 x 128 in TMEM.  TMEM lane = modulus, so in the
 // epilogue each thread reduces one modulus for 32 consecutive entries and stores 32 contiguous
 // residue bytes per plane.  The next tile's limbs are loaded into registers while the current tile
-// is reduced, and two CTAs share each SM, so the kernel stays close to HBM speed.
+// is reduced, and several CTAs share each SM so their phases overlap.
+#include <cstdlib>
+#include <cstring>
+
 #include "common.cuh"
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kTile = 128;          // entries per tile (MMA N)
 constexpr u32 kTileBytes = 128 * 128;
 
-template <int KT>
+// TILE entries per MMA (N), THREADS per CTA; TMEM holds the two accumulators (2*TILE columns), so
+// 512 / (2*TILE) CTAs share an SM and overlap each other's load / MMA / reduce phases.
+constexpr int kStages = 3;          // raw limb tiles in flight per CTA
+
+template <int KT, int TILE>
 struct ResSmem {
   uint8_t tab_lo[KT][kTileBytes];   // A operand images (1024-aligned)
   uint8_t tab_hi[KT][kTileBytes];
-  uint8_t xb[KT][kTileBytes];       // B operand: entry bytes
-  uint8_t neg[kTile];
+  uint8_t xb[KT][TILE * 128];       // B operand: entry bytes (TILE rows of 128 bytes per K tile)
+  u32 raw[kStages][32 * KT - 1][TILE];  // limb planes of the next tiles, filled by cp.async
   u64 bar_tab, bar_mma;
   u32 tmem_slot;
   int abort;
 };
 
-template <int KT>
-__global__ void __launch_bounds__(kThreads, 2)
+template <int KT, int TILE, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
     residues_kernel(const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
-                    int group0, const uint8_t* __restrict__ tab, int ngroups_ctx, const int32_t* __restrict__ mods,
-                    const float* __restrict__ minvs, const int32_t* __restrict__ c1s,
-                    const int32_t* __restrict__ c1m2s, int n, int8_t* __restrict__ Rhi, int8_t* __restrict__ Rlo,
+                    int group0, const uint8_t* __restrict__ tab, const int32_t* __restrict__ mods,
+                    const float* __restrict__ minvs, int n, int8_t* __restrict__ Rhi, int8_t* __restrict__ Rlo, i64 pstride,
                     unsigned* __restrict__ err) {
+  constexpr int P = THREADS / TILE;                    // loader threads per entry
+  constexpr int W = THREADS / 32;
+  constexpr int COLS_PER_WARP = TILE * 4 / W;          // epilogue columns per warp (multiple of 32)
+  constexpr int kMaxChunks = 8 * KT;                   // 16-byte chunks per entry row
+  constexpr int kRegs = (kMaxChunks + P - 1) / P;
+  constexpr u32 TCOLS = 2 * TILE;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  ResSmem<KT>& S = *reinterpret_cast<ResSmem<KT>*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+  ResSmem<KT, TILE>& S =
+      *reinterpret_cast<ResSmem<KT, TILE>*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int grp = group0 + blockIdx.y;                 // 128-modulus group of the table
   const i64 nent = rows * kp;
-  const i64 ntiles = (nent + kTile - 1) / kTile;
+  const i64 ntiles = (nent + TILE - 1) / TILE;
   const i64 plane = rows * ld;
-  const int nchunks = (L + 3) / 4;                     // 16-byte chunks of an entry (4 limbs each)
 
   if (tid == 0) {
     mbar_init(&S.bar_tab, 1);
@@ -51,7 +63,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_fence_init();
   }
   if (warp == 0) {
-    tmem_alloc(&S.tmem_slot, 256);
+    tmem_alloc(&S.tmem_slot, TCOLS);
     tmem_relinquish();
   }
   __syncthreads();
@@ -64,70 +76,67 @@ __global__ void __launch_bounds__(kThreads, 2)
     bulk_load(&S.tab_hi[0][0], src + (size_t)KT * kTileBytes, KT * kTileBytes, &S.bar_tab);
   }
 
-  // Each thread stages chunks c = half, half+2, ... of entry `ent` (4 limbs = one 16-byte chunk).
-  const int ent = tid & (kTile - 1), half = tid >> 7;
-  constexpr int kMaxChunks = 8 * KT;                   // 16-byte chunks per entry row, split over two threads
-  uint4 regs[(kMaxChunks + 1) / 2];
-  int negbit = 0;
-  auto load_tile = [&](i64 tile) {
-    i64 e = tile * kTile + ent;
-    i64 i = e / kp, k = e - (e / kp) * kp;
-    bool ok = (e < nent) && (k < kc);
-    const int32_t* base = X + i * ld + k0 + k;
-    negbit = 0;
-#pragma unroll
-    for (int q = 0; q < (kMaxChunks + 1) / 2; q++) {
-      int c = half + 2 * q;
-      u32 w[4] = {0u, 0u, 0u, 0u};
-      if (c < nchunks && ok) {
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-          int l = 4 * c + t;
-          if (l < L) w[t] = (u32)__ldg(base + (i64)l * plane);
-        }
-      }
-      if (ok && c == (L - 1) / 4) negbit = (int)(w[(L - 1) & 3] >> 31);
-      regs[q] = make_uint4(w[0] ^ 0x80808080u, w[1] ^ 0x80808080u, w[2] ^ 0x80808080u, w[3] ^ 0x80808080u);
+  // Loader: the limb words of a tile land in raw[stage][limb][entry] by 4-byte cp.async (zero fill for
+  // entries past the end or in the k padding); the transform then packs entry rows of 16-byte chunks:
+  // limbs XOR 0x80808080 (signed bytes u - 128), word L = constant byte 1 | sign byte << 8, zeros after.
+  const int ent = tid % TILE, part = tid / TILE;
+  auto issue_tile = [&](i64 tile, int stage) {
+    if (tile < ntiles) {
+      i64 e = tile * TILE + ent;
+      i64 i = e / kp, k = e - (e / kp) * kp;
+      bool ok = (e < nent) && (k < kc);
+      const int32_t* base = X + (ok ? i * ld + k0 + k : 0);
+      for (int l = part; l < L; l += P) cp_async4(&S.raw[stage][l][ent], base + (ok ? (i64)l * plane : 0), ok ? 4u : 0u);
     }
+    cp_async_commit();
   };
-  auto store_tile = [&]() {
+  auto transform = [&](int stage) {
 #pragma unroll
-    for (int q = 0; q < (kMaxChunks + 1) / 2; q++) {
-      int c = half + 2 * q;
-      if (c < 8 * KT) {
-        int kt = c >> 3, cc = c & 7;
-        *reinterpret_cast<uint4*>(&S.xb[kt][sw128_off(ent, cc)]) = regs[q];
+    for (int q = 0; q < kRegs; q++) {
+      int c = part + P * q;
+      if (c >= kMaxChunks) continue;
+      u32 w[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        int l = 4 * c + t;
+        if (l < L) w[t] = S.raw[stage][l][ent] ^ 0x80808080u;
+        else if (l == L) w[t] = 1u | ((S.raw[stage][L - 1][ent] >> 31) << 8);
+        else w[t] = 0u;
       }
+      *reinterpret_cast<uint4*>(&S.xb[c >> 3][sw128_off(ent, c & 7)]) = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    if (half == (((L - 1) / 4) & 1)) S.neg[ent] = (uint8_t)negbit;
   };
 
-  // Per-thread modulus (TMEM lane) and column half for the epilogue.
-  const int quarter = warp & 3, colhalf = warp >> 2;
+  // Epilogue: TMEM lane = modulus of this 128-modulus group.
+  const int quarter = warp & 3, colgroup = warp >> 2;
   const int row = quarter * 32 + lane;
   const int g = grp * 128 + row;
   const bool gvalid = (g >= g0) && (g < g0 + G) && (g < n);
-  int m = 1, c1 = 0, c1m2 = 0;
+  int m = 1;
   float minv = 1.f;
   if (gvalid) {
     m = mods[g];
     minv = minvs[g];
-    c1 = c1s[g];
-    c1m2 = c1m2s[g];
   }
-  int8_t* outh = Rhi + (i64)(g - g0) * nent;
-  int8_t* outl = Rlo + (i64)(g - g0) * nent;
-  const u32 idesc = idesc_i8(128, kTile);
+  const int hm = m >> 1;
+  int8_t* outh = Rhi + (i64)(g - g0) * pstride;
+  int8_t* outl = Rlo + (i64)(g - g0) * pstride;
+  const u32 idesc = idesc_i8(128, TILE);
 
   i64 tile = blockIdx.x;
-  if (tile < ntiles) load_tile(tile);
+#pragma unroll
+  for (int st = 0; st < kStages; st++) issue_tile(tile + (i64)st * gridDim.x, st);
   if (!mbar_wait(&S.bar_tab, 0, err)) S.abort = 1;
   u32 phase = 0;
-  for (; tile < ntiles; tile += gridDim.x) {
-    store_tile();
+  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+    const int stage = it % kStages;
+    cp_async_wait<kStages - 1>();
+    __syncthreads();
+    transform(stage);
     fence_proxy_async_smem();
     __syncthreads();
     if (S.abort) break;
+    issue_tile(tile + (i64)kStages * gridDim.x, stage);   // refill the stage just consumed
     if (tid == 0) {
       tc_fence_after();
 #pragma unroll
@@ -137,38 +146,38 @@ __global__ void __launch_bounds__(kThreads, 2)
           u64 bd = sdesc_sw128(smem_u32(&S.xb[kt][0]) + 32 * s);
           u32 accum = (kt | s) ? 1u : 0u;
           mma_i8(tmem + 0, sdesc_sw128(smem_u32(&S.tab_lo[kt][0]) + 32 * s), bd, idesc, accum);
-          mma_i8(tmem + 128, sdesc_sw128(smem_u32(&S.tab_hi[kt][0]) + 32 * s), bd, idesc, accum);
+          mma_i8(tmem + TILE, sdesc_sw128(smem_u32(&S.tab_hi[kt][0]) + 32 * s), bd, idesc, accum);
         }
       mma_commit(&S.bar_mma);
     }
-    i64 next = tile + gridDim.x;
-    if (next < ntiles) load_tile(next);                // overlaps the MMA and the epilogue below
     if (!mbar_wait(&S.bar_mma, phase, err)) S.abort = 1;
     phase ^= 1;
     tc_fence_after();
 #pragma unroll 1
-    for (int c = 0; c < 2; c++) {
-      const int col = colhalf * 64 + c * 32;
+    for (int c = 0; c < COLS_PER_WARP / 32; c++) {
+      const int col = colgroup * COLS_PER_WARP + c * 32;
       u32 lo[32], hi[32];
       tmem_ld32(tmem + ((u32)(quarter * 32) << 16) + col, lo);
-      tmem_ld32(tmem + ((u32)(quarter * 32) << 16) + 128 + col, hi);
+      tmem_ld32(tmem + ((u32)(quarter * 32) << 16) + TILE + col, hi);
       tmem_ld_wait();
       if (!gvalid) continue;
-      const i64 e0 = tile * kTile + col;
+      const i64 e0 = tile * TILE + col;
       u32 ph[8], pl[8];
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        int v = 128 * (int)hi[j] + (int)lo[j] + (S.neg[col + j] ? c1m2 : c1);
-        int r = mod_exact(v, m, minv);
-        r -= (r > (m >> 1)) ? m : 0;
-        int l8 = ((r + 64) & 127) - 64;
-        int h8 = (r - l8) >> 7;
-        if ((j & 3) == 0) {
-          ph[j >> 2] = 0;
-          pl[j >> 2] = 0;
+      for (int j = 0; j < 32; j += 4) {
+        int hb[4], lb[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          int v = 128 * (int)hi[j + u] + (int)lo[j + u];                 // congruent to the entry mod m
+          float t = fmaf((float)v, minv, 12582912.0f);                     // round(v/m) in the low mantissa
+          int r = v - (__float_as_int(t) - 0x4B400000) * m;                // |r| <= m/2 + m/300
+          r -= (r > hm) ? m : 0;                                           // exact centring
+          r += (r < -hm) ? m : 0;
+          hb[u] = (r + 64) >> 7;                                           // r = 128 hi + lo, lo in [-64, 64)
+          lb[u] = r - (hb[u] << 7);
         }
-        ph[j >> 2] |= (u32)(h8 & 255) << (8 * (j & 3));
-        pl[j >> 2] |= (u32)(l8 & 255) << (8 * (j & 3));
+        ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
+        pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
       }
       if (e0 + 32 <= nent && ((((uintptr_t)(outh + e0)) | ((uintptr_t)(outl + e0))) & 15) == 0) {
         uint4* dh = reinterpret_cast<uint4*>(outh + e0);
@@ -193,7 +202,262 @@ __global__ void __launch_bounds__(kThreads, 2)
     mbar_wait(&S.bar_mma, phase, err);
   }
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, TCOLS);
+}
+
+// ---------------------------------------------------------------- warp-specialised persistent variant
+// One CTA per SM, 13 warps:
+//   warps 0-3  loaders: 4-byte cp.async of the next tiles' limb planes into a raw ring (kRawStages),
+//              then the transform into a double-buffered K-major entry tile (xb[2]);
+//   warp 4     MMA issuer (one lane): D_lo / D_hi of a 128-entry tile into one of two TMEM buffers;
+//   warps 5-12 reducers: TMEM lane quarter = warp % 4, 64 entries each; exact centred reduction,
+//              digit split and 32-byte stores.
+// mbarriers: xb_full (128 loader arrivals), xb_empty (MMA commit), tm_full (MMA commit),
+// tm_empty (256 reducer arrivals).  Every wait is bounded; a timeout aborts all roles.
+constexpr int WS_TILE = 128, WS_LOADERS = 128, WS_REDUCERS = 256;
+constexpr int WS_THREADS = WS_LOADERS + 32 + WS_REDUCERS;
+
+template <int KT, int RAW, int STG>
+struct WsSmem {
+  uint8_t tab_lo[KT][kTileBytes];
+  uint8_t tab_hi[KT][kTileBytes];
+  uint8_t xb[2][KT][WS_TILE * 128];
+  uint8_t out[STG][2][kTileBytes];      // residue tiles (128 moduli x 128 entries, hi | lo), 128-byte swizzle
+  u32 raw[RAW][32 * KT - 1][WS_TILE];
+  u64 bar_tab, xb_full[2], xb_empty[2], tm_full[2], tm_empty[2];
+  u32 tmem_slot;
+  volatile int abort;
+};
+
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+// Named barrier that also ORs a predicate over the participating threads (uniform decision).
+__device__ __forceinline__ bool named_sync_or(int id, int nthreads, bool pred) {
+  u32 out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((u32)pred), "r"(id), "r"(nthreads)
+      : "memory");
+  return out != 0;
+}
+
+template <int KT, int RAW, int STG>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+    residues_ws_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                       int use_tma, const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp,
+                       int g0, int G,
+                       int group0, const uint8_t* __restrict__ tab, const int32_t* __restrict__ mods,
+                       const float* __restrict__ minvs, int n, int8_t* __restrict__ Rhi, int8_t* __restrict__ Rlo, i64 pstride,
+                       unsigned* __restrict__ err) {
+  constexpr int kMaxChunks = 8 * KT;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  WsSmem<KT, RAW, STG>& S =
+      *reinterpret_cast<WsSmem<KT, RAW, STG>*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int grp = group0 + blockIdx.y;
+  const i64 nent = rows * kp;
+  const i64 ntiles = (nent + WS_TILE - 1) / WS_TILE;
+  const i64 plane = rows * ld;
+  const int niter = blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+
+  if (tid == 0) {
+    mbar_init(&S.bar_tab, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&S.xb_full[b], WS_LOADERS);
+      mbar_init(&S.xb_empty[b], 1);
+      mbar_init(&S.tm_full[b], 1);
+      mbar_init(&S.tm_empty[b], WS_REDUCERS);
+    }
+    S.abort = 0;
+    mbar_fence_init();
+  }
+  if (warp == 4) {
+    tmem_alloc(&S.tmem_slot, 512);
+    tmem_relinquish();
+  }
+  __syncthreads();
+  tc_fence_after();
+  const u32 tmem = S.tmem_slot;
+
+  if (warp < 4) {
+    // ------------------------------------------------ loaders
+    const int ent = tid;
+    auto issue = [&](int it) {
+      if (it < niter) {
+        i64 tile = blockIdx.x + (i64)it * gridDim.x;
+        i64 e = tile * WS_TILE + ent;
+        i64 i = e / kp, k = e - (e / kp) * kp;
+        bool ok = (e < nent) && (k < kc);
+        const int32_t* base = X + (ok ? i * ld + k0 + k : 0);
+        u32* dst = &S.raw[it % RAW][0][ent];
+        for (int l = 0; l < L; l++) cp_async4(dst + l * WS_TILE, base + (ok ? (i64)l * plane : 0), ok ? 4u : 0u);
+      }
+      cp_async_commit();
+    };
+    if (tid == 0) {
+      mbar_expect_tx(&S.bar_tab, 2 * KT * kTileBytes);
+      const uint8_t* src = tab + (size_t)grp * 2 * KT * kTileBytes;
+      bulk_load(&S.tab_lo[0][0], src, KT * kTileBytes, &S.bar_tab);
+      bulk_load(&S.tab_hi[0][0], src + (size_t)KT * kTileBytes, KT * kTileBytes, &S.bar_tab);
+    }
+    for (int it = 0; it < RAW - 1; it++) issue(it);
+    for (int it = 0; it < niter; it++) {
+      named_sync(1, WS_LOADERS);                 // everyone is done reading the raw stage refilled next
+      issue(it + RAW - 1);
+      cp_async_wait<RAW - 1>();
+      const int slot = it & 1;
+      bool fail = it >= 2 && !mbar_wait(&S.xb_empty[slot], ((it >> 1) - 1) & 1, err);
+      // tile it's words (from all loaders) have landed; the abort decision is uniform across loaders
+      if (named_sync_or(1, WS_LOADERS, fail || S.abort)) {
+        S.abort = 1;
+        break;
+      }
+      const u32* raw = &S.raw[it % RAW][0][0];
+#pragma unroll
+      for (int c = 0; c < kMaxChunks; c++) {
+        u32 w[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          int l = 4 * c + t;
+          if (l < L) w[t] = raw[l * WS_TILE + ent] ^ 0x80808080u;
+          else if (l == L) w[t] = 1u | ((raw[(L - 1) * WS_TILE + ent] >> 31) << 8);
+          else w[t] = 0u;
+        }
+        *reinterpret_cast<uint4*>(&S.xb[slot][c >> 3][sw128_off(ent, c & 7)]) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&S.xb_full[slot]);
+    }
+    cp_async_wait<0>();
+  } else if (warp == 4) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const u32 idesc = idesc_i8(128, WS_TILE);
+      if (!mbar_wait(&S.bar_tab, 0, err)) S.abort = 1;
+      int issued = 0;
+      for (int it = 0; it < niter && !S.abort; it++) {
+        const int b = it & 1;
+        if (!mbar_wait(&S.xb_full[b], (it >> 1) & 1, err)) { S.abort = 1; break; }
+        if (it >= 2 && !mbar_wait(&S.tm_empty[b], ((it >> 1) - 1) & 1, err)) { S.abort = 1; break; }
+        tc_fence_after();
+        const u32 d = tmem + (u32)b * 256;
+#pragma unroll
+        for (int kt = 0; kt < KT; kt++)
+#pragma unroll
+          for (int s = 0; s < 4; s++) {
+            u64 bd = sdesc_sw128(smem_u32(&S.xb[b][kt][0]) + 32 * s);
+            u32 accum = (kt | s) ? 1u : 0u;
+            mma_i8(d, sdesc_sw128(smem_u32(&S.tab_lo[kt][0]) + 32 * s), bd, idesc, accum);
+            mma_i8(d + WS_TILE, sdesc_sw128(smem_u32(&S.tab_hi[kt][0]) + 32 * s), bd, idesc, accum);
+          }
+        mma_commit(&S.xb_empty[b]);
+        mma_commit(&S.tm_full[b]);
+        issued = it + 1;
+      }
+      // on an abort, let the last committed products finish before TMEM is released (bounded)
+      if (S.abort && issued > 0) mbar_wait(&S.tm_full[(issued - 1) & 1], ((issued - 1) >> 1) & 1, err);
+    }
+  } else {
+    // ------------------------------------------------ reducers
+    const int quarter = warp & 3, half = (warp - 5) >> 2;
+    const int row = quarter * 32 + lane;
+    const int g = grp * 128 + row;
+    const bool gvalid = (g >= g0) && (g < g0 + G) && (g < n);
+    int m = 1;
+    float minv = 1.f;
+    if (gvalid) {
+      m = mods[g];
+      minv = minvs[g];
+    }
+    const int hm = m >> 1;
+    int8_t* outh = Rhi + (i64)(g - g0) * pstride;
+    int8_t* outl = Rlo + (i64)(g - g0) * pstride;
+    const bool elected = (tid == WS_LOADERS + 32);       // first reducer thread issues the bulk stores
+    for (int it = 0; it < niter; it++) {
+      const int b = it & 1, sb = it % STG;
+      bool fail = !mbar_wait(&S.tm_full[b], (it >> 1) & 1, err);
+      if (use_tma && elected) bulk_wait_read<STG - 1>();  // staging buffer sb no longer read by its store
+      // uniform across all reducers (they share named barriers and warp-collective TMEM loads)
+      if (named_sync_or(2, WS_REDUCERS, fail || S.abort)) {
+        S.abort = 1;
+        break;
+      }
+      tc_fence_after();
+      const i64 tile = blockIdx.x + (i64)it * gridDim.x;
+#pragma unroll 1
+      for (int c = 0; c < 2; c++) {
+        const int col = half * 64 + c * 32;
+        u32 lo[32], hi[32];
+        const u32 taddr = tmem + ((u32)(quarter * 32) << 16) + (u32)b * 256 + col;
+        tmem_ld32(taddr, lo);
+        tmem_ld32(taddr + WS_TILE, hi);
+        tmem_ld_wait();
+        u32 ph[8], pl[8];
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+          int hb[4], lb[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            int v = 128 * (int)hi[j + u] + (int)lo[j + u];
+            float t = fmaf((float)v, minv, 12582912.0f);
+            int r = v - (__float_as_int(t) - 0x4B400000) * m;
+            r -= (r > hm) ? m : 0;
+            r += (r < -hm) ? m : 0;
+            hb[u] = (r + 64) >> 7;
+            lb[u] = r - (hb[u] << 7);
+          }
+          ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
+          pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
+        }
+        if (use_tma) {
+          // row = modulus within the group, 16-byte chunks col/16 and col/16 + 1 (128-byte swizzle)
+          uint8_t* oh = &S.out[sb][0][0];
+          uint8_t* ol = &S.out[sb][1][0];
+          *reinterpret_cast<uint4*>(oh + sw128_off(row, col >> 4)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *reinterpret_cast<uint4*>(oh + sw128_off(row, (col >> 4) + 1)) = make_uint4(ph[4], ph[5], ph[6], ph[7]);
+          *reinterpret_cast<uint4*>(ol + sw128_off(row, col >> 4)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+          *reinterpret_cast<uint4*>(ol + sw128_off(row, (col >> 4) + 1)) = make_uint4(pl[4], pl[5], pl[6], pl[7]);
+          continue;
+        }
+        if (!gvalid) continue;
+        const i64 e0 = tile * WS_TILE + col;
+        if (e0 + 32 <= nent && ((((uintptr_t)(outh + e0)) | ((uintptr_t)(outl + e0))) & 15) == 0) {
+          uint4* dh = reinterpret_cast<uint4*>(outh + e0);
+          uint4* dl = reinterpret_cast<uint4*>(outl + e0);
+          dh[0] = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          dh[1] = make_uint4(ph[4], ph[5], ph[6], ph[7]);
+          dl[0] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+          dl[1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
+        } else {
+          for (int j = 0; j < 32 && e0 + j < nent; j++) {
+            outh[e0 + j] = (int8_t)(ph[j >> 2] >> (8 * (j & 3)));
+            outl[e0 + j] = (int8_t)(pl[j >> 2] >> (8 * (j & 3)));
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&S.tm_empty[b]);
+      if (use_tma) {
+        fence_proxy_async_smem();                          // staging writes visible to the bulk copy engine
+        named_sync(2, WS_REDUCERS);
+        if (elected) {
+          // moduli rows beyond g0 + G and entries beyond nent are clipped by the tensor bounds
+          const int y = grp * 128 - g0;
+          tma_store_2d(&map_hi, &S.out[sb][0][0], (int)(tile * WS_TILE), y);
+          tma_store_2d(&map_lo, &S.out[sb][1][0], (int)(tile * WS_TILE), y);
+          bulk_commit();
+        }
+      }
+    }
+    if (use_tma && elected) bulk_wait<0>();
+  }
+  __syncthreads();
+  if (warp == 4) tmem_dealloc(tmem, 512);
 }
 
 int num_sms() {
@@ -207,42 +471,116 @@ int num_sms() {
   return v;
 }
 
-template <int KT>
+template <int KT, int TILE, int THREADS>
 int launch_residues(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
-                    int8_t* Rhi, int8_t* Rlo, cudaStream_t st) {
+                    int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   const sdpv::CtxDev& d = c->d;
-  size_t smem = sizeof(ResSmem<KT>) + 1024;
-  if (smem < 80 * 1024) smem = 80 * 1024;               // at most two CTAs (2 x 256 TMEM columns) per SM
+  size_t smem = sizeof(ResSmem<KT, TILE>) + 1024;
+  int per_sm = 512 / (2 * TILE);                        // CTAs per SM allowed by TMEM ...
+  int by_smem = (int)((228 * 1024) / (smem + 1024));    // ... and by shared memory
+  if (by_smem < per_sm) per_sm = by_smem;
+  if (per_sm < 1) return SDPV_EINVAL;
+  size_t floor_smem = (228 * 1024) / (per_sm + 1) + 1024;   // keep a TMEM-starved extra CTA off the SM
+  if (smem < floor_smem) smem = floor_smem;
+  if (smem > 227 * 1024) return SDPV_EINVAL;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(residues_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(residues_kernel<KT, TILE, THREADS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return sdpv::set_cuda_error(e);
     attr_set[dev & 63] = true;
   }
   int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
-  i64 ntiles = (rows * kp + kTile - 1) / kTile;
-  i64 gx = 2 * (i64)num_sms();
+  i64 ntiles = (rows * kp + TILE - 1) / TILE;
+  i64 gx = per_sm * (i64)num_sms();
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
-  residues_kernel<KT><<<grid, kThreads, smem, st>>>(X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tab, d.npad / 128,
-                                                     d.mods, d.minv, d.c1, d.c1m2, d.n, Rhi, Rlo,
-                                                     sdpv::device_error_word());
+  residues_kernel<KT, TILE, THREADS><<<grid, THREADS, smem, st>>>(X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tab,
+                                                                   d.mods, d.minv, d.n, Rhi, Rlo, ps,
+                                                                   sdpv::device_error_word());
   return sdpv::launch_status();
+}
+
+// 2-D int8 map over one residue plane set: (nent entries, G moduli), plane stride ps, 128 x 128 boxes.
+bool res_store_map(CUtensorMap* map, void* base, i64 nent, i64 G, i64 ps) {
+  sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)nent, (cuuint64_t)G};
+  cuuint64_t strides[1] = {(cuuint64_t)ps};
+  cuuint32_t box[2] = {128, 128};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+template <int KT, int RAW, int STG>
+int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
+              int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
+  const sdpv::CtxDev& d = c->d;
+  size_t smem = sizeof(WsSmem<KT, RAW, STG>) + 1024;
+  if (smem > 227 * 1024) return SDPV_EINVAL;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return sdpv::set_cuda_error(e);
+    attr_set[dev & 63] = true;
+  }
+  const i64 nent = rows * kp;
+  // bulk tensor stores need 16-byte aligned planes and a box that starts at modulus row >= 0
+  CUtensorMap mh, ml;
+  int use_tma = (g0 % 128 == 0) && ((((uintptr_t)Rhi) | ((uintptr_t)Rlo)) & 15) == 0 && nent < (1ll << 31) &&
+                res_store_map(&mh, Rhi, nent, G, ps) && res_store_map(&ml, Rlo, nent, G, ps);
+  if (!use_tma) {
+    memset(&mh, 0, sizeof(mh));
+    memset(&ml, 0, sizeof(ml));
+  }
+  int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
+  i64 ntiles = (nent + WS_TILE - 1) / WS_TILE;
+  i64 gx = num_sms();
+  if (gx > ntiles) gx = ntiles;
+  dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
+  residues_ws_kernel<KT, RAW, STG><<<grid, WS_THREADS, smem, st>>>(mh, ml, use_tma, X, d.L, rows, ld, k0, kc, kp, g0,
+                                                                    G, grp0, d.tab, d.mods, d.minv, d.n, Rhi, Rlo,
+                                                                    ps, sdpv::device_error_word());
+  return sdpv::launch_status();
+}
+
+template <int KT>
+int launch_kt(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
+              int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
+  static int tile = [] {
+    // tuning override: "ws" (warp-specialised, default for L <= 63), 64 or 128 (phase-serial CTAs)
+    const char* v = getenv("SDPV_RES_TILE");
+    if (v && atoi(v) == 128) return 128;
+    if (v && atoi(v) == 64) return 64;
+    return 0;
+  }();
+  if (tile == 0 && KT == 1) return launch_ws<1, 3, 2>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 0 && KT == 2) return launch_ws<2, 2, 1>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 128) return launch_residues<KT, 128, 256>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  return launch_residues<KT, 64, 128>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
 }
 
 }  // namespace
 
 extern "C" int sdpv_residues(const sdpv_ctx* c, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc,
-                             int g0, int G, int8_t* Rhi, int8_t* Rlo, void* stream) {
+                             int g0, int G, int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream) {
   if (!c || rows < 0 || kc < 0 || k0 < 0 || k0 + kc > ld || g0 < 0 || G < 1 || g0 + G > c->d.n) return SDPV_EINVAL;
   i64 kp = (kc + 15) / 16 * 16;
+  i64 ps = plane_stride ? plane_stride : rows * kp;
+  if (ps < rows * kp || (ps & 15)) return SDPV_EINVAL;
   if (rows == 0 || kp == 0) return SDPV_OK;
   cudaStream_t st = sdpv::as_stream(stream);
   switch (c->d.kt) {
-    case 1: return launch_residues<1>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, st);
-    case 2: return launch_residues<2>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, st);
-    default: return SDPV_EINVAL;                        // L > 64
+    case 1: return launch_kt<1>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    case 2: return launch_kt<2>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    case 3: return launch_kt<3>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    default: return SDPV_EINVAL;                        // L > 94
   }
 }

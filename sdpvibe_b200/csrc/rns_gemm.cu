@@ -9,10 +9,14 @@
 //     out-of-range rows / K zero filled) into a 3-stage shared-memory ring;
 //   * warp 1 (one lane) issues per 32-byte K step two tcgen05.mma kind::i8 of M=128, N=256:
 //       TMEM[0:256)   += Ahi [Bhi; Blo]^T   -> hh | hl
-//       TMEM[256:512) += Alo [Bhi; Blo]^T   -> lh | ll
-//     (Bhi and Blo sit back to back in shared memory, so one descriptor covers both);
-//   * warps 2-5 read the four int32 products per entry from TMEM (one row per thread), reduce them
-//     modulo m exactly, add the old int16 residue and store it back.
+//       TMEM[128:384) += Alo [Bhi; Blo]^T   -> (hl + lh) | ll
+//     (Bhi and Blo sit back to back in shared memory, so one descriptor covers both; the second
+//     product overlaps the first by 128 columns so the two cross terms add up in TMEM -- on the
+//     first K step it is issued as two N=128 products so that only the overlap accumulates);
+//   * warps 2-9 (two per TMEM lane quarter, 64 columns each) read hh, hx = hl + lh and ll per entry
+//     from TMEM (one row per thread, old residues prefetched while the MMAs run), form
+//     (hh mod m) 2^14 + (hx mod m) 2^7 + ll + old (exact in int32 for K <= 65536) and store its
+//     canonical residue back, 16 bytes at a time where the row stride allows.
 // int32 accumulation is exact for K <= 65536 (|hh|, |hl + lh| <= K 2^14).
 // Syrk mode (Gram): B = A, only lower-triangle tiles are scheduled and only entries i >= j written.
 #include <mutex>
@@ -23,7 +27,7 @@ namespace {
 
 constexpr int kStages = 3;
 constexpr u32 kSlice = 128 * 128;            // one operand slice: 128 rows x 128 bytes
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue warps
 
 struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
@@ -47,7 +51,7 @@ __device__ __forceinline__ void tile_of(int t, int mode, int ntn, int& tm, int& 
 __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                    int16_t* __restrict__ acc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
+                    int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     unsigned* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -90,7 +94,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const u32 idesc = idesc_i8(128, 256);
+      const u32 idesc = idesc_i8(128, 256), idesc128 = idesc_i8(128, 128);
       bool ok = true;
       for (int kb = 0; kb < nk && ok; kb++) {
         int s = kb % kStages;
@@ -102,42 +106,79 @@ __global__ void __launch_bounds__(kThreads, 1)
         u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
 #pragma unroll
         for (int ks = 0; ks < 4; ks++) {
-          u32 accum = (kb | ks) ? 1u : 0u;
           u64 bd = sdesc_sw128(bh + 32 * ks);
-          mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, accum);
-          mma_i8(tmem + 256, sdesc_sw128(al + 32 * ks), bd, idesc, accum);
+          if ((kb | ks) == 0) {
+            mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                         // hh | hl
+            mma_i8(tmem + 256, sdesc_sw128(al), sdesc_sw128(bh + kSlice), idesc128, 0u);  // ll
+            mma_i8(tmem + 128, sdesc_sw128(al), bd, idesc128, 1u);                      // hl += lh
+          } else {
+            mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
+            mma_i8(tmem + 128, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+          }
         }
         mma_commit(&S.empty[s]);
       }
       mma_commit(&S.acc_full);
     }
   } else {
-    // Epilogue: warps 2..5 -> TMEM lane quarters 2, 3, 0, 1.
-    const int q = warp & 3;
+    // Epilogue: warps 2..9 -> TMEM lane quarter (warp & 3), column half (warp - 2) / 4.
+    const int q = warp & 3, ch = (warp - 2) >> 2;
     const i64 i = m0 + q * 32 + lane;                 // output row within the block
     const int gg = g0 + g;
     const int m = mods[gg], c14 = c14s[gg];
     const float minv = minvs[gg];
+    int16_t* rowp = acc + ((i64)gg * nb * M + (i64)b * M + i) * ldc;
+    const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
+    // the old residues do not depend on the products: load them before waiting for the MMAs
+    int16_t olds[2][32];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const i64 nc = n0 + 64 * ch + 32 * c;
+      const bool full = vec && i < M && nc + 32 <= N && (mode == 0 || nc + 31 <= i);
+      if (full) {
+#pragma unroll
+        for (int v4 = 0; v4 < 4; v4++)
+          *reinterpret_cast<uint4*>(olds[c] + 8 * v4) = reinterpret_cast<const uint4*>(rowp + nc)[v4];
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          olds[c][j] = (i < M && nc + j < N && (mode == 0 || nc + j <= i)) ? rowp[nc + j] : (int16_t)0;
+      }
+    }
     const bool ok = mbar_wait(&S.acc_full, 0, err);
     tc_fence_after();
-    int16_t* rowp = acc + ((i64)gg * nb * M + (i64)b * M + i) * N;
-#pragma unroll 1
-    for (int c = 0; c < 4; c++) {
-      u32 hh[32], hl[32], lh[32], ll[32];
-      u32 base = tmem + ((u32)(q * 32) << 16) + 32 * c;
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      u32 hh[32], hx[32], ll[32];
+      u32 base = tmem + ((u32)(q * 32) << 16) + 64 * ch + 32 * c;
       tmem_ld32(base, hh);
-      tmem_ld32(base + 128, hl);
-      tmem_ld32(base + 256, lh);
-      tmem_ld32(base + 384, ll);
+      tmem_ld32(base + 128, hx);
+      tmem_ld32(base + 256, ll);
       tmem_ld_wait();
       if (!ok || i >= M) continue;
+      const i64 nc = n0 + 64 * ch + 32 * c;
+      if (nc >= N) continue;
+      const bool full = vec && nc + 32 <= N && (mode == 0 || nc + 31 <= i);
+      int16_t* old = olds[c];
 #pragma unroll
       for (int j = 0; j < 32; j++) {
-        i64 n = n0 + 32 * c + j;
-        if (n >= N || (mode == 1 && n > i)) continue;
-        int v = mod_exact((int)hh[j], m, minv) * c14 + mod_exact((int)(hl[j] + lh[j]), m, minv) * 128 +
-                mod_exact((int)ll[j], m, minv) + (int)rowp[n];
-        rowp[n] = (int16_t)mod_exact(v, m, minv);
+        // (hh mod m) and (hx mod m) as |r| <= m/2 + m/300 representatives, then the canonical residue
+        int a = (int)hh[j], x = (int)hx[j];
+        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+        int v = ra * c14 + rx * 128 + (int)ll[j] + (int)old[j];
+        int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+        r += (r < 0) ? m : 0;
+        r -= (r >= m) ? m : 0;
+        old[j] = (int16_t)r;
+      }
+      if (full) {
+#pragma unroll
+        for (int v4 = 0; v4 < 4; v4++)
+          reinterpret_cast<uint4*>(rowp + nc)[v4] = *reinterpret_cast<const uint4*>(old + 8 * v4);
+      } else {
+        for (int j = 0; j < 32; j++)
+          if (nc + j < N && (mode == 0 || nc + j <= i)) rowp[nc + j] = old[j];
       }
     }
   }
@@ -146,30 +187,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) tmem_dealloc(tmem, 512);
 }
 
-// ---- host: tensor maps through the driver entry point (no libcuda link dependency)
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  });
-  return fn;
-}
-
-// 4-D int8 map over (K, rows, nb, G) with 128 x 128 boxes and 128-byte swizzle.
-bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G) {
-  EncodeTiledFn fn = encode_fn();
+// 4-D int8 map over (K, rows, nb, G) with 128 x 128 boxes and 128-byte swizzle; gstride = bytes between
+// the planes of consecutive moduli (>= K*rows*nb).
+bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G, i64 gstride) {
+  sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
   if (!fn) return false;
   cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nb, (cuuint64_t)G};
-  cuuint64_t strides[3] = {(cuuint64_t)K, (cuuint64_t)(K * rows), (cuuint64_t)(K * rows * nb)};
+  cuuint64_t strides[3] = {(cuuint64_t)K, (cuuint64_t)(K * rows), (cuuint64_t)gstride};
   cuuint32_t box[4] = {128, 128, 1, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
@@ -181,8 +205,8 @@ bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G
 }  // namespace
 
 extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t* Alo, const int8_t* Bhi,
-                             const int8_t* Blo, int16_t* acc, int g0, int G, int64_t nb, int64_t M, int64_t N,
-                             int64_t KC, int mode, void* stream) {
+                             const int8_t* Blo, int64_t a_stride, int64_t b_stride, int16_t* acc, int64_t ldc, int g0,
+                             int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream) {
   if (!c || g0 < 0 || G < 1 || g0 + G > c->d.n || nb < 1 || M < 0 || N < 0 || KC < 0 || KC > 65536 ||
       (KC & 15) || (mode != 0 && mode != 1) || nb > 65535 || G > 65535)
     return SDPV_EINVAL;
@@ -190,12 +214,17 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
     Bhi = Ahi;
     Blo = Alo;
     N = M;
+    b_stride = a_stride;
   }
+  if (!a_stride) a_stride = KC * M * nb;
+  if (!b_stride) b_stride = KC * N * nb;
+  if (a_stride < KC * M * nb || b_stride < KC * N * nb || (a_stride & 15) || (b_stride & 15)) return SDPV_EINVAL;
+  if (ldc < N) return SDPV_EINVAL;
   if (M == 0 || N == 0 || KC == 0) return SDPV_OK;
   if (((uintptr_t)Ahi | (uintptr_t)Alo | (uintptr_t)Bhi | (uintptr_t)Blo) & 15) return SDPV_EINVAL;
   CUtensorMap mAh, mAl, mBh, mBl;
-  if (!make_map(&mAh, Ahi, KC, M, nb, G) || !make_map(&mAl, Alo, KC, M, nb, G) ||
-      !make_map(&mBh, Bhi, KC, N, nb, G) || !make_map(&mBl, Blo, KC, N, nb, G))
+  if (!make_map(&mAh, Ahi, KC, M, nb, G, a_stride) || !make_map(&mAl, Alo, KC, M, nb, G, a_stride) ||
+      !make_map(&mBh, Bhi, KC, N, nb, G, b_stride) || !make_map(&mBl, Blo, KC, N, nb, G, b_stride))
     return SDPV_EINVAL;
   size_t smem = sizeof(GemmSmem) + 1024;
   static std::once_flag attr;
@@ -209,7 +238,7 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   if (tiles > 0x7fffffff) return SDPV_EINVAL;
   dim3 grid((unsigned)tiles, (unsigned)nb, (unsigned)G);
   rns_gemm_kernel<<<grid, kThreads, smem, sdpv::as_stream(stream)>>>(
-      mAh, mAl, mBh, mBl, acc, c->d.mods, c->d.minv, c->d.c14, g0, nb, M, N, KC, mode, ntn,
+      mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, nb, M, N, KC, mode, ntn,
       sdpv::device_error_word());
   return sdpv::launch_status();
 }

@@ -41,6 +41,7 @@ def main():
     ap.add_argument("--K", type=int, default=7000)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--packed", action="store_true", help="contiguous residue planes (no channel spreading)")
     a = ap.parse_args()
     dev = "cuda"
     rng = np.random.default_rng(0)
@@ -50,11 +51,11 @@ def main():
         X = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.N, a.K), dtype=np.int64)
                              .astype(np.int32)).to(dev)
         if a.kernel == "residues":
-            ts = _events(lambda: R.residues(X, 0, a.K), a.reps, a.warmup)
+            ts = _events(lambda: R.residues(X, 0, a.K, spread=not a.packed), a.reps, a.warmup)
             bytes_ = a.N * a.K * (4 * a.L + 2 * R.n)
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), gbs=bytes_ / (min(ts) * 1e-3) / 1e9)
         else:
-            Ah, Al = R.residues(X, 0, a.K)
+            Ah, Al = R.residues(X, 0, a.K, spread=not a.packed)
             if a.kernel == "syrk":
                 acc = torch.zeros((R.n, a.N, a.N), dtype=torch.int16, device=dev)
                 ts = _events(lambda: R.accumulate(Ah, Al, None, None, acc, syrk=True), a.reps, a.warmup)
@@ -62,7 +63,7 @@ def main():
             else:
                 Y = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.M, a.K), dtype=np.int64)
                                      .astype(np.int32)).to(dev)
-                Bh, Bl = R.residues(Y, 0, a.K)
+                Bh, Bl = R.residues(Y, 0, a.K, spread=not a.packed)
                 acc = torch.zeros((R.n, a.M, a.N), dtype=torch.int16, device=dev)
                 ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc), a.reps, a.warmup)
                 ops = R.n * 8 * a.M * a.N * a.K

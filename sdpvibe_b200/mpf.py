@@ -298,16 +298,47 @@ def trace(A):
 
 
 # ------------------------------------------------------------------ GEMM
+def _dims3(A):
+    """(nb, R, C) view sizes of a 2-D or 3-D MPF."""
+    sh = A.shape
+    return (1,) + tuple(sh) if len(sh) == 2 else tuple(sh)
+
+
+def top_max(A, over_rows):
+    """max of top = e + bitlen over the rows (over_rows=True -> per column, (nb, C)) or over the
+    columns (-> per row, (nb, R)) of a 2-D / 3-D MPF, in one kernel."""
+    nb, R, C = _dims3(A)
+    m, e = A.m.contiguous(), A.e.contiguous()
+    out = torch.empty((nb, C if over_rows else R), dtype=torch.int64, device=m.device)
+    _lib.call("sdpv_top_max", _lib.ptr(m), _lib.ptr(e), A.L, nb, R, C, 0 if over_rows else 1, _lib.ptr(out),
+              _lib.stream())
+    return out
+
+
+def aligned(A, target, per_col, transpose, Lout=None):
+    """Mantissas of A rounded to the exponents target (nb, R) per row or (nb, C) per column, as Lout
+    limbs, optionally transposed to (Lout, nb, C, R); zero entries give 0 (one kernel)."""
+    nb, R, C = _dims3(A)
+    Lout = Lout or A.L
+    m, e = A.m.contiguous(), A.e.contiguous()
+    out = torch.empty((Lout, nb, C, R) if transpose else (Lout, nb, R, C), dtype=torch.int32, device=m.device)
+    _lib.call("sdpv_align", _lib.ptr(m), _lib.ptr(e), A.L, nb, R, C, _lib.ptr(target.contiguous()), int(per_col),
+              int(transpose), Lout, _lib.ptr(out), _lib.stream())
+    return out
+
+
+def _row_exponents(tmax, L):
+    """mpf.py:394-395: common exponent max(top) - NB per row, 0 for all-zero rows."""
+    E = tmax - NBITS(L)
+    return torch.where(E < EZ // 2, torch.zeros_like(E), E)
+
+
 def _align_rows(A):
-    """A (..., R, K) -> (mantissas with a common exponent per row, row exponents (..., R))
-    (sdpvibe/mpf.py:390-398)"""
-    L = A.L
-    tp = _top(A)
-    E = tp.amax(-1) - NBITS(L)
-    E = torch.where(E < EZ // 2, torch.zeros_like(E), E)
-    s = (E[..., None] - A.e).reshape(-1)
-    s = torch.where(A.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
-    return shift_round(A.m.reshape(L, -1), s, L).view(A.m.shape), E
+    """A (..., R, K) -> (mantissas (L, ..., R, K) with a common exponent per row, row exps (..., R))
+    (sdpvibe/mpf.py:390-398)."""
+    E = _row_exponents(top_max(A, over_rows=False), A.L)
+    out = aligned(A, E, per_col=False, transpose=False)
+    return out.view(A.m.shape), E.view(A.shape[:-1])
 
 
 def gemm(A, B, transA=False, transB=False):
@@ -318,16 +349,19 @@ def gemm(A, B, transA=False, transB=False):
         B1 = MPF(B.m[:, None], B.e[None])
         C = gemm(A1, B1, transA, transB)
         return MPF(C.m[:, 0], C.e[0])
-    if transA:
-        A = A.T
-    if not transB:
-        B = B.T                                                     # B as (nb, N, K)
-    nb, M, K = A.shape
-    nb2, N, K2 = B.shape
-    assert K == K2 and nb == nb2, (A.shape, B.shape)
+    # op(A) rows and op(B) columns aligned to their own exponents; the transposes are fused into the
+    # alignment kernel (stored A is (nb, K, M) when transA; stored B is (nb, K, N) unless transB)
+    nb = A.shape[0]
+    M = A.shape[2] if transA else A.shape[1]
+    K = A.shape[1] if transA else A.shape[2]
+    N = B.shape[1] if transB else B.shape[2]
+    K2 = B.shape[2] if transB else B.shape[1]
+    assert K == K2 and B.shape[0] == nb, (A.shape, B.shape)
     L = A.L
-    Am, rA = _align_rows(A)                                         # (L, nb, M, K), (nb, M)
-    Bm, cB = _align_rows(B)                                         # (L, nb, N, K), (nb, N)
+    rA = _row_exponents(top_max(A, over_rows=transA), L)            # (nb, M)
+    Am = aligned(A, rA, per_col=transA, transpose=transA)          # (L, nb, M, K)
+    cB = _row_exponents(top_max(B, over_rows=not transB), L)        # (nb, N)
+    Bm = aligned(B, cB, per_col=not transB, transpose=not transB)  # (L, nb, N, K)
     R = ctx(L)
     acc = torch.zeros((R.n, nb * M, N), dtype=torch.int16, device=dev)
     if K:
@@ -362,7 +396,7 @@ class GramAcc:
     def add(self, P):
         """P: MPF (rows, N)."""
         L, N, R = self.L, self.N, self.R
-        tp = _top(P).amax(0)
+        tp = top_max(P, over_rows=True)[0]                           # column tops (mpf.py:563)
         live = tp > EZ // 2
         self.Tmax = torch.maximum(self.Tmax, tp)
         known = self.E > EZ // 2
@@ -371,14 +405,12 @@ class GramAcc:
             self.E = torch.where(live & (tp > self.E), tp, self.E)
             known = self.E > EZ // 2
         self.E = torch.where(live & ~known, tp, self.E)
-        PT = P.T                                                    # (N, rows) contiguous
-        rows = PT.shape[1]
-        s = ((self.E - NBITS(L))[:, None] - PT.e).reshape(-1)
-        s = torch.where(PT.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
-        X = shift_round(PT.m.reshape(L, -1), s, L + 1).view(L + 1, N, rows)
-        del PT, s
+        rows = P.shape[0]
+        # columns aligned to E_j - NB in L+1 limbs and transposed to (N, rows), one kernel
+        X = aligned(P, (self.E - NBITS(L))[None, :], per_col=True, transpose=True, Lout=L + 1).view(L + 1, N, rows)
         if self.acc is None:
-            self.acc = torch.zeros((R.n, N, N), dtype=torch.int16, device=dev)
+            # rows padded to a multiple of 8 entries (16 bytes) for the vectorised GEMM epilogue
+            self.acc = torch.zeros((R.n, N, -(-N // 8) * 8), dtype=torch.int16, device=dev)
         if rows:
             from .mpmat import residue_product
             residue_product(R, X, None, self.acc, syrk=True)
@@ -386,7 +418,7 @@ class GramAcc:
     def _crt(self):
         L, N, R = self.L, self.N, self.R
         rE = torch.where(self.E > EZ // 2, self.E - NBITS(L), torch.zeros_like(self.E))
-        Om, Oe = R.crt_norm(self.acc, N, 0, N, N, rE, rE[None, :], L)
+        Om, Oe = R.crt_norm(self.acc, self.acc.shape[2], 0, N, N, rE, rE[None, :], L)
         return MPF(Om.view(L, N, N), Oe.view(N, N))
 
     def _flush(self):

@@ -192,11 +192,11 @@ def residue_product(R, Av, Bv, acc, nb=1, syrk=False):
         kk = min(KC_MAX, K - k0)
         for g0 in range(0, R.n, GR):
             G = min(GR, R.n - g0)
-            Ah, Al = R.residues(Av, k0, kk, g0, G)
+            Ah, Al = R.residues(Av, k0, kk, g0, G, spread=True)
             if syrk:
                 R.accumulate(Ah, Al, None, None, acc, g0, nb=nb, syrk=True)
             else:
-                Bh, Bl = R.residues(Bv, k0, kk, g0, G)
+                Bh, Bl = R.residues(Bv, k0, kk, g0, G, spread=True)
                 R.accumulate(Ah, Al, Bh, Bl, acc, g0, nb=nb)
             del Ah, Al
 
@@ -224,7 +224,7 @@ def _same_product(R, X, acc):
     K = X.shape[2]
     for k0 in range(0, K, KC_MAX):
         kk = min(KC_MAX, K - k0)
-        Ah, Al = R.residues(X, k0, kk)
+        Ah, Al = R.residues(X, k0, kk, spread=True)
         R.accumulate(Ah, Al, Ah, Al, acc)
 
 

@@ -55,28 +55,43 @@ class RNS:
                 pass
 
     # ---- step 1: residues (sdpvibe/rns.py:196-214)
-    def residues(self, X, k0, kc, g0=0, G=None):
-        """X: (L, rows, K) int32 limb planes -> (Rhi, Rlo) (G, rows, kp) int8, kp = kc rounded up to 16."""
+    def residues(self, X, k0, kc, g0=0, G=None, spread=False):
+        """X: (L, rows, K) int32 limb planes -> (Rhi, Rlo) (G, rows, kp) int8, kp = kc rounded up to 16.
+        spread=True places the modulus planes an odd multiple of 2 KB apart (a strided view) so the
+        2G output streams spread over the HBM channels; accumulate() accepts either layout."""
         L, rows, K = X.shape
         assert L == self.L
         G = G or self.n
         kp = -(-kc // self.KPAD) * self.KPAD
         X = X.contiguous()
-        Rhi = torch.empty((G, rows, kp), dtype=torch.int8, device=X.device)
-        Rlo = torch.empty_like(Rhi)
-        _lib.call("sdpv_residues", self._h, _lib.ptr(X), rows, K, k0, kc, g0, G, _lib.ptr(Rhi), _lib.ptr(Rlo),
-                  _lib.stream())
+        if spread:
+            ps = plane_stride(rows * kp)
+            buf_h = torch.empty((G * ps,), dtype=torch.int8, device=X.device)
+            buf_l = torch.empty_like(buf_h)
+            Rhi = buf_h.as_strided((G, rows, kp), (ps, kp, 1))
+            Rlo = buf_l.as_strided((G, rows, kp), (ps, kp, 1))
+        else:
+            ps = 0
+            Rhi = torch.empty((G, rows, kp), dtype=torch.int8, device=X.device)
+            Rlo = torch.empty_like(Rhi)
+        _lib.call("sdpv_residues", self._h, _lib.ptr(X), rows, K, k0, kc, g0, G, _lib.ptr_strided(Rhi),
+                  _lib.ptr_strided(Rlo), ps, _lib.stream())
         return Rhi, Rlo
 
     # ---- step 2: accumulate residues of A @ Bt^T (sdpvibe/rns.py:217-224)
     def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False):
-        """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows."""
+        """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows.
+        acc may have padded rows (acc.shape[2] >= N): its row stride is passed to the kernel."""
         G, Mt, KC = Ahi.shape
         M = Mt // nb
         N = M if syrk else Bhi.shape[1] // nb
-        _lib.call("sdpv_rns_gemm", self._h, _lib.ptr(Ahi), _lib.ptr(Alo), _lib.ptr(Bhi if not syrk else Ahi),
-                  _lib.ptr(Blo if not syrk else Alo), _lib.ptr(acc), g0, G, nb, M, N, KC, 1 if syrk else 0,
-                  _lib.stream())
+        if syrk:
+            Bhi, Blo = Ahi, Alo
+        for t in (Ahi, Alo, Bhi, Blo):
+            assert t.stride(2) == 1 and t.stride(1) == KC, "residue planes must have packed rows"
+        _lib.call("sdpv_rns_gemm", self._h, _lib.ptr_strided(Ahi), _lib.ptr_strided(Alo), _lib.ptr_strided(Bhi),
+                  _lib.ptr_strided(Blo), Ahi.stride(0), Bhi.stride(0), _lib.ptr(acc), acc.stride(1), g0, G, nb, M, N,
+                  KC, 1 if syrk else 0, _lib.stream())
 
     # ---- step 3: CRT of a block of entries (sdpvibe/rns.py:227-245)
     def crt_block(self, acc, N, j0, w, rows):
@@ -99,6 +114,13 @@ class RNS:
                   _lib.ptr(rowexp.contiguous()), _lib.ptr(colexp.contiguous()), L, _lib.ptr(O), _lib.ptr(eO),
                   _lib.stream())
         return O, eO
+
+
+def plane_stride(nbytes):
+    """Bytes between residue planes of consecutive moduli: nbytes rounded up to an odd multiple of 2 KB,
+    so that planes of different moduli start on different HBM channels."""
+    q = -(-nbytes // 2048)
+    return 2048 * (q if q % 2 else q + 1)
 
 
 def gemm_config(M, N, K):

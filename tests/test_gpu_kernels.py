@@ -287,3 +287,92 @@ def test_gramacc_golden(sb, name):
     om, oe = _lower(np_(Q.m), np_(Q.e))
     assert np.array_equal(om, gm) and np.array_equal(oe, ge)
     assert acc.flushes == int(g["flushes"])
+
+
+# ------------------------------------------------------------------ operand alignment
+def _rand_mpf_np(rng, L, shape, lo=-40, hi=40, zero_frac=0.1):
+    n = int(np.prod(shape))
+    m = rng.integers(-(1 << 31), 1 << 31, size=(L, n), dtype=np.int64).astype(np.int32)
+    e = rng.integers(lo, hi + 1, size=n).astype(np.int64)
+    z = rng.random(n) < zero_frac
+    m[:, z] = 0
+    e[z] = O.EZ
+    m, e = O.mpf_norm(m, e, L)
+    e = np.where(z, O.EZ, e)
+    return m.reshape((L,) + shape), e.reshape(shape)
+
+
+@pytest.mark.parametrize("L,shape", [(26, (1, 300, 274)), (24, (3, 37, 50)), (27, (2, 16, 33))])
+def test_top_max_and_align(sb, L, shape):
+    from sdpvibe_b200.mpf import MPF, top_max, aligned
+    rng = np.random.default_rng(L + shape[1])
+    m, e = _rand_mpf_np(rng, L, shape)
+    A = MPF(cu(m), cu(e))
+    tp = OM.top(m, e)                                               # (nb, R, C)
+    for over_rows in (True, False):
+        ref = tp.max(axis=1 if over_rows else 2)
+        assert np.array_equal(np_(top_max(A, over_rows)), ref)
+    nb, R, C = shape
+    for per_col in (False, True):
+        target = rng.integers(-900, 900, size=(nb, C if per_col else R)).astype(np.int64)
+        tgt_full = target[:, None, :] if per_col else target[:, :, None]
+        s = np.where(e == O.EZ, 1 << 30, tgt_full - e).reshape(-1)
+        for Lout in (L, L + 1):
+            ref, _ = O.shift_round(m.reshape(L, -1), s, Lout)
+            ref = ref.reshape((Lout,) + shape)
+            for transpose in (False, True):
+                got = np_(aligned(A, cu(target), per_col, transpose, Lout))
+                want = np.swapaxes(ref, 2, 3) if transpose else ref
+                assert np.array_equal(got, want), (per_col, transpose, Lout)
+
+
+# ------------------------------------------------------------------ full-size configurations
+def _normal_mpf_np(rng, L, shape, lo, hi):
+    n = int(np.prod(shape))
+    m = rng.integers(0, 1 << 32, size=(L, n), dtype=np.uint64).astype(np.uint32)
+    m[L - 1] = (m[L - 1] & np.uint32((1 << 29) - 1)) | np.uint32(1 << 29)
+    neg = rng.random(n) < 0.5
+    m = m.view(np.int32).copy()
+    val, _ = O.mpf_norm(m, np.zeros(n, np.int64), L)                    # normalised positive mantissas
+    negm = O.add_same(np.zeros_like(val), val, -1)
+    m = np.where(neg[None, :], negm, val)
+    e = rng.integers(lo, hi + 1, size=n).astype(np.int64)
+    return m.reshape((L,) + shape), e.reshape(shape)
+
+
+def test_mpf_gemm_256_cube_L24(sb):
+    """The mp-GEMM configuration: 256 x 256 x 256 at 768 bits, exponents U[-4, 4], bit-exact."""
+    from sdpvibe_b200.mpf import MPF, gemm
+    rng = np.random.default_rng(0)
+    am, ae = _normal_mpf_np(rng, 24, (256, 256), -4, 4)
+    bm, be = _normal_mpf_np(rng, 24, (256, 256), -4, 4)
+    cm, ce = OM.mpf_gemm(am, ae, bm, be)
+    C = gemm(MPF(cu(am), cu(ae)), MPF(cu(bm), cu(be)))
+    assert np.array_equal(np_(C.m), cm) and np.array_equal(np_(C.e), ce)
+
+
+def test_gramacc_chunking_invariance_full_size(sb):
+    """The Gram configuration at full size (400 blocks, 274 columns, L = 26): with fixed reference
+    exponents the residue accumulation is exact, so 4 chunks, 2 chunks and 1 chunk give identical Q."""
+    from sdpvibe_b200.mpf import MPF, GramAcc, top_max
+    rng = np.random.default_rng(0)
+    rows = rng.integers(20, 121, size=400)
+    R = int(rows.sum())
+    m = torch.randint(-(1 << 31), (1 << 31) - 1, (26, R, 274), dtype=torch.int32, device="cuda")
+    m[-1] = (m[-1] & ((1 << 29) - 1)) | (1 << 29)
+    e = torch.randint(-8, 9, (R, 274), dtype=torch.int64, device="cuda")
+    P = MPF(m, e)
+    Eref = top_max(P, over_rows=True)[0] + 4
+    cuts = np.cumsum(rows)
+    results = []
+    for nch in (4, 2, 1):
+        bounds = [0] + [int(cuts[len(rows) * (c + 1) // nch - 1]) for c in range(nch)]
+        acc = GramAcc(274, 26, E_ref=Eref)
+        for a, b in zip(bounds[:-1], bounds[1:]):
+            acc.add(MPF(m[:, a:b].contiguous(), e[a:b].contiguous()))
+        Q = acc.result()
+        assert acc.flushes == 0
+        low = torch.tril(torch.ones(274, 274, dtype=torch.bool, device="cuda"))
+        results.append((torch.where(low, Q.m, 0), torch.where(low, Q.e, 0)))
+    for r in results[1:]:
+        assert torch.equal(r[0], results[0][0]) and torch.equal(r[1], results[0][1])
