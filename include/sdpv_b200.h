@@ -142,6 +142,18 @@ int sdpv_crt_norm(const sdpv_ctx* ctx, const int16_t* acc, int64_t ldg, int64_t 
                   int64_t rows, int64_t rows_per_block, const int64_t* rowexp, const int64_t* colexp, int L,
                   int32_t* O, int64_t* eO, void* stream);
 
+/* ---------------------------------------------------------------- Cholesky base case (e)
+ * Wide fixed point: a tile entry is WL 32-bit words (two's complement) with F = 32*LF fraction bits;
+ * tiles are entry-major (ntiles, 32, 32, WL); bt must be 32; WL <= 96.
+ * sdpv_chol_tiles: in-place lower Cholesky of each tile (upper part untouched) and the pivot reciprocals
+ * RINV (ntiles, 32, WL); a non-positive pivot sets SDPV_ERRBIT_NOTSPD in the device error word.
+ * Replaces chol_tiles (sdpvibe/basecase.py:158-193). */
+int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL, int LF, void* stream);
+/* X = L^-1 of lower tiles whose upper part is zero; S: caller workspace of the same size as X.
+ * Replaces trinv_tiles (sdpvibe/basecase.py:195-226). */
+int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
+                     int WL, int LF, void* stream);
+
 /* ---------------------------------------------------------------- errors
  * Read and clear the device error word (bits SDPV_ERRBIT_*) after synchronising `stream`.
  * Replaces limbops.check_errors (sdpvibe/limbops.py:156-169). */

@@ -8,6 +8,8 @@ Elementwise operations are libsdpv_b200 kernels with the reference's rounding (m
 renormalises each entry inside the CRT kernel (one launch for CRT + rounding).  ``GramAcc`` keeps
 Q = sum_c P_c^T P_c in residue form across chunks (lower-triangle tiles only) with one CRT at the end.
 """
+import os
+
 import mpmath as mp
 import numpy as np
 import torch
@@ -442,3 +444,90 @@ class GramAcc:
         q = self._crt()
         self.acc = None
         return q if self.part is None else add(self.part, q)
+
+
+# ------------------------------------------------------------------ Cholesky (equilibrated, batched)
+def fx_exp(L):
+    """exponent of the equilibrated fixed-point format (sdpvibe/linalg.py:19)"""
+    return -(32 * L - 40)
+
+
+class Chol:
+    """A = L L^T per block, with L = D^-1 Lt, D = diag(2^-k): Lt fixed point, k integer
+    (sdpvibe/mpf.py:461-532).  A: MPF (n, n) or batched (nb, n, n); padded internally to a multiple of
+    bt with the fixed-point identity."""
+
+    SOLVE_REFINE = int(os.environ.get("SDPB_GPU_SOLVE_REFINE", "0"))
+
+    def __init__(self, A, bt=32, refine=1):
+        from .batched import BMP, bchol
+        self.two_d = A.e.dim() == 2
+        if self.two_d:
+            A = MPF(A.m[:, None], A.e[None])
+        nb, n, _ = A.shape
+        L = A.L
+        self.nb, self.n, self.L, self.bt, self.refine = nb, n, L, bt, refine
+        idx = torch.arange(n, device=dev)
+        tpd = _top(A)[:, idx, idx]                                  # (nb, n)
+        if bool((A.m[-1][:, idx, idx] < 0).any()) or bool((tpd <= EZ // 2).any()):
+            raise ValueError("matrix is not positive definite (diagonal)")
+        k = torch.div(tpd + 1, 2, rounding_mode="floor")            # A_ii < 2^(2k)
+        self.k = k
+        npad = max(bt, (n + bt - 1) // bt * bt)
+        self.npad = npad
+        efx = fx_exp(L)
+        s = (efx - (A.e - k[:, :, None] - k[:, None, :])).reshape(-1)
+        s = torch.where(A.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
+        Af = shift_round(A.m.reshape(L, -1), s, L).view(L, nb, n, n)
+        P = torch.zeros((L, nb, npad, npad), dtype=torch.int32, device=dev)
+        P[:, :, :n, :n] = Af
+        if npad > n:
+            one = from_mp([1], L, (1,))
+            onefx = shift_round(one.m, torch.tensor([efx - int(one.e[0])], device=dev), L)[:, 0]
+            ii = torch.arange(n, npad, device=dev)
+            P[:, :, ii, ii] = onefx[:, None, None]
+        self.Lt, self.tiles = bchol(BMP(P, efx), bt, refine)
+
+    def _to_bmp(self, B):
+        from .batched import BMP
+        L = self.L
+        Bm, cE = _align_rows(B.T)                                   # per column of B: (L, nb, m, n)
+        P = torch.zeros((L, self.nb, self.npad, B.shape[-1]), dtype=torch.int32, device=dev)
+        P[:, :, :self.n] = Bm.transpose(2, 3)
+        return BMP(P, cE)
+
+    def _from_bmp(self, P):
+        L = self.L
+        m = P.shape[2]
+        X = P.limbs[:, :, :self.n].reshape(L, -1)
+        ein = P.expt()[:, None, :].expand(self.nb, self.n, m).reshape(-1)
+        return normalize(X.contiguous(), ein.contiguous(), L).reshape(self.nb, self.n, m)
+
+    def _io(self, B, f):
+        if self.two_d:
+            r = f(MPF(B.m[:, None], B.e[None]))
+            return MPF(r.m[:, 0], r.e[0])
+        return f(B)
+
+    def solve_lower(self, B):
+        """L^-1 B = Lt^-1 (D B)"""
+        from .batched import btrsm_left
+
+        def f(B):
+            P = btrsm_left(self.Lt, self._to_bmp(B.shift(-self.k[:, :, None])), self.tiles, self.bt,
+                           self.SOLVE_REFINE)
+            return self._from_bmp(P)
+        return self._io(B, f)
+
+    def solve_upper(self, B):
+        """L^-T B = D (Lt^-T B)"""
+        from .batched import btrsm_left_T
+
+        def f(B):
+            P = btrsm_left_T(self.Lt, self._to_bmp(B), self.tiles, self.bt, self.SOLVE_REFINE)
+            return self._from_bmp(P).shift(-self.k[:, :, None])
+        return self._io(B, f)
+
+    def solve(self, B):
+        """A^-1 B"""
+        return self.solve_upper(self.solve_lower(B))

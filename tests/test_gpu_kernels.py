@@ -376,3 +376,57 @@ def test_gramacc_chunking_invariance_full_size(sb):
         results.append((torch.where(low, Q.m, 0), torch.where(low, Q.e, 0)))
     for r in results[1:]:
         assert torch.equal(r[0], results[0][0]) and torch.equal(r[1], results[0][1])
+
+
+# ------------------------------------------------------------------ Cholesky / trsm (e)
+@pytest.mark.parametrize("name", golden_names("basecase_"))
+def test_basecase_tile_golden(sb, name):
+    from sdpvibe_b200.mpmat import MP
+    from sdpvibe_b200.basecase import chol_inv_tile
+    g = golden(name)
+    L = g["A"].shape[0]
+    Lg, Xg = chol_inv_tile(MP(cu(g["A"]), -(32 * L - 40)))
+    assert np.array_equal(np_(Lg.limbs), g["L"])
+    assert np.array_equal(np_(Xg.limbs), g["X"])
+    assert np.array_equal(np.broadcast_to(np_(Xg.exp), g["Xe"].shape), g["Xe"])
+
+
+@pytest.mark.parametrize("name", golden_names("chol_"))
+def test_chol_and_solves_golden(sb, name):
+    from sdpvibe_b200.mpf import MPF, Chol
+    g = golden(name)
+    ch = Chol(MPF(cu(g["Am"]), cu(g["Ae"])))
+    assert np.array_equal(np_(ch.k), g["k"])
+    assert np.array_equal(np_(ch.Lt.limbs), g["Lt"])
+    for i, t in enumerate(ch.tiles):
+        assert np.array_equal(np_(t.X.limbs), g[f"X{i}m"]) and np.array_equal(np_(t.X.exp), g[f"X{i}e"])
+    B = MPF(cu(g["Bm"]), cu(g["Be"]))
+    for key, fn in (("lo", ch.solve_lower), ("up", ch.solve_upper), ("x", ch.solve)):
+        R = fn(B)
+        assert np.array_equal(np_(R.m), g[f"{key}_m"]), key
+        assert np.array_equal(np_(R.e), g[f"{key}_e"]), key
+
+
+@pytest.mark.parametrize("L,nb,n,nr", [(24, 5, 96, 8), (26, 3, 160, 8), (24, 7, 17, 3)])
+def test_chol_random_vs_oracle(sb, L, nb, n, nr):
+    """Batched Cholesky + both solves on SPD blocks G G^T + n I (scaled rows), against the oracle."""
+    from sdpvibe_b200.mpf import MPF, Chol
+    rng = np.random.default_rng(n + nb)
+    vals, exps = [], []
+    for b in range(nb):
+        G = rng.integers(-40, 41, size=(n, n)).astype(object)
+        d = rng.integers(-20, 21, size=n)
+        A = G.dot(G.T) + np.eye(n, dtype=object) * (50 * n)
+        for i in range(n):
+            for j in range(n):
+                vals.append(int(A[i, j]))
+                exps.append(int(d[i] + d[j]))
+    m, e = O.mpf_norm(O.to_limbs(vals, L), np.array(exps, np.int64), L)
+    Am, Ae = m.reshape(L, nb, n, n), e.reshape(nb, n, n)
+    Bm, Be = _normal_mpf_np(rng, L, (nb, n, nr), -20, 20)
+    ref = OM.Chol(Am, Ae)
+    ch = Chol(MPF(cu(Am), cu(Ae)))
+    assert np.array_equal(np_(ch.Lt.limbs), ref.Lt)
+    B = MPF(cu(Bm), cu(Be))
+    for (rm, re_), got in ((ref.solve_lower(Bm, Be), ch.solve_lower(B)), (ref.solve(Bm, Be), ch.solve(B))):
+        assert np.array_equal(np_(got.m), rm) and np.array_equal(np_(got.e), re_)
