@@ -154,6 +154,18 @@ int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL,
 int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
                      int WL, int LF, void* stream);
 
+/* Allocation-free sdpv_trinv_tiles, for callers that cannot allocate device memory at the point of the call
+ * (their process has handed all device memory to another allocator, or the calling code must not allocate).
+ * No counterpart in the reference.  The product scratch is a fixed 16 MiB array inside the library image
+ * (4 Mi 32-bit words, reserved on every device that loads the library until exit), so the call allocates
+ * nothing: it needs ntiles * 32 * 32 * WL <= 4 Mi words and returns SDPV_EINVAL beyond that.  The first
+ * call on a device looks up the array's device address; make that first call before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU (different streams, no ordering)
+ * race on it.  Nothing in the array needs to start at zero; every word a call reads was written earlier
+ * in the same call. */
+int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, int64_t ntiles, int bt, int WL,
+                             int LF, void* stream);
+
 /* ---------------------------------------------------------------- errors
  * Read and clear the device error word (bits SDPV_ERRBIT_*) after synchronising `stream`.
  * Replaces limbops.check_errors (sdpvibe/limbops.py:156-169). */

@@ -13,6 +13,7 @@
 // One CTA (256 threads) per tile.  The Newton steps run warp-cooperatively (each lane forms product
 // columns, lane 0 carries); column scaling and the trailing update give one product to each thread.
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -293,5 +294,52 @@ extern "C" int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
   trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, S, WL, LF);
+  return sdpv::launch_status();
+}
+
+// ---------------------------------------------------------------- allocation-free variant of sdpv_trinv_tiles
+// Some callers cannot allocate device memory when they need the inverse: their process has already handed
+// all device memory to another allocator (a framework's caching pool or a fixed memory budget), or they
+// call from code that must not allocate.  This variant takes its product scratch from a fixed array that is
+// part of the library image: SDPV_TRINV_NOALLOC_WORDS 32-bit words (16 MiB), reserved on every device that
+// loads the library until the process exits.  A call needs ntiles * 32 * 32 * WL words of it.
+#define SDPV_TRINV_NOALLOC_WORDS (4u << 20)
+static __device__ __align__(256) uint32_t g_trinv_scratch[SDPV_TRINV_NOALLOC_WORDS];
+
+namespace {
+std::mutex g_scratch_mu;
+uint32_t* g_scratch_addr[64] = {};
+
+// Device address of g_trinv_scratch on the current device, looked up once per device.  Host code must
+// not pass the symbol itself to a kernel: on the host it names a stand-in, not device memory.
+int trinv_scratch_address(uint32_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return sdpv::set_cuda_error(e);
+  if (dev < 0 || dev >= 64) return SDPV_EINVAL;
+  std::lock_guard<std::mutex> g(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_trinv_scratch);
+    if (e != cudaSuccess) return sdpv::set_cuda_error(e);
+    g_scratch_addr[dev] = (uint32_t*)p;
+  }
+  *out = g_scratch_addr[dev];
+  return SDPV_OK;
+}
+}  // namespace
+
+extern "C" int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, int64_t ntiles,
+                                        int bt, int WL, int LF, void* stream) {
+  if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
+  if (ntiles == 0) return SDPV_OK;
+  if ((uint64_t)ntiles * BT * BT * (uint64_t)WL > SDPV_TRINV_NOALLOC_WORDS) {
+    sdpv::set_message("sdpv_trinv_tiles_noalloc: ntiles * 32 * 32 * WL exceeds the fixed scratch of 4 Mi words");
+    return SDPV_EINVAL;
+  }
+  uint32_t* scratch = nullptr;
+  int st = trinv_scratch_address(&scratch);
+  if (st != SDPV_OK) return st;
+  trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, scratch, WL, LF);
   return sdpv::launch_status();
 }

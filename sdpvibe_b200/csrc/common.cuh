@@ -16,6 +16,7 @@ typedef int64_t i64;
 namespace sdpv {
 
 int set_cuda_error(cudaError_t e);         // records the text, returns SDPV_ECUDA
+void set_message(const char* msg);         // records a diagnostic for sdpv_last_error
 unsigned* device_error_word();             // this device's error word (no allocation)
 inline int launch_status() {
   cudaError_t e = cudaGetLastError();

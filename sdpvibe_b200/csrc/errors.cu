@@ -22,6 +22,8 @@ int set_cuda_error(cudaError_t e) {
   return SDPV_ECUDA;
 }
 
+void set_message(const char* msg) { snprintf(g_last, sizeof(g_last), "%s", msg); }
+
 unsigned* device_error_word() {
   int dev = 0;
   cudaGetDevice(&dev);
