@@ -325,6 +325,118 @@ def run_b200(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ batched Cholesky + solve workload
+CS_BLOCKS, CS_NMIN, CS_NMAX, CS_NRHS, CS_L = 600, 8, 160, 8, 26
+
+
+def cholsolve_macs(ns):
+    ns = np.asarray(ns, dtype=np.float64)
+    return float((ns ** 3 / 6).sum() + (ns ** 2 * CS_NRHS).sum())
+
+
+def cholsolve_cpu_baseline(ns, threads, every=20):
+    """cpu_baseline/mpf_baseline.c (GMP mpf at 832 bits, OpenMP): Cholesky + trsm with 8 right-hand
+    sides per block, on every `every`-th block of the workload (trsm timed once, counted twice: lower and
+    upper solve), scaled to the whole workload by mp-MACs."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mpf_baseline")
+    if not os.path.exists(exe):
+        from oracle import ref_build
+        ref_build.build_cpu_baseline()
+    sample = [int(n) for n in ns[::every]]
+    t = 0.0
+    for n in sample:
+        out = subprocess.run([exe, "832", str(n), str(CS_NRHS), str(threads)], capture_output=True, text=True,
+                             timeout=600).stdout
+        for line in out.splitlines():
+            w = line.split()
+            if w and w[0] == "cholesky":
+                t += float(w[1])
+            elif w and w[0] == "trsm":
+                t += 2 * float(w[1])
+    t_all = t * cholsolve_macs(ns) / cholsolve_macs(sample)
+    return {"value": cholsolve_macs(ns) / t_all, "unit": "mp-MAC/s", "cores": threads, "kind": "reference",
+            "sample": f"mpf_baseline.c chol + 2 trsm (nrhs {CS_NRHS}) on {len(sample)} of {len(ns)} blocks "
+                      f"(every {every}th), scaled by mp-MACs", "s_per_step": t_all}
+
+
+def run_cholsolve(args, rank, world, local_rank):
+    """600 SPD blocks A = G G^T + n I (n ~ U[8,160], numpy seed 0, float64 values exact in MPF), L = 26,
+    8 right-hand sides: one batched Chol + solve per padded size (32..160), as the reference's callers
+    group blocks.  Metric: mp-MAC/s over the unpadded work sum n^3/6 + 2 * 8 n^2 / 2."""
+    import torch
+    from sdpvibe_b200 import mpf, _trace
+    from sdpvibe_b200.kernel_bench import cholsolve_inputs, cholsolve_buckets
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    cases = cholsolve_inputs(CS_BLOCKS, CS_NMIN, CS_NMAX, CS_NRHS)
+    ns = [c[0] for c in cases]
+    buckets = cholsolve_buckets(cases, CS_L)
+    pinned = [(A.m.cpu().pin_memory(), A.e.cpu().pin_memory(), B.m.cpu().pin_memory(), B.e.cpu().pin_memory())
+              for _, _, A, B in buckets]
+    outs = [(torch.empty(B.m.shape, dtype=torch.int32).pin_memory(), torch.empty(B.e.shape, dtype=torch.int64)
+             .pin_memory()) for _, _, _, B in buckets]
+    h2d = sum(sum(t.numel() * t.element_size() for t in p) for p in pinned)
+    d2h = sum(a.numel() * 4 + b.numel() * 8 for a, b in outs)
+
+    def step():
+        for _, _, A, B in buckets:
+            mpf.Chol(A).solve(B)
+
+    def step_e2e():
+        for (am, ae, bm, be), (om, oe) in zip(pinned, outs):
+            A = mpf.MPF(am.to(dev, non_blocking=True), ae.to(dev, non_blocking=True))
+            B = mpf.MPF(bm.to(dev, non_blocking=True), be.to(dev, non_blocking=True))
+            X = mpf.Chol(A).solve(B)
+            om.copy_(X.m, non_blocking=True)
+            oe.copy_(X.e, non_blocking=True)
+
+    def timed(fn, k, trace=None):
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        with (trace or _trace.Trace()):
+            for _ in range(k):
+                fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_norm",
+             "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
+    tr = _trace.Trace(timed=names)
+    with ClockSampler(local_rank) as clk:
+        ms = timed(step, args.steps, tr)
+    ms_e2e = timed(step_e2e, args.steps)
+    if rank != 0:
+        return
+    macs = cholsolve_macs(ns)
+    t_step = ms / args.steps * 1e-3
+    kms = {k: sum(tr.kernel_ms(k)) / args.steps for k in names if tr.launches[k]}
+    top = max(kms, key=kms.get)
+    line = {"metric": "batched Cholesky + solve, 600 SPD blocks n~U[8,160], 8 RHS, 832-bit MPF (mp-MAC/s)",
+            "value": world * macs / t_step, "unit": "mp-MAC/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 wide fixed point + int8 residue GEMM",
+            "data": "synthetic",
+            "config": {"workload": "cholsolve: 600 SPD blocks A = G G^T + n I, n~U[8,160] (numpy seed 0), "
+                                   "8 RHS U(-1,1), L=26, one Chol + solve per padded size",
+                       "buckets": {int(b[0]): len(b[1]) for b in buckets}, "limbs": CS_LIMBS_NOTE,
+                       "l2": "working set ~0.2 GB, no flush (latency bound)"},
+            "kernel_ms_per_step": kms, "top_kernel": top,
+            "e2e": {"value": world * macs / (ms_e2e / args.steps * 1e-3), "unit": "mp-MAC/s",
+                    "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": tr.total_launches // args.steps, "launches_by_entry": dict(tr.launches),
+            "clocks": clk.summary()}
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cholsolve_cpu_baseline(ns, os.cpu_count() or 1)
+    print(json.dumps(line), flush=True)
+
+
+CS_LIMBS_NOTE = "26 (832 bits); base tiles in WL = 50-word fixed point"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,6 +444,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", choices=("gram", "cholsolve"), default="gram",
+                    help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -345,7 +459,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_b200(args, rank, world, local_rank)
+        (run_cholsolve if args.workload == "cholsolve" else run_b200)(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -521,3 +521,15 @@ class Chol:
 
     def solve(self, Bm, Be):
         return self.solve_upper(*self.solve_lower(Bm, Be))
+
+
+def mpf_from_float(V, L):
+    """solver.py:1012-1018: float64 array -> MPF exactly (53-bit mantissa as two 32-bit limbs, then
+    mpf_norm).  Returns (m (L, *shape), e (*shape))."""
+    V = np.asarray(V, dtype=np.float64)
+    m, e = np.frexp(V)
+    mi = (m * 2.0 ** 53).astype(np.int64).reshape(-1)
+    w = np.stack([(mi & 0xFFFFFFFF).astype(np.uint32).view(np.int32), (mi >> 32).astype(np.int32)])
+    ein = np.where(mi != 0, e.reshape(-1).astype(np.int64) - 53, EZ)
+    om, oe = mpf_norm(w, ein, L)
+    return om.reshape(L, *V.shape), oe.reshape(V.shape)

@@ -1,7 +1,7 @@
 """Per-kernel timing of the multiprecision hot path on one GPU (CUDA events, after warm-up).
 
   python -m sdpvibe_b200.kernel_bench --kernel syrk --N 274 --K 7000 --L 27 --reps 20
-  kernels: residues | gemm | syrk | crt | mpfgemm
+  kernels: residues | gemm | syrk | crt | mpfgemm | cholsolve (batched Cholesky + solve over uneven blocks)
 
 Inputs are seeded random limb planes / residues of the given shape; rates are algorithmic (the
 reference's operation counts: moduli x 4 digit products x 2 ops per multiply-add; decomposition
@@ -29,12 +29,88 @@ def _events(fn, reps, warmup=3):
     return ts
 
 
+def cholsolve_inputs(blocks, nmin, nmax, nrhs, seed=0):
+    """SPD blocks A_b = G G^T + n I (G Gaussian, float64, numpy seed), n_b ~ U[nmin, nmax], with nrhs
+    right-hand sides U(-1, 1); all values exact float64.  Returns a list of (n, A, B) numpy arrays."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, size=blocks)
+    out = []
+    for n in ns:
+        G = rng.standard_normal((n, n))
+        A = G @ G.T + n * np.eye(n)
+        A = (A + A.T) / 2
+        out.append((int(n), A, rng.uniform(-1.0, 1.0, size=(n, nrhs))))
+    return out
+
+
+def cholsolve_buckets(cases, L, bt=32):
+    """group blocks by padded size (multiple of bt) as the reference's callers do (one batched Chol per
+    size): each block is padded with the identity, its right-hand sides with zero rows.
+    Returns [(npad, [block indices], A MPF (nb, npad, npad), B MPF (nb, npad, nrhs))]."""
+    from . import mpf
+    by = {}
+    for i, (n, _, _) in enumerate(cases):
+        by.setdefault(max(bt, -(-n // bt) * bt), []).append(i)
+    res = []
+    for npad in sorted(by):
+        idx = by[npad]
+        nrhs = cases[idx[0]][2].shape[1]
+        A = np.zeros((len(idx), npad, npad))
+        B = np.zeros((len(idx), npad, nrhs))
+        for q, i in enumerate(idx):
+            n, Ai, Bi = cases[i]
+            A[q] = np.eye(npad)
+            A[q, :n, :n] = Ai
+            B[q, :n] = Bi
+        res.append((npad, idx, mpf.from_float(A, L), mpf.from_float(B, L)))
+    return res
+
+
+def _cholsolve(a, rng):
+    """batched Cholesky + 2 triangular solves (nrhs right-hand sides) over uneven SPD blocks"""
+    from . import mpf, _trace
+    cases = cholsolve_inputs(a.blocks, a.nmin, a.nmax, a.nrhs)
+    buckets = cholsolve_buckets(cases, a.L)
+
+    def step():
+        for _, _, A, B in buckets:
+            ch = mpf.Chol(A)
+            ch.solve(B)
+
+    def chol_only():
+        for _, _, A, _ in buckets:
+            mpf.Chol(A)
+    ts = _events(step, a.reps, a.warmup)
+    tc = _events(chol_only, a.reps, a.warmup)
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_block",
+             "sdpv_crt_norm", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
+    with _trace.Trace(timed=names) as tr:
+        step()
+        torch.cuda.synchronize()
+    kms = {n: round(sum(tr.kernel_ms(n)), 3) for n in names if tr.launches[n]}
+    ns = np.array([c[0] for c in cases], dtype=np.float64)
+    mac_chol = float((ns ** 3 / 6).sum())
+    mac_solve = float((2 * ns ** 2 / 2 * a.nrhs).sum())
+    t = min(ts)
+    return dict(blocks=a.blocks, nrhs=a.nrhs, buckets={int(b[0]): len(b[1]) for b in buckets},
+                ms=t, ms_mean=float(np.mean(ts)), ms_chol=min(tc),
+                mp_mac_chol=mac_chol, mp_mac_solve=mac_solve,
+                mp_mac_per_s=(mac_chol + mac_solve) / (t * 1e-3),
+                launches=tr.total_launches, ms_per_launch=t / max(1, tr.total_launches),
+                launches_by_entry=dict(tr.launches), kernel_ms=kms)
+
+
 def main():
     from .mpmat import ctx
     from . import mpf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm"))
+    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve"))
+    ap.add_argument("--blocks", type=int, default=600, help="cholsolve: number of SPD blocks")
+    ap.add_argument("--nmin", type=int, default=8)
+    ap.add_argument("--nmax", type=int, default=160)
+    ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--L", type=int, default=27)
     ap.add_argument("--M", type=int, default=274)
     ap.add_argument("--N", type=int, default=274)
@@ -68,6 +144,8 @@ def main():
                 ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc), a.reps, a.warmup)
                 ops = R.n * 8 * a.M * a.N * a.K
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12)
+    elif a.kernel == "cholsolve":
+        out.update(_cholsolve(a, rng))
     elif a.kernel == "crt":
         m = torch.tensor(R.mods, dtype=torch.int64, device=dev)[:, None, None]
         acc = (torch.randint(0, 1 << 30, (R.n, a.M, a.N), device=dev) % m).to(torch.int16)

@@ -197,6 +197,17 @@ def from_mp(vals, L, shape=None):
 
 
 # ------------------------------------------------------------------ elementwise kernels
+def from_float(V, L):
+    """float64 array -> MPF, exactly: 53-bit mantissas as two 32-bit limbs, then normalised
+    (sdpvibe/solver.py:1012-1018)."""
+    V = np.asarray(V, dtype=np.float64)
+    m, e = np.frexp(V)
+    mi = (m * 2.0 ** 53).astype(np.int64).reshape(-1)
+    w = np.stack([(mi & 0xFFFFFFFF).astype(np.uint32).view(np.int32), (mi >> 32).astype(np.int32)])
+    ein = np.where(mi != 0, e.reshape(-1).astype(np.int64) - 53, EZ)
+    return normalize(torch.from_numpy(w).to(dev), torch.from_numpy(ein).to(dev), L).reshape(*V.shape)
+
+
 def normalize(Xw, ein, L):
     """Xw: (LI, n) int32 wide two's complement, ein (n,) -> normalised MPF (n,) (sdpvibe/mpf.py:307-313)"""
     LI, n = Xw.shape

@@ -430,3 +430,32 @@ def test_chol_random_vs_oracle(sb, L, nb, n, nr):
     B = MPF(cu(Bm), cu(Be))
     for (rm, re_), got in ((ref.solve_lower(Bm, Be), ch.solve_lower(B)), (ref.solve(Bm, Be), ch.solve(B))):
         assert np.array_equal(np_(got.m), rm) and np.array_equal(np_(got.e), re_)
+
+
+def test_from_float_matches_oracle(sb):
+    from sdpvibe_b200.mpf import from_float
+    rs = np.random.default_rng(7)
+    V = rs.standard_normal((3, 5, 5)) * 2.0 ** np.random.default_rng(8).integers(-900, 900, (3, 5, 5))
+    V[0, 0, 0] = 0
+    for L in (2, 26, 40):
+        got = from_float(V, L)
+        rm, re_ = OM.mpf_from_float(V, L)
+        assert np.array_equal(np_(got.m), rm) and np.array_equal(np_(got.e), re_)
+
+
+def test_cholsolve_buckets_vs_oracle(sb):
+    """The batched Cholesky + solve workload (SPD blocks of uneven size grouped by padded size, identity
+    padding) on a few blocks, bit-exact against the oracle per bucket."""
+    from sdpvibe_b200 import mpf
+    from sdpvibe_b200.kernel_bench import cholsolve_inputs, cholsolve_buckets
+    cases = cholsolve_inputs(6, 8, 70, 8, seed=3)
+    for npad, idx, A, B in cholsolve_buckets(cases, 26):
+        X = mpf.Chol(A).solve(B)
+        ref = OM.Chol(np_(A.m), np_(A.e))
+        rm, re_ = ref.solve(np_(B.m), np_(B.e))
+        assert np.array_equal(np_(X.m), rm) and np.array_equal(np_(X.e), re_), npad
+        # the solution solves the float64 system to double accuracy
+        for q, i in enumerate(idx):
+            n, Ai, Bi = cases[i]
+            xf = mpf.MPF(X.m[:, q, :n], X.e[q, :n]).to_float()
+            assert np.allclose(Ai @ xf, Bi, rtol=0, atol=1e-9)
