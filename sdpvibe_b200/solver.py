@@ -239,3 +239,504 @@ def min_eig(chols, dMs, lam=None, gamma=None, stats=None):
 
 def step_length(chols, dMs, gamma):
     return step_from_eig(min_eig(chols, dMs), gamma)
+
+
+# ------------------------------------------------------------------ SDP input (sdpvibe/solver.py:399-521)
+class Group:
+    """one chunk of blocks of equal dim, zero-padded to common K (points) and h (bilinear basis size)"""
+
+
+def _chunks_by_dim(blocks):
+    """single-GPU resident plan: one chunk per dim, blocks ordered by (K, max(he, ho)) inside it
+    (sdpvibe/solver.py:277-279, the unchunked branch of Layout)"""
+    bydim = {}
+    for j, b in enumerate(blocks):
+        bydim.setdefault(b["dim"], []).append(j)
+    for d in bydim:
+        bydim[d].sort(key=lambda j: (blocks[j]["K"], max(blocks[j]["he"], blocks[j]["ho"])))
+    return [bydim[d] for d in sorted(bydim)]
+
+
+def _host_mpf(H, L):
+    """host data of one MPF array -> device MPF.  H is (limbs (L, *shape) int32, exps (*shape) int64)
+    of normalised entries, a float64 numpy array (converted exactly) or already an MPF."""
+    if isinstance(H, MPF):
+        return H
+    if isinstance(H, np.ndarray):
+        return F.from_float(H, L)
+    m, e = H
+    return MPF(torch.from_numpy(np.ascontiguousarray(m)).to(dev), torch.from_numpy(np.ascontiguousarray(e)).to(dev))
+
+
+def _shape(H):
+    if isinstance(H, (MPF, np.ndarray)):
+        return H.shape
+    return H[1].shape
+
+
+def _rand_host_mpf(rng, shape, L, spread=4):
+    """random normalised MPF host data: |mantissa| of exactly 32L-2 bits, random sign, |value| in
+    [2^u, 2^(u+1)) with u ~ U[-spread, spread] (numpy generator)"""
+    n = int(np.prod(shape))
+    mag = rng.integers(0, 1 << 32, size=(L, n), dtype=np.uint64).astype(np.uint32)
+    mag[L - 1] = (mag[L - 1] & np.uint32((1 << 29) - 1)) | np.uint32(1 << 29)
+    neg = rng.random(n) < 0.5
+    m = mag.copy()
+    m[:, neg] = ~m[:, neg]
+    carry = neg.copy()
+    for k in range(L):                                     # two's complement: +1 with carry
+        v = m[k].astype(np.uint64) + carry
+        m[k] = v.astype(np.uint32)
+        carry = carry & (v > 0xffffffff)
+    e = rng.integers(-spread, spread + 1, size=n).astype(np.int64) - (32 * L - 3)
+    return m.view(np.int32).reshape(L, *shape), e.reshape(shape)
+
+
+class SDP:
+    """SDP in SDPB's block form, batched by dim (one chunk per dim, every array resident on the GPU).
+
+    Block j: dim, K points, even / odd bilinear bases V_e (he, K), V_o (ho, K), c_j (K npair, 1),
+    B_j (K npair, N) with npair = dim (dim + 1) / 2; then b (N, 1) and const.  Arrays are MPF, host MPF
+    data (limbs, exps) or float64 numpy arrays (exact)."""
+
+    def __init__(self, blocks, b, const, L):
+        """blocks: [dict(dim, K, Ve, Vo, c, B)] (Ve / Vo None for an empty basis)"""
+        mp.mp.prec = F.NBITS(L) + 64
+        shapes = []
+        for bl in blocks:
+            he = 0 if bl.get("Ve") is None else _shape(bl["Ve"])[0]
+            ho = 0 if bl.get("Vo") is None else _shape(bl["Vo"])[0]
+            shapes.append(dict(dim=bl["dim"], K=bl["K"], he=he, ho=ho))
+        self._build(shapes, lambda j: (blocks[j].get("Ve"), blocks[j].get("Vo"), blocks[j]["c"], blocks[j]["B"]),
+                    _host_mpf(b, L), mp.mpf(const), L)
+
+    @classmethod
+    def synthetic(cls, blocks, N, L, seed=0):
+        """random SDP with the given block shapes [dict(dim, K, he, ho)] (benchmarks)"""
+        self = cls.__new__(cls)
+        mp.mp.prec = F.NBITS(L) + 64
+        rng = np.random.default_rng(seed)
+        b = _rand_host_mpf(rng, (N, 1), L)
+        data = []
+        for bl in blocks:
+            npair = bl["dim"] * (bl["dim"] + 1) // 2
+            data.append((_rand_host_mpf(rng, (bl["he"], bl["K"]), L) if bl["he"] else None,
+                         _rand_host_mpf(rng, (bl["ho"], bl["K"]), L) if bl["ho"] else None,
+                         _rand_host_mpf(rng, (bl["K"] * npair, 1), L), _rand_host_mpf(rng, (bl["K"] * npair, N), L)))
+        self._build(blocks, lambda j: data[j], _host_mpf(b, L), mp.mpf(0), L)
+        return self
+
+    def _build(self, blocks, data, b, const, L):
+        self.const, self.b, self.N, self.L = const, b, b.shape[0], L
+        N = self.N
+        self.groups = []
+        for c in _chunks_by_dim(blocks):
+            g = Group()
+            nb, dim = len(c), blocks[c[0]]["dim"]
+            K = max(blocks[j]["K"] for j in c)
+            h = max(max(blocks[j]["he"], blocks[j]["ho"]) for j in c)
+            npair = dim * (dim + 1) // 2
+            P = K * npair
+            g.idx, g.nb, g.dim, g.K, g.h, g.nbp, g.P = list(c), nb, dim, K, [h], 2 * nb, P
+            g.psd_rows = sum(blocks[j]["dim"] * (blocks[j]["he"] + blocks[j]["ho"]) for j in c)
+            V = F.zeros((2 * nb, h, K), L)
+            xm = torch.zeros((2 * nb, dim * h), dtype=torch.bool, device=dev)
+            g.c = F.zeros((nb, P, 1), L)
+            B = F.zeros((nb, P, N), L)
+            g.xmask = torch.zeros((nb, P), dtype=torch.bool, device=dev)
+            for q, j in enumerate(c):
+                Kj = blocks[j]["K"]
+                Ve, Vo, cj, Bj = data(j)
+                for par, v in enumerate((Ve, Vo)):
+                    z = par * nb + q
+                    hj = 0
+                    if v is not None:
+                        v = _host_mpf(v, L)
+                        hj = v.shape[0]
+                        V.m[:, z, :hj, :Kj] = v.m
+                        V.e[z, :hj, :Kj] = v.e
+                    for cc in range(dim):
+                        xm[z, cc * h:cc * h + hj] = True
+                cj, Bj = _host_mpf(cj, L), _host_mpf(Bj, L)
+                for s in range(npair):                      # pair segment s: Kj points -> K slots
+                    rows = slice(s * Kj, (s + 1) * Kj)
+                    g.c.m[:, q, s * K:s * K + Kj] = cj.m[:, rows]
+                    g.c.e[q, s * K:s * K + Kj] = cj.e[rows]
+                    B.m[:, q, s * K:s * K + Kj] = Bj.m[:, rows]
+                    B.e[q, s * K:s * K + Kj] = Bj.e[rows]
+                    g.xmask[q, s * K:s * K + Kj] = True
+            Vx = F.zeros((2 * nb, dim * h, dim * K), L)
+            for cc in range(dim):
+                put(Vx, cc * h, cc * K, V)
+            g.Xmask = [xm]
+            g.B = B
+            g.V = dict(V=[V], Vx=[Vx])
+            assert g.psd_rows == int(xm.sum())
+            self.groups.append(g)
+        self.total_psd_rows = sum(g.psd_rows for g in self.groups)
+        self.nblocks = len(blocks)
+
+
+# ------------------------------------------------------------------ solver (sdpvibe/solver.py:524-982)
+DEFAULTS = dict(maxIterations=500, findPrimalFeasible=False, findDualFeasible=False,
+                detectPrimalFeasibleJump=False, detectDualFeasibleJump=False,
+                dualityGapThreshold="1e-30", primalErrorThreshold="1e-30", dualErrorThreshold="1e-30",
+                initialMatrixScalePrimal="1e20", initialMatrixScaleDual="1e20",
+                feasibleCenteringParameter="0.1", infeasibleCenteringParameter="0.3",
+                stepLengthReduction="0.7", maxComplementarity="1e100", minPrimalStep="0", minDualStep="0")
+
+
+def fmt_big(v, digits):
+    """a number printed the way SDPB prints a BigFloat: C++ defaultfloat (%g style) with `digits`
+    significant digits and an exponent of at least two digits with its sign (sdpvibe/solver.py:533-546)"""
+    v = mp.mpf(v)
+    if v == 0:
+        return "0"
+    txt = mp.nstr(v, digits, min_fixed=-5, max_fixed=digits, strip_zeros=True)
+    mant, _, ex = txt.partition("e")
+    if mant.endswith(".0"):
+        mant = mant[:-2]
+    if not ex:
+        return mant
+    sign = "-" if ex.startswith("-") else "+"
+    ex = ex.lstrip("+-").lstrip("0") or "0"
+    return f"{mant}e{sign}{ex.zfill(2)}"
+
+
+def chol_log2_cond(ch, mask=None):
+    """per block log2 of SDPB's Cholesky condition estimate (max / min diagonal of L)^2, over the rows
+    where mask (nb, n) is True (sdpvibe/solver.py:563-576)"""
+    L = ch.L
+    i = torch.arange(ch.n, device=dev)
+    d = ch.Lt.limbs[:, :, i, i]
+    top = d[-1].double() * 2.0 ** 32 + (d[-2].double() % 2.0 ** 32) if L > 1 else d[-1].double()
+    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.Lt.exp + 32 * (L - 2)) + ch.k.double()
+    if mask is None:
+        mask = torch.ones_like(lg, dtype=torch.bool)
+    hi = torch.where(mask, lg, torch.full_like(lg, -1e300)).amax(1)
+    lo = torch.where(mask, lg, torch.full_like(lg, 1e300)).amin(1)
+    return torch.where(mask.any(1), 2 * (hi - lo), torch.zeros_like(hi))
+
+
+class PhaseTimer:
+    """per-phase device time of Solver.run: CUDA events on the current stream, read after the run"""
+
+    def __init__(self, on):
+        self.on, self.marks = on, []
+
+    def __call__(self, name):
+        if not self.on:
+            return
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        self.marks.append((name, ev))
+
+    def totals(self):
+        if not self.on or len(self.marks) < 2:
+            return {}
+        torch.cuda.synchronize()
+        out = {}
+        for (name, a), (_, b) in zip(self.marks, self.marks[1:]):
+            out[name] = out.get(name, 0.0) + a.elapsed_time(b) * 1e-3
+        return out
+
+
+class Solver:
+    """SDPB's Mehrotra predictor-corrector iteration (sdpvibe/solver.py:579-982) on one GPU with every
+    chunk resident.  Per chunk the iteration keeps x, X, Y, their Cholesky factors, the residues, the
+    pairings, the Schur complement factor and P = L_S^-1 B; y, b and Q are global."""
+
+    def __init__(self, sdp, L, precision=None, timing=False, **params):
+        self.sdp, self.L = sdp, L
+        mp.mp.prec = F.NBITS(L) + 64
+        self.precision = precision or (32 * (L - 1) - 2)
+        self.digits = int(mp.ceil(self.precision * mp.log10(2))) + 1      # SDPB's stream precision
+        p = dict(DEFAULTS)
+        p.update(params)
+        self.p = {k: (mp.mpf(v) if isinstance(v, str) else v) for k, v in p.items()}
+        self.S = lambda v: F.scalar(v, L)
+        self.st = []
+        for g in sdp.groups:
+            I = bexpand(F.eye(g.dim * g.h[0], L, 1), g.nbp)
+            X = [set_diag_where(I, self.S(self.p["initialMatrixScalePrimal"]), g.Xmask[0])]
+            Y = [set_diag_where(I, self.S(self.p["initialMatrixScaleDual"]), g.Xmask[0])]
+            self.st.append(dict(xs=dict(x=F.zeros((g.nb, g.P, 1), L), X=X, Y=Y)))
+        self.y = F.zeros((sdp.N, 1), L)
+        self.timer = PhaseTimer(timing)
+        self.eig_refined = self.eig_unresolved = 0
+
+    # -- per-chunk pieces (sdpvibe/solver.py:622-665)
+    @staticmethod
+    def segments(g):
+        return [(c, r, (c * (c + 1) // 2 + r) * g.K) for c in range(g.dim) for r in range(c + 1)]
+
+    def cmws(self, g, Vs, a):
+        """sum_p a_p A_p per parity batch (constraint_matrix_weighted_sum)"""
+        a2 = dup(a)
+        h = g.h[0]
+        R = F.zeros((g.nbp, g.dim * h, g.dim * h), self.L)
+        V = Vs["V"][0]
+        for c, r, off in self.segments(g):
+            s = gemm(V, col_scale(V, sub(a2, off, off + g.K, 0, 1)), transB=True)
+            if r != c:
+                s = s.shift(-1)
+            put(R, r * h, c * h, s)
+            if r != c:
+                put(R, c * h, r * h, s.T)
+        return [R]
+
+    def pairings(self, g, Vs, cholX, Y):
+        Vx = Vs["Vx"][0]
+        T = cholX[0].solve_lower(Vx)
+        AXI = copy_lower_to_upper(gemm(T, T, transA=True))
+        AY = copy_lower_to_upper(gemm(Vx, gemm(Y[0], Vx), transA=True))
+        return [AXI], [AY]
+
+    def schur(self, g, AXI, AY):
+        K = g.K
+        if g.dim == 1:
+            S = fold(mul(AXI[0], AY[0]), g.nb)
+        else:
+            def sb(M, c, r):                                  # A_X_inv[c][r]
+                return sub(M, c * K, (c + 1) * K, r * K, (r + 1) * K)
+
+            def sy(M, c, r):                                  # A_Y[c][r]
+                return sub(M, r * K, (r + 1) * K, c * K, (c + 1) * K)
+            S = F.zeros((g.nb, g.P, g.P), self.L)
+            A, Yp = AXI[0], AY[0]
+            for c0, r0, ro in self.segments(g):
+                for c1, r1, co in self.segments(g):
+                    if co > ro:
+                        break
+                    el = None
+                    for t in (mul(sb(A, c0, r1), sy(Yp, c1, r0)), mul(sb(A, r0, r1), sy(Yp, c1, c0)),
+                              mul(sb(A, c0, c1), sy(Yp, r1, r0)), mul(sb(A, r0, c1), sy(Yp, r1, c0))):
+                        el = t if el is None else add(el, t)
+                    put(S, ro, co, fold(el, g.nb).shift(-2))
+        S = copy_lower_to_upper(S)
+        return set_diag_where(S, self.S(1), ~g.xmask)
+
+    def seg_diag(self, g, Ms, hs):
+        v = F.zeros((g.nb, g.P, 1), self.L)
+        for c, r, off in self.segments(g):
+            d = diag_of(sub(Ms[0], r * hs[0], (r + 1) * hs[0], c * hs[0], (c + 1) * hs[0]))
+            put(v, off, 0, fold(d, g.nb))
+        return v
+
+    # -- the iteration (sdpvibe/solver.py:680-982)
+    def run(self, max_iter=None, log=None, verbose=False, on_iteration=None, record=None):
+        """iterate until a termination criterion holds; returns the result dict.  record(it, solver,
+        info) is called after each iteration's update of y (tests read the iterates there)."""
+        p, sdp, S = self.p, self.sdp, self.S
+        G = sdp.groups
+        tm = self.timer
+        alphaP = alphaD = mp.mpf(0)
+        t0 = time.time()
+        it = 0
+        update = None
+        pobj = dobj = gap = primal_err = dual_err = mp.mpf(0)
+
+        def mk2(g):
+            return g.Xmask[0][:, :, None] & g.Xmask[0][:, None, :]
+
+        def result(reason, iterations):
+            return dict(terminateReason=reason, primalObjective=pobj, dualObjective=dobj, dualityGap=gap,
+                        primalError=primal_err, dualError=dual_err, iterations=iterations, time=time.time() - t0)
+        while True:
+            it += 1
+            ti = time.time()
+            cond = [mp.mpf(0), ""]
+
+            def upd_cond(lg2, name):
+                if lg2 > float(mp.log(cond[0], 2) if cond[0] > 0 else -1):
+                    cond[0] = mp.mpf(2) ** mp.mpf(lg2)
+                    cond[1] = name
+            tm("residues")
+            dobj = sdp.const + dot(sdp.b, self.y)
+            psum = musum = mp.mpf(0)
+            dual_err = primal_err_P = mp.mpf(0)
+            pvec = sdp.b
+            for gi, g in enumerate(G):
+                o = self.st[gi]
+                xs = o["xs"]
+                if update:
+                    aP, aD = update
+                    dc = o.pop("dc")
+                    xs = dict(x=add(xs["x"], mul(dc["dx"], aP)),
+                              X=[add(X, mul(d, aP)) for X, d in zip(xs["X"], dc["dX"])],
+                              Y=[add(Y, mul(d, aD)) for Y, d in zip(xs["Y"], dc["dY"])])
+                psum += dot(g.c, xs["x"])
+                cX = [Chol(X) for X in xs["X"]]
+                cY = [Chol(Y) for Y in xs["Y"]]
+                for tag, chs in (("X", cX), ("Y", cY)):
+                    lg = chol_log2_cond(chs[0], g.Xmask[0]).cpu().tolist()
+                    z = max(range(len(lg)), key=lambda i: lg[i])
+                    upd_cond(lg[z], f"{tag}_cholesky.block_{g.idx[z % g.nb]}_{z // g.nb}")
+                Vs = g.V
+                a, y_ = self.pairings(g, Vs, cX, xs["Y"])
+                d = -self.seg_diag(g, y_, [g.K])
+                o["AXI"], o["AY"] = a, y_
+                B = g.B
+                By = gemm(B, bexpand(self.y, g.nb))
+                d = add(d, By, -1)
+                dres = add(d, g.c)
+                pvec = add(pvec, gemm(flat_rows(B), flat_rows(xs["x"]), transA=True), -1)
+                Ax = self.cmws(g, Vs, xs["x"])
+                Pres = [masked(add(Ax[0], xs["X"][0], -1), mk2(g))]
+                dual_err = max(dual_err, max_abs(dres))
+                primal_err_P = max([primal_err_P] + [max_abs(P) for P in Pres])
+                mXY = [masked(-gemm(X, Y), mk2(g)) for X, Y in zip(xs["X"], xs["Y"])]
+                for M in mXY:
+                    musum += total(diag_of(M))
+                o["xs"], o["ch"] = xs, dict(X=cX, Y=cY)
+                o["res"] = dict(dres=dres, Pres=Pres, mXY=mXY)
+            update = None
+            pobj = sdp.const + psum
+            gap = abs(pobj - dobj) / max(abs(pobj) + abs(dobj), mp.mpf(1))
+            primal_err_p = max_abs(pvec)
+            primal_err = max(primal_err_P, primal_err_p)
+            dual_feas = dual_err < p["dualErrorThreshold"]
+            primal_feas = primal_err < p["primalErrorThreshold"]
+            pd_feas = dual_feas and primal_feas
+            reason = None
+            if pd_feas and gap < p["dualityGapThreshold"]:
+                reason = "found primal-dual optimal solution"
+            elif dual_feas and p["findDualFeasible"]:
+                reason = "found dual feasible solution"
+            elif primal_feas and p["findPrimalFeasible"]:
+                reason = "found primal feasible solution"
+            elif alphaD == 1 and p["detectDualFeasibleJump"]:
+                reason = "dual feasible jump detected"
+            elif alphaP == 1 and p["detectPrimalFeasibleJump"]:
+                reason = "primal feasible jump detected"
+            elif it > (max_iter or p["maxIterations"]):
+                reason = "maxIterations exceeded"
+            elif it > 1 and alphaP < p["minPrimalStep"]:
+                reason = "primal step too small"
+            elif it > 1 and alphaD < p["minDualStep"]:
+                reason = "dual step too small"
+            if reason:
+                self.result = result(reason, it - 1)
+                break
+            mu = -musum / sdp.total_psd_rows
+            if mu > p["maxComplementarity"]:
+                self.result = result("maxComplementarity exceeded", it - 1)
+                break
+            # Schur complement, its Cholesky factor, Q = sum_g P_g^T P_g (all chunks resident: P kept)
+            Q = None
+            for gi, g in enumerate(G):
+                o = self.st[gi]
+                tm("schur: assemble S")
+                Sg = self.schur(g, o.pop("AXI"), o.pop("AY"))
+                tm("schur: chol(S)")
+                cs = Chol(Sg)
+                lg = chol_log2_cond(cs, g.xmask).cpu().tolist()
+                q = max(range(len(lg)), key=lambda i: lg[i])
+                upd_cond(lg[q], f"schur_complement_cholesky.block_{g.idx[q]}")
+                tm("schur: P = L^-1 B")
+                P = cs.solve_lower(g.B)
+                tm("schur: Q += P^T P")
+                qg = gemm(flat_rows(P), flat_rows(P), transA=True)
+                Q = qg if Q is None else add(Q, qg)
+                o["cholS"], o["Pm"] = cs, P
+            tm("chol(Q)")
+            cholQ = Chol(copy_lower_to_upper(Q))
+            Q_cond = mp.mpf(2) ** mp.mpf(float(chol_log2_cond(cholQ)[0]))
+            del Q
+            dy, acc = self._direction(mu, pvec, cholQ, corr=False,
+                                      beta=mp.mpf(0) if pd_feas else p["infeasibleCenteringParameter"])
+            R_err = acc["Rerr"]
+            r = acc["fr"] / (mu * sdp.total_psd_rows)
+            beta = r * r if r < 1 else r
+            if pd_feas:
+                beta_c = min(max(p["feasibleCenteringParameter"], beta), mp.mpf(1))
+            else:
+                beta_c = max(p["infeasibleCenteringParameter"], beta)
+            dy, acc = self._direction(mu, pvec, cholQ, corr=True, beta=beta_c)
+            if acc.get("eig_refined"):
+                self.eig_refined += acc["eig_refined"]
+                self.eig_unresolved += acc.get("eig_unresolved", 0)
+            for o in self.st:
+                o.pop("cholS", None)
+                o.pop("Pm", None)
+            del cholQ
+            gm = p["stepLengthReduction"]
+            alphaP = step_from_eig(acc["lamP"], gm)
+            alphaD = step_from_eig(acc["lamD"], gm)
+            if pd_feas:
+                alphaP = alphaD = min(alphaP, alphaD)
+            tm("update")
+            aP, aD = S(alphaP), S(alphaD)
+            update = (aP, aD)
+            self.y = add(self.y, mul(dy, aD))
+            row = dict(iteration=it, total_time=round(time.time() - t0, 3), iter_time=round(time.time() - ti, 3),
+                       mu=mu, pobj=pobj, dobj=dobj, gap=gap, P_err=primal_err_P, p_err=primal_err_p, D_err=dual_err,
+                       R_err=R_err, P_step=alphaP, D_step=alphaD, beta=beta_c, Q_cond=Q_cond,
+                       max_block_cond=cond[0], block_name=cond[1])
+            self.last_mu, self.last_steps = mu, (alphaP, alphaD, beta_c)
+            if log is not None:
+                log.append(row)
+            if on_iteration is not None:
+                on_iteration(row)
+            if record is not None:
+                record(it, self, dict(dy=dy, aP=aP, aD=aD, row=row))
+            if verbose:
+                f = lambda v: mp.nstr(v, 3)
+                print(f"{it:4d} {time.time() - t0:7.2f} mu {f(mu)} P-obj {f(pobj)} D-obj {f(dobj)} gap {f(gap)} "
+                      f"P-err {f(primal_err_P)} D-err {f(dual_err)} steps {f(alphaP)} {f(alphaD)} beta {f(beta_c)}",
+                      flush=True)
+        self._pending_update = update
+        return self.result
+
+    def _direction(self, mu, pvec, cholQ, corr, beta):
+        """predictor (corr=False) or corrector search direction (sdpvibe/solver.py:870-933): dy, and per
+        chunk dp (predictor) or dc (corrector) with the step-length eigenvalues"""
+        p, S, G = self.p, self.S, self.sdp.groups
+        tm = self.timer
+        bm, muS = S(beta * mu), S(mu)
+
+        def mk2(g):
+            return g.Xmask[0][:, :, None] & g.Xmask[0][:, None, :]
+        acc = dict(Rerr=mp.mpf(0), fr=mp.mpf(0), lamP=None, lamD=None)
+        tm("direction (corrector) 1" if corr else "direction (predictor) 1")
+        dy = pvec
+        for gi, g in enumerate(G):
+            o = self.st[gi]
+            xs, res, cX = o["xs"], o["res"], o["ch"]["X"]
+            if not corr:
+                acc["Rerr"] = max([acc["Rerr"]] + [max_abs(add_diag(M, muS, g.Xmask[0])) for M in res["mXY"]])
+            Rb = res["mXY"][0] if not corr else add(res["mXY"][0], gemm(o["dp"]["dX"][0], o["dp"]["dY"][0]), -1)
+            Rb = add_diag(Rb, bm, g.Xmask[0])
+            Z = symmetrize(cX[0].solve(add(gemm(res["Pres"][0], xs["Y"][0]), Rb, -1)))
+            Vx = g.V["Vx"][0]
+            VZV = gemm(Vx, gemm(Z, Vx), transA=True)
+            rhs = add(-res["dres"], self.seg_diag(g, [VZV], [g.K]), -1)
+            w = o["cholS"].solve_lower(rhs)
+            o["dir"] = dict(R=[Rb], W=w)
+            dy = add(dy, gemm(flat_rows(o["Pm"]), flat_rows(w), transA=True), -1)
+        dy = cholQ.solve(dy)
+        tm("direction (corrector) 2 + step length" if corr else "direction (predictor) 2")
+        for gi, g in enumerate(G):
+            o = self.st[gi]
+            xs, res, cX, dr = o["xs"], o["res"], o["ch"]["X"], o.pop("dir")
+            Pdy = gemm(o["Pm"], bexpand(dy, g.nb))
+            dxg = o["cholS"].solve_upper(add(dr["W"], Pdy))
+            Ad = self.cmws(g, g.V, dxg)
+            dXg = [add(Ad[0], res["Pres"][0])]
+            dYg = [masked(-symmetrize(cX[0].solve(add(gemm(dXg[0], xs["Y"][0]), dr["R"][0], -1))), mk2(g))]
+            if not corr:
+                acc["fr"] += dot(masked(add(xs["X"][0], dXg[0]), mk2(g)), masked(add(xs["Y"][0], dYg[0]), mk2(g)))
+                o["dp"] = dict(dX=dXg, dY=dYg)
+            else:
+                gm = p["stepLengthReduction"]
+                st = {}
+                lamP = min_eig(o["ch"]["X"], dXg, gamma=gm, stats=st)
+                lamD = min_eig(o["ch"]["Y"], dYg, gamma=gm, stats=st)
+                for k, v in (("lamP", lamP), ("lamD", lamD)):
+                    if v is not None:
+                        acc[k] = v if acc[k] is None else min(acc[k], v)
+                for k in ("eig_refined", "eig_unresolved"):
+                    acc[k] = acc.get(k, 0) + st.get(k, 0)
+                o.pop("dp", None)
+                o["dc"] = dict(dx=dxg, dX=dXg, dY=dYg)
+        return dy, acc
