@@ -437,6 +437,63 @@ def run_cholsolve(args, rank, world, local_rank):
 CS_LIMBS_NOTE = "26 (832 bits); base tiles in WL = 50-word fixed point"
 
 
+# ------------------------------------------------------------------ full solver iterations (SDP s/iter)
+def run_solver(args, rank, world, local_rank):
+    """SDPB iterations on the Ising-structured synthetic SDP: 300 blocks (dims 1/2/3 = 180/90/30,
+    degree d ~ U[20,40], K = d+1), N = 1000, L = 26 (the 768-bit precision rule).  A step is one
+    iteration; `--warmup` first iterations are excluded; metric s/iteration (lower is better)."""
+    import torch
+    import mpmath as mp
+    from sdpvibe_b200 import _trace
+    from sdpvibe_b200.solver import Solver
+    from sdpvibe_b200.synthetic import ising_like_sdp
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    Ls = 26
+    t0 = time.perf_counter()
+    sdp, blocks = ising_like_sdp(Ls)
+    t_build = time.perf_counter() - t0
+    sol = Solver(sdp, Ls, timing=True)
+    marks = []
+
+    def rec(it, s, info):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        marks.append((it, ev, info["row"]))
+    tr = _trace.Trace()
+    warm = max(args.warmup, 1)
+    total_it = warm + args.steps
+    with ClockSampler(local_rank) as clk, tr:
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        sol.run(max_iter=total_it, record=rec)
+        torch.cuda.synchronize()
+    if rank != 0:
+        return
+    ev = [start] + [m[1] for m in marks]
+    per_it = [ev[i].elapsed_time(ev[i + 1]) * 1e-3 for i in range(len(ev) - 1)]
+    timed = per_it[warm:]
+    s_it = statistics.mean(timed)
+    last = marks[-1][2]
+    line = {"metric": "768-bit SDP s/iter (Ising-structured synthetic SDP, 300 blocks, N=1000)",
+            "value": s_it, "unit": "s/iter", "n_gpus": world, "steps": len(timed), "warmup": warm,
+            "ms_per_step": s_it * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int8 residue GEMM + int32 fixed point (832-bit MPF, L=26)", "data": "synthetic",
+            "config": {"workload": "solver: SDPB predictor-corrector iterations, ising_like SDP "
+                                   "(300 blocks dims 1/2/3 = 180/90/30, d~U[20,40], K=d+1, damped monomial "
+                                   "bases, random B/c/b; numpy seed 0), N=1000, L=26",
+                       "sum_P_padded": int(sum(g.nb * g.P for g in sdp.groups)),
+                       "chunks": [dict(dim=g.dim, nb=g.nb, K=g.K, h=g.h[0], P=g.P) for g in sdp.groups],
+                       "l2": "working set of several GB; no flush"},
+            "per_iteration_s": per_it, "build_s": t_build,
+            "last_row": {k: (mp.nstr(v, 6) if isinstance(v, mp.mpf) else v) for k, v in last.items()},
+            "phase_s_per_iter": {k: v / total_it for k, v in sol.timer.totals().items()},
+            "gpu_launches": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
+            "eig_refined": sol.eig_refined, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,8 +501,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=("gram", "cholsolve"), default="gram",
-                    help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve")
+    ap.add_argument("--workload", choices=("gram", "cholsolve", "solver"), default="gram",
+                    help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "
+                         "solver: SDPB iterations (s/iter)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -459,7 +517,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        (run_cholsolve if args.workload == "cholsolve" else run_b200)(args, rank, world, local_rank)
+        run = {"gram": run_b200, "cholsolve": run_cholsolve, "solver": run_solver}[args.workload]
+        run(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

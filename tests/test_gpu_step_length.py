@@ -117,5 +117,5 @@ def test_step_from_eig_unconstrained():
     X, D = _case(16, [Fraction(k + 1, 4) for k in range(16)], 5)          # dM positive definite
     ch = Chol(MPF(X.m[:, None], X.e[None]))
     lam = min_eig([ch], [MPF(D.m[:, None], D.e[None])], gamma=GAMMA)
-    assert abs(lam - mp.mpf(1) / 4) < mp.mpf(2) ** -60
+    assert abs(lam - mp.mpf(1) / 4) < 1e-13                                # float64 eigenvalue
     assert step_from_eig(lam, GAMMA) == 1
