@@ -279,11 +279,422 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_kernel(const u32* __rest
   }
 }
 
+
+// ================================================================ shared-memory tile kernels (WL <= 64)
+// The same arithmetic as the kernels above, organised for latency: the tile lives in shared memory,
+// serial products (Newton, pivot-column scaling, the row sums of the inverse) run warp-cooperatively with
+// one product column per lane and carries resolved by warp ballots, and the bulk products (trailing update,
+// inverse row products) run one per thread on 96-bit column accumulators (mad.cc carry chains) straight
+// from shared-memory magnitudes.  Every product is the same truncated product (same columns, same kept
+// words), and sums of products are exact in WL words, so the results are bit-identical to the kernels above.
+constexpr int FW = 64;                    // fast path: WL <= FW
+constexpr unsigned kFull = 0xffffffffu;
+
+struct WarpScratch {                      // per-warp product scratch
+  u32 xa[FW], xb[FW], acc[FW];
+};
+
+__device__ __forceinline__ void mac96(u32& c0, u32& c1, u32& c2, u32 x, u32 y) {
+  asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+      "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "+r"(c0), "+r"(c1), "+r"(c2)
+      : "r"(x), "r"(y));
+}
+
+// Carry into this lane of a 32-lane digit chain: g = this lane's digit overflowed (carry out whatever
+// comes in), p = this lane's digit is all ones (passes a carry on).  cin: carry into lane 0; cout: carry
+// out of lane 31.  g and p are never both set.  With X = G|P and Y = G as 32-bit numbers, the internal
+// carries of X + Y + cin are exactly the chain's carries.
+__device__ __forceinline__ u32 chain_carry(bool g, bool p, u32 cin, u32& cout) {
+  const unsigned G = __ballot_sync(kFull, g), P = __ballot_sync(kFull, p);
+  const unsigned X = G | P;
+  const u64 sum = (u64)X + G + cin;
+  cout = (u32)(sum >> 32);
+  return (((u32)sum ^ X ^ G) >> (threadIdx.x & 31)) & 1u;
+}
+
+// Words lane and lane+32 of a two's-complement WL-word number negated (mod 2^(32 WL)): ~x plus a carry that
+// enters word w when every lower word is zero.
+__device__ __forceinline__ void warp_negate(u32& v0, u32& v1, int WL) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lower = (1u << lane) - 1u;
+  const unsigned nz0 = __ballot_sync(kFull, lane < WL && v0 != 0);
+  const unsigned nz1 = __ballot_sync(kFull, lane + 32 < WL && v1 != 0);
+  v0 = ~v0 + (((nz0 & lower) == 0) ? 1u : 0u);
+  v1 = ~v1 + ((nz0 == 0 && (nz1 & lower) == 0) ? 1u : 0u);
+}
+
+__device__ __forceinline__ int warp_top(u32 v0, u32 v1, int WL) {
+  const int lane = threadIdx.x & 31;
+  const unsigned b0 = __ballot_sync(kFull, lane < WL && v0 != 0);
+  const unsigned b1 = __ballot_sync(kFull, lane + 32 < WL && v1 != 0);
+  return b1 ? 63 - __clz(b1) : (b0 ? 31 - __clz(b0) : 0);
+}
+
+// Magnitude of a two's-complement WL-word operand (shared or global memory) into m[0..WL); returns its sign,
+// top = index of its highest nonzero word (0 for zero).  Warp-collective.
+__device__ __forceinline__ int load_mag(const u32* src, u32* m, int WL, int& top) {
+  const int lane = threadIdx.x & 31;
+  const int sign = (int)(src[WL - 1] >> 31);
+  u32 v0 = lane < WL ? src[lane] : 0u, v1 = lane + 32 < WL ? src[lane + 32] : 0u;
+  if (sign) warp_negate(v0, v1, WL);
+  if (lane < WL) m[lane] = v0;
+  if (lane + 32 < WL) m[lane + 32] = v1;
+  top = warp_top(v0, v1, WL);
+  return sign;
+}
+
+// Warp-cooperative truncated product a * b >> F (top t words of each operand when t > 0): one product
+// column per lane, columns kmin .. min(kmax + 2, LF + WL - 1), each a 96-bit exact sum; the column sums are
+// added with their 32- and 64-bit shifts and the carries resolved by chain_carry.  Outputs (any may be
+// null): out = signed result (may alias a or b), omag = magnitude, *osign / *otop (written by lane 0).
+__device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScratch& s, u32* out, u32* omag,
+                     uint8_t* osign, uint8_t* otop) {
+  const int lane = threadIdx.x & 31;
+  int ta, tb;
+  const int sa = load_mag(a, s.xa, WL, ta);
+  const int sb = load_mag(b, s.xb, WL, tb);
+  __syncwarp();
+  s.acc[lane] = 0;
+  s.acc[lane + 32] = 0;
+  const int la = t ? max(0, ta - t + 1) : 0, lb = t ? max(0, tb - t + 1) : 0;
+  const int kmin = max(LF - 2, la + lb), kmax = ta + tb;
+  const int ncol = min(kmax + 2, LF + WL - 1) - kmin + 1;
+  __syncwarp();
+  u32 p_c1 = 0, p_c2a = 0, p_c2b = 0, p_h = 0, cin = 0;          // carried over from the previous 32 columns
+  for (int q0 = 0; q0 < ncol; q0 += 32) {
+    const int q = q0 + lane, k = kmin + q;
+    u32 c0 = 0, c1 = 0, c2 = 0;
+    if (q < ncol && k <= kmax) {
+      const int i0 = max(la, k - tb), i1 = min(ta, k - lb);
+      for (int i = i0; i <= i1; i++) mac96(c0, c1, c2, s.xa[i], s.xb[k - i]);
+    }
+    u32 c1u = __shfl_up_sync(kFull, c1, 1), c2u = __shfl_up_sync(kFull, c2, 2);
+    if (lane == 0) c1u = p_c1;
+    if (lane == 0) c2u = p_c2a;
+    if (lane == 1) c2u = p_c2b;
+    const u32 n_c1 = __shfl_sync(kFull, c1, 31), n_c2a = __shfl_sync(kFull, c2, 30), n_c2b = __shfl_sync(kFull, c2, 31);
+    const u64 v = (u64)c0 + c1u + c2u;                                 // < 3 * 2^32
+    const u32 lo = (u32)v, h = (u32)(v >> 32);
+    u32 hu = __shfl_up_sync(kFull, h, 1);
+    if (lane == 0) hu = p_h;
+    const u32 n_h = __shfl_sync(kFull, h, 31);
+    const u32 e = lo + hu;
+    u32 cout;
+    const u32 cj = chain_carry(e < lo, e == kFull, cin, cout);
+    const int w = k - LF;
+    if (q < ncol && w >= 0 && w < WL) s.acc[w] = e + cj;
+    p_c1 = n_c1;
+    p_c2a = n_c2a;
+    p_c2b = n_c2b;
+    p_h = n_h;
+    cin = cout;
+  }
+  __syncwarp();
+  u32 m0 = lane < WL ? s.acc[lane] : 0u, m1 = lane + 32 < WL ? s.acc[lane + 32] : 0u;
+  const int sg = sa ^ sb;
+  if (omag) {
+    if (lane < WL) omag[lane] = m0;
+    if (lane + 32 < WL) omag[lane + 32] = m1;
+  }
+  if (otop) {
+    const int tp = warp_top(m0, m1, WL);
+    if (lane == 0) *otop = (uint8_t)tp;
+  }
+  if (osign && lane == 0) *osign = (uint8_t)sg;
+  if (out) {
+    if (sg) warp_negate(m0, m1, WL);
+    if (lane < WL) out[lane] = m0;
+    if (lane + 32 < WL) out[lane + 32] = m1;
+  }
+  __syncwarp();
+}
+
+// dst (two's complement, WL words) += trunc(|x| |y|) if add, else -= ; x, y magnitudes with tops tx, ty.
+// Columns from LF - 2 (t = 0 products), product scanning on a 96-bit accumulator; the kept words are
+// added into dst as they come out, then the carry (borrow) runs up until it dies.  One thread.
+__device__ void fx_rmw(u32* dst, const u32* x, int tx, const u32* y, int ty, bool add, int WL, int LF) {
+  const int kmin = LF - 2, kmax = tx + ty;
+  u32 c0 = 0, c1 = 0, c2 = 0, cy = 0;
+  int w = 0;
+  auto emit = [&](u32 d) {
+    if (w < WL) {
+      const u32 o = dst[w];
+      if (add) {
+        const u64 r = (u64)o + d + cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 32);
+      } else {
+        const u64 r = (u64)o - d - cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 63);
+      }
+      w++;
+    }
+  };
+  for (int k = kmin; k <= kmax; k++) {
+    const int i0 = max(0, k - ty), i1 = min(tx, k);
+    for (int i = i0; i <= i1; i++) mac96(c0, c1, c2, x[i], y[k - i]);
+    if (k >= LF) emit(c0);
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  for (int k = max(kmax + 1, kmin); k <= kmax + 2; k++) {
+    if (k >= LF) emit(c0);
+    c0 = c1;
+    c1 = 0;
+  }
+  while (cy && w < WL) emit(0);
+}
+
+
+// Warp-parallel WL-word arithmetic for the Newton steps (words lane and lane + 32 of each operand).
+__device__ __forceinline__ void warp_addsub(u32* r, const u32* a, const u32* b, bool sub, int WL) {
+  const int lane = threadIdx.x & 31;
+  u32 carry = sub ? 1u : 0u;                                  // a - b = a + ~b + 1
+  for (int c = 0; c < 2; c++) {
+    const int w = lane + 32 * c;
+    const u32 av = w < WL ? a[w] : 0u, bv = w < WL ? (sub ? ~b[w] : b[w]) : 0u;
+    const u64 v = (u64)av + bv;
+    const u32 e = (u32)v;
+    u32 cout;
+    const u32 cj = chain_carry((v >> 32) != 0, e == kFull, carry, cout);
+    __syncwarp();
+    if (w < WL) r[w] = e + cj;
+    carry = cout;
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arithmetic shift right by one bit
+  const int lane = threadIdx.x & 31;
+  u32 n[2];
+  for (int c = 0; c < 2; c++) {
+    const int w = lane + 32 * c;
+    n[c] = 0;
+    if (w < WL - 1) n[c] = (x[w] >> 1) | (x[w + 1] << 31);
+    else if (w == WL - 1) n[c] = (u32)(((int32_t)x[w]) >> 1);
+  }
+  __syncwarp();
+  for (int c = 0; c < 2; c++)
+    if (lane + 32 * c < WL) x[lane + 32 * c] = n[c];
+  __syncwarp();
+}
+
+__host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
+  return (size_t)(528 + 32) * WL * 4 + 8 * sizeof(WarpScratch) + 5 * FW * 4 + 64;
+}
+__host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
+  return (size_t)(528 + 32 + 288) * WL * 4 + 8 * sizeof(WarpScratch) + 2 * 528 + 64;
+}
+
+__device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
+__global__ void __launch_bounds__(kThreads) chol_tiles_smem_kernel(u32* __restrict__ A, u32* __restrict__ RINV,
+                                                                   int WL, int LF, unsigned* __restrict__ err) {
+  extern __shared__ __align__(16) u32 sm[];
+  u32* T = sm;                                                   // lower triangle, entry (i, j) at tri(i, j)
+  u32* colmag = T + 528 * WL;                                    // |l_ik| of the current column
+  WarpScratch* ws = reinterpret_cast<WarpScratch*>(colmag + 32 * WL);
+  u32* nw = reinterpret_cast<u32*>(ws + 8);
+  u32 *sd = nw, *sr = nw + FW, *st1 = nw + 2 * FW, *st2 = nw + 3 * FW, *sone = nw + 4 * FW;
+  uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * FW);
+  uint8_t* coltop = colsign + 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  u32* G = A + (size_t)blockIdx.x * BT * BT * WL;
+  u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
+  for (int i = 0; i < BT; i++) {
+    const u32* src = G + (size_t)i * BT * WL;
+    u32* dst = T + (size_t)tri(i, 0) * WL;
+    for (int w = tid; w < (i + 1) * WL; w += kThreads) dst[w] = src[w];
+  }
+  __syncthreads();
+  for (int k = 0; k < BT; k++) {
+    u32* akk = T + (size_t)tri(k, k) * WL;
+    if (warp == 0) {
+      for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
+      for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
+      __syncwarp();
+      if (lane == 0) {
+        if ((sd[WL - 1] >> 31) || (top_word(sd, WL) == 0 && sd[0] == 0)) atomicOr(err, SDPV_ERRBIT_NOTSPD);
+        fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
+      }
+      __syncwarp();
+      for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
+        int t = bits / 32 + 2;
+        if (t >= WL) t = 0;
+        wmul(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+        wmul(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+        warp_addsub(st1, sone, st2, true, WL);
+        wmul(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+        warp_shr1(st2, WL);
+        warp_addsub(sr, sr, st2, false, WL);
+        if (t == 0) break;
+      }
+      wmul(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);   // l_kk = d * d^-1/2
+      for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
+    }
+    __syncthreads();
+    for (int i = k + 1 + warp; i < BT; i += 8) {                 // l_ik = a_ik * r_k
+      u32* aik = T + (size_t)tri(i, k) * WL;
+      wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WL, colsign + i, coltop + i);
+    }
+    __syncthreads();
+    const int m = BT - k - 1, npairs = m * (m + 1) / 2;
+    for (int p = tid; p < npairs; p += kThreads) {               // a_ij -= l_ik l_jk, k < j <= i
+      int ii = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+      while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
+      while (ii * (ii + 1) / 2 > p) ii--;
+      const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
+      fx_rmw(T + (size_t)tri(i, j) * WL, colmag + (size_t)i * WL, coltop[i], colmag + (size_t)j * WL, coltop[j],
+             colsign[i] != colsign[j], WL, LF);
+    }
+    __syncthreads();
+  }
+  for (int i = 0; i < BT; i++) {
+    u32* dst = G + (size_t)i * BT * WL;
+    const u32* src = T + (size_t)tri(i, 0) * WL;
+    for (int w = tid; w < (i + 1) * WL; w += kThreads) dst[w] = src[w];
+  }
+}
+
+// Number of partial-sum slots of column k in row i when each slot takes up to c products.
+__device__ __forceinline__ int nslots(int i, int k, int c) { return (i - k + c - 1) / c; }
+
+__global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* __restrict__ Lt,
+                                                                    const u32* __restrict__ RINV,
+                                                                    u32* __restrict__ X, int WL, int LF) {
+  extern __shared__ __align__(16) u32 sm[];
+  u32* Xm = sm;                                                  // |x_ik|, lower triangle
+  u32* Lrow = Xm + 528 * WL;                                     // |l_ij|, j < i, of the current row
+  u32* part = Lrow + 32 * WL;                                    // partial sums (two's complement)
+  WarpScratch* ws = reinterpret_cast<WarpScratch*>(part + 288 * WL);
+  uint8_t* xs = reinterpret_cast<uint8_t*>(ws + 8);             // signs, tops of x
+  uint8_t* xt = xs + 528;
+  uint8_t* ls = xt + 528;                                        // signs, tops of the row of L
+  uint8_t* lt = ls + 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32* LG = Lt + (size_t)blockIdx.x * BT * BT * WL;
+  const u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
+  u32* XG = X + (size_t)blockIdx.x * BT * BT * WL;
+  if (warp == 0) {                                               // x_00 = r_0
+    int top;
+    const int sg = load_mag(RI, Xm, WL, top);
+    if (lane == 0) {
+      xs[0] = (uint8_t)sg;
+      xt[0] = (uint8_t)top;
+    }
+  }
+  for (int i = 1; i < BT; i++) {
+    for (int j = warp; j <= i; j += 8) {
+      int top, sg;
+      if (j < i) {
+        sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lrow + (size_t)j * WL, WL, top);
+        if (lane == 0) {
+          ls[j] = (uint8_t)sg;
+          lt[j] = (uint8_t)top;
+        }
+      } else {                                                   // x_ii = r_i
+        sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WL, WL, top);
+        if (lane == 0) {
+          xs[tri(i, i)] = (uint8_t)sg;
+          xt[tri(i, i)] = (uint8_t)top;
+        }
+      }
+    }
+    __syncthreads();
+    // partial sums of l_ij x_jk over runs of up to c consecutive j, for every k < i
+    const int c = (i * (i + 1) / 2 + kThreads - 1) / kThreads;
+    int total = 0;
+    for (int k = 0; k < i; k++) total += nslots(i, k, c);
+    for (int slot = tid; slot < total; slot += kThreads) {
+      int k = 0, r = slot;
+      while (r >= nslots(i, k, c)) r -= nslots(i, k, c), k++;
+      const int j0 = k + r * c, j1 = min(i, j0 + c);
+      u32* dst = part + (size_t)slot * WL;
+      for (int w = 0; w < WL; w++) dst[w] = 0;
+      for (int j = j0; j < j1; j++) {
+        const int e = tri(j, k);
+        fx_rmw(dst, Lrow + (size_t)j * WL, lt[j], Xm + (size_t)e * WL, xt[e], ls[j] == xs[e], WL, LF);
+      }
+    }
+    __syncthreads();
+    // x_ik = -(sum of the partials) * r_i
+    for (int k = warp; k < i; k += 8) {
+      int base = 0;
+      for (int kk = 0; kk < k; kk++) base += nslots(i, kk, c);
+      const int n = nslots(i, k, c);
+      WarpScratch& s = ws[warp];
+      u32 carry = 0, hprev = 0;
+      for (int cc = 0; cc < 2; cc++) {
+        const int w = lane + 32 * cc;
+        u64 v = 0;
+        if (w < WL)
+          for (int q = 0; q < n; q++) v += part[(size_t)(base + q) * WL + w];
+        const u32 lo = (u32)v, h = (u32)(v >> 32);
+        u32 hu = __shfl_up_sync(kFull, h, 1);
+        if (lane == 0) hu = hprev;
+        hprev = __shfl_sync(kFull, h, 31);
+        const u32 e = lo + hu;
+        u32 cout;
+        const u32 cj = chain_carry(e < lo, e == kFull, carry, cout);
+        if (w < WL) s.acc[w] = e + cj;
+        carry = cout;
+      }
+      __syncwarp();
+      const int ei = tri(i, k);
+      wmul(s.acc, RI + (size_t)i * WL, 0, WL, LF, s, nullptr, Xm + (size_t)ei * WL, xs + ei, xt + ei);
+      if (lane == 0) xs[ei] ^= 1;                                // the negation
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+  for (int e = warp; e < BT * BT; e += 8) {                      // two's complement out; upper part zero
+    const int i = e / BT, k = e % BT;
+    u32* dst = XG + (size_t)e * WL;
+    if (k > i) {
+      for (int w = lane; w < WL; w += 32) dst[w] = 0;
+      continue;
+    }
+    const int ei = tri(i, k);
+    u32 v0 = lane < WL ? Xm[(size_t)ei * WL + lane] : 0u, v1 = lane + 32 < WL ? Xm[(size_t)ei * WL + lane + 32] : 0u;
+    if (xs[ei]) warp_negate(v0, v1, WL);
+    if (lane < WL) dst[lane] = v0;
+    if (lane + 32 < WL) dst[lane + 32] = v1;
+  }
+}
+
+}  // namespace
+
+namespace {
+// Opt-in shared memory of the tile kernels, set once per process for the largest fast-path tile (WL = FW).
+int smem_attributes() {
+  static std::once_flag once;
+  static cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+  std::call_once(once, [] {
+    e1 = cudaFuncSetAttribute(chol_tiles_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)chol_smem_bytes(FW));
+    e2 = cudaFuncSetAttribute(trinv_tiles_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)trinv_smem_bytes(FW));
+  });
+  if (e1 != cudaSuccess) return sdpv::set_cuda_error(e1);
+  if (e2 != cudaSuccess) return sdpv::set_cuda_error(e2);
+  return SDPV_OK;
+}
 }  // namespace
 
 extern "C" int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
+  if (WL <= FW) {
+    int st = smem_attributes();
+    if (st != SDPV_OK) return st;
+    chol_tiles_smem_kernel<<<(unsigned)ntiles, kThreads, chol_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+        A, RINV, WL, LF, sdpv::device_error_word());
+    return sdpv::launch_status();
+  }
   chol_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(A, RINV, WL, LF,
                                                                                sdpv::device_error_word());
   return sdpv::launch_status();
@@ -293,6 +704,13 @@ extern "C" int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32
                                 int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
+  if (WL <= FW) {                                   // shared-memory kernel: S is not used
+    int st = smem_attributes();
+    if (st != SDPV_OK) return st;
+    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreads, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+        Lt, RINV, X, WL, LF);
+    return sdpv::launch_status();
+  }
   trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, S, WL, LF);
   return sdpv::launch_status();
 }

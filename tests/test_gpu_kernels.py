@@ -459,3 +459,53 @@ def test_cholsolve_buckets_vs_oracle(sb):
             n, Ai, Bi = cases[i]
             xf = mpf.MPF(X.m[:, q, :n], X.e[q, :n]).to_float()
             assert np.allclose(Ai @ xf, Bi, rtol=0, atol=1e-9)
+
+
+def _spd_tiles(rng, nb, L, ill):
+    """nb random 32 x 32 SPD tiles in wide fixed point (WL = L + 24 words, F = 32 L fraction bits),
+    entry-major (nb, 32, 32, WL) uint32; diagonal below 1.  ill: columns of the generator scaled by
+    2^-e, e up to 8 L bits, so pivots get tiny and the pivot reciprocals and the inverse get large."""
+    WL, F = L + 24, 32 * L
+    out = np.zeros((nb, 32, 32, WL), np.uint32)
+    for b in range(nb):
+        G = [[int(v) for v in row] for row in rng.integers(-(1 << 20), 1 << 20, size=(32, 32))]
+        ex = [int(v) for v in rng.integers(0, 8 * L if ill else 4, size=32)]
+        emax = 2 * max(ex)
+        A = [[sum(G[i][k] * G[j][k] << (emax - 2 * ex[k]) for k in range(32)) for j in range(32)] for i in range(32)]
+        if not ill:
+            for i in range(32):
+                A[i][i] += 1 << (emax + 30)
+        s = max(A[i][i] for i in range(32)).bit_length() + 1
+        for i in range(32):
+            for j in range(32):
+                v = A[i][j]
+                v = (v << (F - s)) if F >= s else (v >> (s - F))
+                u = v % (1 << (32 * WL))
+                out[b, i, j] = [(u >> (32 * w)) & 0xffffffff for w in range(WL)]
+    return out
+
+
+@pytest.mark.parametrize("L", [8, 26, 40, 44])
+@pytest.mark.parametrize("ill", [False, True])
+def test_tile_kernels_vs_oracle(sb, L, ill):
+    """sdpv_chol_tiles / sdpv_trinv_tiles on random SPD tiles against the oracle, bit for bit: the
+    shared-memory kernels (WL <= 64) and the global-memory kernels (WL > 64), well and ill conditioned."""
+    from sdpvibe_b200 import _lib
+    rng = np.random.default_rng(L * 7 + ill)
+    nb, WL, LF = 3, L + 24, L
+    W = _spd_tiles(rng, nb, L, ill)
+    RA, RR = O.chol_tiles(W, 32, WL, LF)
+    A = cu(W.view(np.int32))
+    RINV = torch.zeros((nb, 32, WL), dtype=torch.int32, device="cuda")
+    _lib.call("sdpv_chol_tiles", _lib.ptr(A), _lib.ptr(RINV), nb, 32, WL, LF, _lib.stream())
+    got = np_(A).view(np.uint32)
+    tri = np.tril(np.ones((32, 32), bool))
+    assert np.array_equal(got[:, tri], RA[:, tri])
+    assert np.array_equal(np_(RINV).view(np.uint32), RR)
+    Lw = np.where(tri[None, :, :, None], RA, 0).astype(np.uint32)
+    RX = O.trinv_tiles(Lw, RR, 32, WL, LF)
+    X = torch.empty_like(A)
+    S = torch.empty_like(A)
+    _lib.call("sdpv_trinv_tiles", _lib.ptr(cu(Lw.view(np.int32))), _lib.ptr(RINV), _lib.ptr(X), _lib.ptr(S), nb, 32,
+              WL, LF, _lib.stream())
+    assert np.array_equal(np_(X).view(np.uint32), RX)
