@@ -118,8 +118,9 @@ int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t l
  *   acc[g0+g][b*M + i][j] <- (acc + A_gb B_gb^T) mod m, A_gb = 128 Ahi + Alo (M x KC), B likewise (N x KC)
  * with A* (G, nb*M, KC), B* (G, nb*N, KC) int8 whose modulus planes are a_stride / b_stride bytes apart (0: packed),
  * acc (n, nb*M, ldc) int16 (row stride ldc >= N; a
- * multiple of 8 lets the epilogue move 16 bytes at a time).  mode 0: all entries;
- * mode 1 (syrk): B = A (Bhi/Blo ignored, N = M) and only entries with i >= j are updated.
+ * multiple of 8 lets the epilogue move 16 bytes at a time).  mode bit 0 clear: all entries;
+ * set (syrk): B = A (Bhi/Blo ignored, N = M) and only entries with i >= j are updated.  mode bit 1 set
+ * (fresh): the updated entries of acc are taken as zero and overwritten, not read.
  * KC must be a multiple of 16 and <= 65536.  Replaces RNS.accumulate / _gemm_kernel
  * (sdpvibe/rns.py:106-137, 217-224), batched._bgemm_kernel (sdpvibe/batched.py:96-127) and
  * batched._syrk_lower_kernel (sdpvibe/batched.py:130-162). */

@@ -88,13 +88,13 @@ def bgemm_nt(A, Bt, out_exp="col", kc=4096, bt_rowexp=None):
     L = A.L
     R = ctx(L)
     eA = A.exp if isinstance(A.exp, int) else A.exp[:, 0]
-    acc = torch.zeros((R.n, nb * M, N), dtype=torch.int16, device=dev)
+    acc = (torch.empty if K else torch.zeros)((R.n, nb * M, N), dtype=torch.int16, device=dev)
     if K:
         Av = A.limbs.reshape(L, nb * M, K)
         if A.limbs.data_ptr() == Bt.limbs.data_ptr() and M == N:
-            residue_product(R, Av, Av, acc, nb=nb)
+            residue_product(R, Av, Av, acc, nb=nb, fresh=True)
         else:
-            residue_product(R, Av, Bt.limbs.reshape(L, nb * N, K), acc, nb=nb)
+            residue_product(R, Av, Bt.limbs.reshape(L, nb * N, K), acc, nb=nb, fresh=True)
     eB = Bt.exp if bt_rowexp is None else bt_rowexp
     if isinstance(eA, int) and isinstance(eB, int):
         e_in = eA + eB

@@ -29,6 +29,12 @@ struct CrtSmemHead {
   int abort;
 };
 
+constexpr int kNmax = 320;                  // moduli tables staged in shared memory (n <= 320)
+struct CrtTables {
+  int m[kNmax], inv[kNmax];
+  float minv[kNmax];
+};
+
 // Dynamic shared memory: [head (1 KB)] [Yh: ktc slices] [Yl: ktc slices] [Ct: Epad/128 * ktc slices]
 template <int MODE>
 __global__ void __launch_bounds__(kThreads)
@@ -40,7 +46,8 @@ __global__ void __launch_bounds__(kThreads)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   CrtSmemHead& H = *reinterpret_cast<CrtSmemHead*>(base);
-  uint8_t* Yh = base + 1024;
+  CrtTables& TB = *reinterpret_cast<CrtTables*>(base + 64);
+  uint8_t* Yh = base + 4096;
   uint8_t* Yl = Yh + (size_t)ktc * kSlice;
   uint8_t* Ct = Yl + (size_t)ktc * kSlice;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -56,6 +63,11 @@ __global__ void __launch_bounds__(kThreads)
   if (warp == 0) {
     tmem_alloc(&H.tmem_slot, 2 * kDig);
     tmem_relinquish();
+  }
+  for (int g = tid; g < kNmax; g += kThreads) {
+    TB.m[g] = g < n ? mods[g] : 1;
+    TB.inv[g] = g < n ? invs[g] : 0;
+    TB.minv[g] = g < n ? minvs[g] : 1.f;
   }
   __syncthreads();
   tc_fence_after();
@@ -80,26 +92,35 @@ __global__ void __launch_bounds__(kThreads)
     const i64 r = valid ? e / w : 0, jj = valid ? e - (e / w) * w : 0;
     const int16_t* ap = acc + r * N + j0 + jj;
     float ks = 0.f;
-    for (int g16 = 0; g16 < ktc * 128; g16 += 16) {
-      u32 ph[4], pl[4];
+    for (int g32 = 0; g32 < ktc * 128; g32 += 32) {
+      // issue all 32 loads of this group before using any (they are independent)
+      int av[32];
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        int g = g16 + q, y = 0;
-        if (valid && g < n) {
-          int m = mods[g];
-          float mi = minvs[g];
-          y = mod_exact((int)ap[(i64)g * ldg] * invs[g], m, mi);
-          y -= (y > (m >> 1)) ? m : 0;
-          ks += (float)y * mi;
+      for (int q = 0; q < 32; q++) av[q] = (valid && g32 + q < n) ? (int)__ldcs(ap + (i64)(g32 + q) * ldg) : 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        u32 ph[4], pl[4];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+          const int g = g32 + 16 * h + q;
+          int y = 0;
+          if (valid && g < n) {
+            const int m = TB.m[g];
+            const float mi = TB.minv[g];
+            y = mod_exact(av[16 * h + q] * TB.inv[g], m, mi);
+            y -= (y > (m >> 1)) ? m : 0;
+            ks += (float)y * mi;
+          }
+          int yl = ((y + 64) & 127) - 64, yh = (y - yl) >> 7;
+          if ((q & 3) == 0) ph[q >> 2] = pl[q >> 2] = 0;
+          ph[q >> 2] |= (u32)(yh & 255) << (8 * (q & 3));
+          pl[q >> 2] |= (u32)(yl & 255) << (8 * (q & 3));
         }
-        int yl = ((y + 64) & 127) - 64, yh = (y - yl) >> 7;
-        if ((q & 3) == 0) ph[q >> 2] = pl[q >> 2] = 0;
-        ph[q >> 2] |= (u32)(yh & 255) << (8 * (q & 3));
-        pl[q >> 2] |= (u32)(yl & 255) << (8 * (q & 3));
+        const int g16 = g32 + 16 * h;
+        int kt = g16 >> 7, chunk = (g16 & 127) >> 4;
+        *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+        *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
       }
-      int kt = g16 >> 7, chunk = (g16 & 127) >> 4;
-      *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-      *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
     }
     const i64 kq = (i64)__float2int_rd(ks + 0.5f);
     fence_proxy_async_smem();
@@ -187,7 +208,8 @@ template <int MODE>
 int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rpb,
                const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st) {
   const CtxDev& d = c->d;
-  size_t smem = 1024 + 1024 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
+  if (d.n > kNmax) return SDPV_EINVAL;
+  size_t smem = 1024 + 4096 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
   if (smem > 227 * 1024) return SDPV_EINVAL;
   static bool attr_set[64] = {};
   static size_t attr_val[64] = {};

@@ -4,7 +4,7 @@
 // i.e. 2^14 Ahi Bhi^T + 2^7 (Ahi Blo^T + Alo Bhi^T) + Alo Blo^T  (sdpvibe/rns.py:106-137,
 // sdpvibe/batched.py:96-162).
 //
-// One CTA computes a 128 x 128 output tile of one (modulus, block):
+// Persistent: one CTA per SM loops over the work items (128 x 128 output tile, block, modulus); per item:
 //   * warp 0 (one lane) streams 128-byte K slices of Ahi, Alo, Bhi, Blo with TMA (128-byte swizzle,
 //     out-of-range rows / K zero filled) into a 3-stage shared-memory ring;
 //   * warp 1 (one lane) issues per 32-byte K step two tcgen05.mma kind::i8 of M=128, N=256:
@@ -16,7 +16,9 @@
 //   * warps 2-9 (two per TMEM lane quarter, 64 columns each) read hh, hx = hl + lh and ll per entry
 //     from TMEM (one row per thread, old residues prefetched while the MMAs run), form
 //     (hh mod m) 2^14 + (hx mod m) 2^7 + ll + old (exact in int32 for K <= 65536) and store its
-//     canonical residue back, 16 bytes at a time where the row stride allows.
+//     canonical residue back, 16 bytes at a time where the row stride allows.  As soon as an item's
+//     accumulators are in registers the epilogue releases TMEM (mbarrier), so the next item's MMAs run
+//     while it reduces and stores; the producer streams the next item's slices through the same ring.
 // int32 accumulation is exact for K <= 65536 (|hh|, |hl + lh| <= K 2^14).
 // Syrk mode (Gram): B = A, only lower-triangle tiles are scheduled and only entries i >= j written.
 #include <mutex>
@@ -29,11 +31,27 @@ constexpr int kStages = 3;
 constexpr u32 kSlice = 128 * 128;            // one operand slice: 128 rows x 128 bytes
 constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue warps
 
+constexpr int kStg = 130;                   // staging row pitch (int16): 65 words, conflict-free by row
+
 struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
-  u64 full[kStages], empty[kStages], acc_full;
+  int16_t stg[128][kStg];                   // epilogue staging of one output tile (coalesced global I/O)
+  u64 full[kStages], empty[kStages], acc_full, tmem_empty;
   u32 tmem_slot;
+  int abort;
 };
+
+// Named barrier 1 over the 256 epilogue threads; the _or form returns the OR of pred over them.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ bool epi_sync_or(bool pred) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, 1, 256, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((int)pred)
+      : "memory");
+  return r != 0;
+}
 
 __device__ __forceinline__ void tile_of(int t, int mode, int ntn, int& tm, int& tn) {
   if (mode == 0) {
@@ -53,14 +71,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
-                    unsigned* __restrict__ err) {
+                    i64 tiles, i64 nitems, bool fresh, unsigned* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   GemmSmem& S = *reinterpret_cast<GemmSmem*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int tm, tn;
-  tile_of(blockIdx.x, mode, ntn, tm, tn);
-  const int b = blockIdx.y, g = blockIdx.z;
-  const int m0 = tm * 128, n0 = tn * 128;
   const int nk = (int)((KC + 127) / 128);
 
   if (tid == 0) {
@@ -69,6 +83,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&S.empty[s], 1);
     }
     mbar_init(&S.acc_full, 1);
+    mbar_init(&S.tmem_empty, 8);                // one arrival per epilogue warp
+    S.abort = 0;
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -79,106 +95,215 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc_fence_after();
   const u32 tmem = S.tmem_slot;
 
+  // Work items (tile, block, modulus), round robin over the CTAs; item = (g * nb + b) * tiles + t.
   if (warp == 0) {
     if (lane == 0) {
-      for (int kb = 0; kb < nk; kb++) {
-        int s = kb % kStages;
-        if (kb >= kStages && !mbar_wait(&S.empty[s], ((kb / kStages) - 1) & 1, err)) break;
-        mbar_expect_tx(&S.full[s], 4 * kSlice);
-        int kx = kb * 128;
-        tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
-        tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
-        tma_load_4d(S.stage[s][2], &mBh, &S.full[s], kx, n0, b, g);
-        tma_load_4d(S.stage[s][3], &mBl, &S.full[s], kx, n0, b, g);
+      u32 kbg = 0;                              // k-blocks issued by this CTA so far (ring position)
+      for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
+        const i64 t = item % tiles, bg = item / tiles;
+        const int b = (int)(bg % nb), g = (int)(bg / nb);
+        int tm, tn;
+        tile_of((int)t, mode, ntn, tm, tn);
+        const int m0 = tm * 128, n0 = tn * 128;
+        for (int kb = 0; kb < nk; kb++, kbg++) {
+          const u32 s = kbg % kStages;
+          if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
+            *(volatile int*)&S.abort = 1;
+            break;
+          }
+          mbar_expect_tx(&S.full[s], 4 * kSlice);
+          const int kx = kb * 128;
+          tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
+          tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
+          tma_load_4d(S.stage[s][2], &mBh, &S.full[s], kx, n0, b, g);
+          tma_load_4d(S.stage[s][3], &mBl, &S.full[s], kx, n0, b, g);
+        }
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const u32 idesc = idesc_i8(128, 256), idesc128 = idesc_i8(128, 128);
-      bool ok = true;
-      for (int kb = 0; kb < nk && ok; kb++) {
-        int s = kb % kStages;
-        if (!mbar_wait(&S.full[s], (kb / kStages) & 1, err)) {
-          ok = false;
+      u32 kbg = 0, li = 0;
+      for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
+        // the epilogue must have read the previous item's accumulators out of TMEM
+        if (li > 0 && !mbar_wait(&S.tmem_empty, (li - 1) & 1, err)) {
+          *(volatile int*)&S.abort = 1;
           break;
         }
         tc_fence_after();
-        u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
-#pragma unroll
-        for (int ks = 0; ks < 4; ks++) {
-          u64 bd = sdesc_sw128(bh + 32 * ks);
-          if ((kb | ks) == 0) {
-            mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                         // hh | hl
-            mma_i8(tmem + 256, sdesc_sw128(al), sdesc_sw128(bh + kSlice), idesc128, 0u);  // ll
-            mma_i8(tmem + 128, sdesc_sw128(al), bd, idesc128, 1u);                      // hl += lh
-          } else {
-            mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
-            mma_i8(tmem + 128, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+        bool ok = true;
+        for (int kb = 0; kb < nk; kb++, kbg++) {
+          const u32 s = kbg % kStages;
+          if (!mbar_wait(&S.full[s], (kbg / kStages) & 1, err)) {
+            ok = false;
+            break;
           }
+          tc_fence_after();
+          u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
+#pragma unroll
+          for (int ks = 0; ks < 4; ks++) {
+            u64 bd = sdesc_sw128(bh + 32 * ks);
+            if ((kb | ks) == 0) {
+              mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                             // hh | hl
+              mma_i8(tmem + 256, sdesc_sw128(al), sdesc_sw128(bh + kSlice), idesc128, 0u);  // ll
+              mma_i8(tmem + 128, sdesc_sw128(al), bd, idesc128, 1u);                        // hl += lh
+            } else {
+              mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
+              mma_i8(tmem + 128, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+            }
+          }
+          mma_commit(&S.empty[s]);
         }
-        mma_commit(&S.empty[s]);
+        if (!ok) {
+          *(volatile int*)&S.abort = 1;
+          break;
+        }
+        mma_commit(&S.acc_full);
       }
-      mma_commit(&S.acc_full);
     }
   } else {
-    // Epilogue: warps 2..9 -> TMEM lane quarter (warp & 3), column half (warp - 2) / 4.
-    const int q = warp & 3, ch = (warp - 2) >> 2;
-    const i64 i = m0 + q * 32 + lane;                 // output row within the block
-    const int gg = g0 + g;
-    const int m = mods[gg], c14 = c14s[gg];
-    const float minv = minvs[gg];
-    int16_t* rowp = acc + ((i64)gg * nb * M + (i64)b * M + i) * ldc;
+    // Epilogue: warps 2..9 -> TMEM lane quarter (warp & 3), column half (warp - 2) / 4; one output row per
+    // thread.  Rows whose stride allows 16-byte access (vec) are read and written directly, 16 bytes per
+    // access; other strides go through the shared staging tile, one warp per row (coalesced).  With
+    // `fresh` the accumulator is known to be zero: old residues are not read.
+    const int q = warp & 3, ch = (warp - 2) >> 2, ew = warp - 2;
     const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
-    // the old residues do not depend on the products: load them before waiting for the MMAs
-    int16_t olds[2][32];
+    u32 li = 0;
+    for (i64 item = blockIdx.x; item < nitems; item += gridDim.x, li++) {
+      const i64 t = item % tiles, bg = item / tiles;
+      const int b = (int)(bg % nb), g = (int)(bg / nb);
+      int tm, tn;
+      tile_of((int)t, mode, ntn, tm, tn);
+      const int m0 = tm * 128, n0 = tn * 128;
+      const int gg = g0 + g;
+      const int m = mods[gg], c14 = c14s[gg];
+      const float minv = minvs[gg];
+      const i64 rowbase = (i64)gg * nb * M + (i64)b * M + m0;       // acc row of tile row 0
+      const int nrow = (int)(M - m0 < 128 ? M - m0 : 128), ncol = (int)(N - n0 < 128 ? N - n0 : 128);
+      const int rrow = q * 32 + lane;
+      const i64 i = m0 + rrow;                                      // output row within the block
+      int16_t* rowp = acc + (rowbase + rrow) * ldc;
+      u32 olds[2][16];                                              // old residues of this row, in pairs
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
-      const i64 nc = n0 + 64 * ch + 32 * c;
-      const bool full = vec && i < M && nc + 32 <= N && (mode == 0 || nc + 31 <= i);
-      if (full) {
+      for (int c = 0; c < 2; c++)
 #pragma unroll
-        for (int v4 = 0; v4 < 4; v4++)
-          *reinterpret_cast<uint4*>(olds[c] + 8 * v4) = reinterpret_cast<const uint4*>(rowp + nc)[v4];
-      } else {
+        for (int j = 0; j < 16; j++) olds[c][j] = 0;
+      if (!fresh) {
+        if (vec) {
 #pragma unroll
-        for (int j = 0; j < 32; j++)
-          olds[c][j] = (i < M && nc + j < N && (mode == 0 || nc + j <= i)) ? rowp[nc + j] : (int16_t)0;
+          for (int c = 0; c < 2; c++) {
+            const int nc = n0 + 64 * ch + 32 * c;
+            const bool full = rrow < nrow && nc + 32 <= N && (mode == 0 || nc + 31 <= i);
+            if (full) {
+#pragma unroll
+              for (int v4 = 0; v4 < 4; v4++) {
+                const uint4 x = reinterpret_cast<const uint4*>(rowp + nc)[v4];
+                olds[c][4 * v4] = x.x;
+                olds[c][4 * v4 + 1] = x.y;
+                olds[c][4 * v4 + 2] = x.z;
+                olds[c][4 * v4 + 3] = x.w;
+              }
+            } else if (rrow < nrow) {
+              for (int j = 0; j < 32; j++)
+                if (nc + j < N && (mode == 0 || nc + j <= i))
+                  olds[c][j >> 1] |= ((u32)(uint16_t)rowp[nc + j]) << (16 * (j & 1));
+            }
+          }
+        } else {
+          epi_sync();                                    // the previous tile has left the staging area
+          for (int r0 = ew; r0 < nrow; r0 += 32) {       // 4 rows x 4 column groups of loads in flight
+            int16_t v[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const int r = r0 + 8 * u;
+              const int jmax = r >= nrow ? 0 : (mode == 0 ? ncol : min(ncol, m0 + r - n0 + 1));
+              const int16_t* src = acc + (rowbase + r) * ldc + n0;
+#pragma unroll
+              for (int w = 0; w < 4; w++) v[u][w] = (lane + 32 * w < jmax) ? src[lane + 32 * w] : (int16_t)0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+              for (int w = 0; w < 4; w++)
+                if (r0 + 8 * u < nrow) S.stg[r0 + 8 * u][lane + 32 * w] = v[u][w];
+          }
+          epi_sync();
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+              olds[c][j] = *reinterpret_cast<const u32*>(&S.stg[rrow][64 * ch + 32 * c + 2 * j]);
+        }
       }
-    }
-    const bool ok = mbar_wait(&S.acc_full, 0, err);
-    tc_fence_after();
+      const bool ok_me = mbar_wait(&S.acc_full, li & 1, err);
+      const bool fail = epi_sync_or(!ok_me);             // uniform over the epilogue warps
+      if (fail) break;
+      tc_fence_after();
+      u32 outp[2][16];
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
-      u32 hh[32], hx[32], ll[32];
-      u32 base = tmem + ((u32)(q * 32) << 16) + 64 * ch + 32 * c;
-      tmem_ld32(base, hh);
-      tmem_ld32(base + 128, hx);
-      tmem_ld32(base + 256, ll);
-      tmem_ld_wait();
-      if (!ok || i >= M) continue;
-      const i64 nc = n0 + 64 * ch + 32 * c;
-      if (nc >= N) continue;
-      const bool full = vec && nc + 32 <= N && (mode == 0 || nc + 31 <= i);
-      int16_t* old = olds[c];
+      for (int c = 0; c < 2; c++) {
+        u32 hh[32], hx[32], ll[32];
+        u32 base = tmem + ((u32)(q * 32) << 16) + 64 * ch + 32 * c;
+        tmem_ld32(base, hh);
+        tmem_ld32(base + 128, hx);
+        tmem_ld32(base + 256, ll);
+        tmem_ld_wait();
+        if (c == 1) {                                   // accumulators read: the next item's MMAs may start
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&S.tmem_empty);
+        }
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        // (hh mod m) and (hx mod m) as |r| <= m/2 + m/300 representatives, then the canonical residue
-        int a = (int)hh[j], x = (int)hx[j];
-        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
-        int v = ra * c14 + rx * 128 + (int)ll[j] + (int)old[j];
-        int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-        r += (r < 0) ? m : 0;
-        r -= (r >= m) ? m : 0;
-        old[j] = (int16_t)r;
+        for (int j2 = 0; j2 < 16; j2++) {
+          u32 pair = 0;
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int j = 2 * j2 + h;
+            // (hh mod m) and (hx mod m) as |r| <= m/2 + m/300 representatives, then the canonical residue
+            const int old = (int)(int16_t)(olds[c][j2] >> (16 * h));
+            int a = (int)hh[j], x = (int)hx[j];
+            int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+            int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+            int v = ra * c14 + rx * 128 + (int)ll[j] + old;
+            int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+            r += (r < 0) ? m : 0;
+            r -= (r >= m) ? m : 0;
+            pair |= ((u32)r & 0xffffu) << (16 * h);
+          }
+          outp[c][j2] = pair;
+        }
       }
-      if (full) {
+      if (vec) {
+        if (rrow < nrow) {
 #pragma unroll
-        for (int v4 = 0; v4 < 4; v4++)
-          reinterpret_cast<uint4*>(rowp + nc)[v4] = *reinterpret_cast<const uint4*>(old + 8 * v4);
+          for (int c = 0; c < 2; c++) {
+            const int nc = n0 + 64 * ch + 32 * c;
+            if (nc >= N) continue;
+            const bool full = nc + 32 <= N && (mode == 0 || nc + 31 <= i);
+            if (full) {
+#pragma unroll
+              for (int v4 = 0; v4 < 4; v4++)
+                reinterpret_cast<uint4*>(rowp + nc)[v4] =
+                    make_uint4(outp[c][4 * v4], outp[c][4 * v4 + 1], outp[c][4 * v4 + 2], outp[c][4 * v4 + 3]);
+            } else {
+              for (int j = 0; j < 32; j++)
+                if (nc + j < N && (mode == 0 || nc + j <= i)) rowp[nc + j] = (int16_t)(outp[c][j >> 1] >> (16 * (j & 1)));
+            }
+          }
+        }
       } else {
-        for (int j = 0; j < 32; j++)
-          if (nc + j < N && (mode == 0 || nc + j <= i)) rowp[nc + j] = old[j];
+        epi_sync();                                      // (fresh: the previous tile's stores are done)
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+          for (int j2 = 0; j2 < 16; j2++)
+            *reinterpret_cast<u32*>(&S.stg[rrow][64 * ch + 32 * c + 2 * j2]) = outp[c][j2];
+        epi_sync();
+        for (int r = ew; r < nrow; r += 8) {
+          int16_t* dst = acc + (rowbase + r) * ldc + n0;
+          const int jmax = mode == 0 ? ncol : min(ncol, m0 + r - n0 + 1);
+          for (int j = lane; j < jmax; j += 32) dst[j] = S.stg[r][j];
+        }
       }
     }
   }
@@ -208,8 +333,10 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
                              const int8_t* Blo, int64_t a_stride, int64_t b_stride, int16_t* acc, int64_t ldc, int g0,
                              int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream) {
   if (!c || g0 < 0 || G < 1 || g0 + G > c->d.n || nb < 1 || M < 0 || N < 0 || KC < 0 || KC > 65536 ||
-      (KC & 15) || (mode != 0 && mode != 1) || nb > 65535 || G > 65535)
+      (KC & 15) || (mode & ~3) || nb > 65535 || G > 65535)
     return SDPV_EINVAL;
+  const bool fresh = (mode & 2) != 0;                  // accumulator known to be zero: overwrite
+  mode &= 1;
   if (mode == 1) {
     Bhi = Ahi;
     Blo = Alo;
@@ -236,9 +363,13 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
   if (tiles > 0x7fffffff) return SDPV_EINVAL;
-  dim3 grid((unsigned)tiles, (unsigned)nb, (unsigned)G);
-  rns_gemm_kernel<<<grid, kThreads, smem, sdpv::as_stream(stream)>>>(
-      mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, nb, M, N, KC, mode, ntn,
-      sdpv::device_error_word());
+  const i64 nitems = tiles * nb * G;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);     // one resident CTA per SM, items looped
+  rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+      mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, nb, M, N, KC, mode, ntn, tiles, nitems,
+      fresh, sdpv::device_error_word());
   return sdpv::launch_status();
 }

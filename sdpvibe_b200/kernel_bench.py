@@ -1,7 +1,8 @@
 """Per-kernel timing of the multiprecision hot path on one GPU (CUDA events, after warm-up).
 
   python -m sdpvibe_b200.kernel_bench --kernel syrk --N 274 --K 7000 --L 27 --reps 20
-  kernels: residues | gemm | syrk | crt | mpfgemm | cholsolve (batched Cholesky + solve over uneven blocks)
+  kernels: residues | gemm | syrk | crt | mpfgemm | bgemm (--nb stacked blocks) | cholsolve (batched
+  Cholesky + solve over uneven blocks)
 
 Inputs are seeded random limb planes / residues of the given shape; rates are algorithmic (the
 reference's operation counts: moduli x 4 digit products x 2 ops per multiply-add; decomposition
@@ -106,7 +107,8 @@ def main():
     from . import mpf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve"))
+    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve", "bgemm"))
+    ap.add_argument("--nb", type=int, default=1, help="bgemm: number of stacked blocks")
     ap.add_argument("--blocks", type=int, default=600, help="cholsolve: number of SPD blocks")
     ap.add_argument("--nmin", type=int, default=8)
     ap.add_argument("--nmax", type=int, default=160)
@@ -144,6 +146,20 @@ def main():
                 ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc), a.reps, a.warmup)
                 ops = R.n * 8 * a.M * a.N * a.K
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12)
+    elif a.kernel == "bgemm":
+        # batched residue GEMM of nb stacked blocks (M x K) (N x K), as the Cholesky/trsm recursion issues
+        X = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.nb * a.M, a.K), dtype=np.int64)
+                             .astype(np.int32)).to(dev)
+        Y = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.nb * a.N, a.K), dtype=np.int64)
+                             .astype(np.int32)).to(dev)
+        Ah, Al = R.residues(X, 0, a.K, spread=True)
+        Bh, Bl = R.residues(Y, 0, a.K, spread=True)
+        acc = torch.zeros((R.n, a.nb * a.M, a.N), dtype=torch.int16, device=dev)
+        ts = _events(lambda: R.accumulate(Ah, Al, Bh, Bl, acc, nb=a.nb), a.reps, a.warmup)
+        tr = _events(lambda: R.residues(X, 0, a.K, spread=True), a.reps, a.warmup)
+        ops = R.n * 8 * a.nb * a.M * a.N * a.K
+        out.update(nb=a.nb, ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12,
+                   items=((a.M + 127) // 128) * ((a.N + 127) // 128) * a.nb * R.n, ms_residues_A=min(tr))
     elif a.kernel == "cholsolve":
         out.update(_cholsolve(a, rng))
     elif a.kernel == "crt":

@@ -376,10 +376,10 @@ def gemm(A, B, transA=False, transB=False):
     cB = _row_exponents(top_max(B, over_rows=not transB), L)        # (nb, N)
     Bm = aligned(B, cB, per_col=not transB, transpose=not transB)  # (L, nb, N, K)
     R = ctx(L)
-    acc = torch.zeros((R.n, nb * M, N), dtype=torch.int16, device=dev)
+    acc = (torch.empty if K else torch.zeros)((R.n, nb * M, N), dtype=torch.int16, device=dev)
     if K:
         from .mpmat import residue_product
-        residue_product(R, Am.view(L, nb * M, K), Bm.view(L, nb * N, K), acc, nb=nb)
+        residue_product(R, Am.view(L, nb * M, K), Bm.view(L, nb * N, K), acc, nb=nb, fresh=True)
     Om, Oe = R.crt_norm(acc, N, 0, N, nb * M, rA.reshape(-1), cB, L, rows_per_block=M)
     return MPF(Om.view(L, nb, M, N), Oe.view(nb, M, N))
 

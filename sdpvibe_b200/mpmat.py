@@ -182,8 +182,9 @@ def ctx(L):
     return _ctx[key]
 
 
-def residue_product(R, Av, Bv, acc, nb=1, syrk=False):
-    """acc += residues of the exact products of nb stacked blocks: Av (L, nb*M, K), Bv (L, nb*N, K)."""
+def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False):
+    """acc += residues of the exact products of nb stacked blocks: Av (L, nb*M, K), Bv (L, nb*N, K).
+    fresh: acc holds no data yet (the first K chunk overwrites instead of adding)."""
     K = Av.shape[2]
     rows = Av.shape[1] + (0 if syrk else Bv.shape[1])
     per_mod = rows * min(K, KC_MAX) * 2
@@ -193,11 +194,12 @@ def residue_product(R, Av, Bv, acc, nb=1, syrk=False):
         for g0 in range(0, R.n, GR):
             G = min(GR, R.n - g0)
             Ah, Al = R.residues(Av, k0, kk, g0, G, spread=True)
+            first = fresh and k0 == 0
             if syrk:
-                R.accumulate(Ah, Al, None, None, acc, g0, nb=nb, syrk=True)
+                R.accumulate(Ah, Al, None, None, acc, g0, nb=nb, syrk=True, fresh=first)
             else:
                 Bh, Bl = R.residues(Bv, k0, kk, g0, G, spread=True)
-                R.accumulate(Ah, Al, Bh, Bl, acc, g0, nb=nb)
+                R.accumulate(Ah, Al, Bh, Bl, acc, g0, nb=nb, fresh=first)
             del Ah, Al
 
 
@@ -212,10 +214,13 @@ def gemm_nt(A, Bt, out_exp="col", kc=4096, colblock=None, bt_rowexp=None):
     R = ctx(L)
     eA = A.uniform_exp()
     e_in = (eA + bt_rowexp) if bt_rowexp is not None else eA + Bt.uniform_exp()
-    acc = torch.zeros((R.n, M, N), dtype=torch.int16, device=dev)
+    acc = (torch.empty if K else torch.zeros)((R.n, M, N), dtype=torch.int16, device=dev)
     same = A.limbs.data_ptr() == Bt.limbs.data_ptr() and M == N
     if K:
-        residue_product(R, A.limbs, Bt.limbs, acc, syrk=False) if not same else _same_product(R, A.limbs, acc)
+        if same:
+            _same_product(R, A.limbs, acc)
+        else:
+            residue_product(R, A.limbs, Bt.limbs, acc, syrk=False, fresh=True)
     return _crt_round(acc, e_in, out_exp, L)
 
 
@@ -225,7 +230,7 @@ def _same_product(R, X, acc):
     for k0 in range(0, K, KC_MAX):
         kk = min(KC_MAX, K - k0)
         Ah, Al = R.residues(X, k0, kk, spread=True)
-        R.accumulate(Ah, Al, Ah, Al, acc)
+        R.accumulate(Ah, Al, Ah, Al, acc, fresh=(k0 == 0))
 
 
 def _crt_round(acc, e_in, out_exp, L, colblock=None):

@@ -79,9 +79,10 @@ class RNS:
         return Rhi, Rlo
 
     # ---- step 2: accumulate residues of A @ Bt^T (sdpvibe/rns.py:217-224)
-    def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False):
+    def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False, fresh=False):
         """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows.
-        acc may have padded rows (acc.shape[2] >= N): its row stride is passed to the kernel."""
+        acc may have padded rows (acc.shape[2] >= N): its row stride is passed to the kernel.  fresh: the
+        updated entries are overwritten (acc's content there is taken as zero and not read)."""
         G, Mt, KC = Ahi.shape
         M = Mt // nb
         N = M if syrk else Bhi.shape[1] // nb
@@ -91,7 +92,7 @@ class RNS:
             assert t.stride(2) == 1 and t.stride(1) == KC, "residue planes must have packed rows"
         _lib.call("sdpv_rns_gemm", self._h, _lib.ptr_strided(Ahi), _lib.ptr_strided(Alo), _lib.ptr_strided(Bhi),
                   _lib.ptr_strided(Blo), Ahi.stride(0), Bhi.stride(0), _lib.ptr(acc), acc.stride(1), g0, G, nb, M, N,
-                  KC, 1 if syrk else 0, _lib.stream())
+                  KC, (1 if syrk else 0) | (2 if fresh else 0), _lib.stream())
 
     # ---- step 3: CRT of a block of entries (sdpvibe/rns.py:227-245)
     def crt_block(self, acc, N, j0, w, rows):
