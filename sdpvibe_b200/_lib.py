@@ -69,7 +69,9 @@ def lib():
 
 
 def stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    """torch's current stream on the current device, as a cudaStream_t (the direct C lookups: the
+    torch.cuda.current_stream() wrapper costs more than a small kernel launch)."""
+    return ctypes.c_void_p(torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice()))
 
 
 def ptr(t):

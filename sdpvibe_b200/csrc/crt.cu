@@ -126,9 +126,12 @@ __global__ void __launch_bounds__(kThreads)
     fence_proxy_async_smem();
     __syncthreads();
 
-    // ---- digit chunks: MMA, then carry into words
+    // ---- digit chunks: MMA, then carry into words (crt_block streams them straight out, tracking the
+    //      highest word that differs from each possible sign extension for the bit length)
     i64 carry = 0;
     int nw = 0;
+    int hz = -1, ho = -1;                              // highest word != 0, != 0xffffffff
+    u32 hzv = 0, hov = 0, wtop = 0;
     for (int ch = 0; ch < nchunk; ch++) {
       if (tid == 0) {
         tc_fence_after();
@@ -160,7 +163,16 @@ __global__ void __launch_bounds__(kThreads)
             i64 z = 128 * (i64)(int)zh[j + u] + (i64)(int)zl[j + u] - kq * (i64)md[t0 + u];
             v += z << (8 * u);
           }
-          words[nw++] = (u32)v;
+          const u32 wv = (u32)v;
+          if (MODE == 0) {
+            if (valid) out[(i64)nw * B + e] = (int32_t)wv;
+            if (wv != 0u) hz = nw, hzv = wv;
+            if (wv != 0xffffffffu) ho = nw, hov = wv;
+            wtop = wv;
+          } else {
+            words[nw] = wv;
+          }
+          nw++;
           carry = v >> 32;
         }
       }
@@ -171,17 +183,11 @@ __global__ void __launch_bounds__(kThreads)
     // ---- outputs
     if (valid) {
       if (MODE == 0) {
-        for (int k = 0; k < W; k++) out[(i64)k * B + e] = (int32_t)words[k];
-        u32 ext = (words[W - 1] >> 31) ? 0xffffffffu : 0u;
-        i64 bl = 0;
-        for (int k = W - 1; k >= 0; k--) {
-          u32 x = words[k] ^ ext;
-          if (x) {
-            bl = 32 * (i64)k + 32 - __clz(x);
-            break;
-          }
-        }
-        out2[e] = bl;
+        // bit length of v (v >= 0) or of ~v (v < 0): the highest word differing from the extension
+        const bool ng = (wtop >> 31) != 0;
+        const int k = ng ? ho : hz;
+        const u32 x = ng ? ~hov : hzv;
+        out2[e] = k < 0 ? 0 : 32 * (i64)k + 32 - __clz(x);
       } else {
         bool ng = words[W - 1] >> 31;
         if (ng) neg_words(words, W);

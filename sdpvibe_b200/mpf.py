@@ -480,7 +480,7 @@ class Chol:
         self.nb, self.n, self.L, self.bt, self.refine = nb, n, L, bt, refine
         idx = torch.arange(n, device=dev)
         tpd = _top(A)[:, idx, idx]                                  # (nb, n)
-        if bool((A.m[-1][:, idx, idx] < 0).any()) or bool((tpd <= EZ // 2).any()):
+        if bool(((A.m[-1][:, idx, idx] < 0) | (tpd <= EZ // 2)).any()):          # one host sync
             raise ValueError("matrix is not positive definite (diagonal)")
         k = torch.div(tpd + 1, 2, rounding_mode="floor")            # A_ii < 2^(2k)
         self.k = k
