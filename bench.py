@@ -463,7 +463,7 @@ def run_solver(args, rank, world, local_rank):
     names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
              "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
-    tr = _trace.Trace(timed=names)
+    tr = _trace.Trace(timed=names)              # graph replays are timed whole, as "graph_replay"
     warm = max(args.warmup, 1)
     total_it = warm + args.steps
     with ClockSampler(local_rank) as clk, tr:
@@ -492,7 +492,7 @@ def run_solver(args, rank, world, local_rank):
             "per_iteration_s": per_it, "build_s": t_build,
             "last_row": {k: (mp.nstr(v, 6) if isinstance(v, mp.mpf) else v) for k, v in last.items()},
             "phase_s_per_iter": {k: v / total_it for k, v in sol.timer.totals().items()},
-            "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / total_it for k in names if tr.launches[k]},
+            "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / total_it for k in sorted(tr.events)},
             "gpu_launches": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
             "eig_refined": sol.eig_refined, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)

@@ -46,9 +46,24 @@ def before(name):
     if t is None or name in NON_LAUNCH:
         return None
     t.launches[name] += 1
-    if name in t.timed:
+    if name in t.timed and not torch.cuda.is_current_stream_capturing():
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         t.events[name].append((a, b))
         return b
     return None
+
+
+def replay(launches):
+    """A CUDA graph of recorded library launches is about to be replayed: count them, and time the replay
+    as "graph_replay" when the active trace times anything.  Returns the end event to record, or None."""
+    t = _active
+    if t is None:
+        return None
+    t.launches.update(launches)
+    if not t.timed:
+        return None
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    t.events["graph_replay"].append((a, b))
+    return b

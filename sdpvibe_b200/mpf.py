@@ -14,7 +14,7 @@ import mpmath as mp
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, graphs
 from .limbops import shift_round, bitlen_words
 from .mpmat import ctx, KC_MAX, RES_BUDGET
 from .rns import dev
@@ -497,7 +497,8 @@ class Chol:
             onefx = shift_round(one.m, torch.tensor([efx - int(one.e[0])], device=dev), L)[:, 0]
             ii = torch.arange(n, npad, device=dev)
             P[:, :, ii, ii] = onefx[:, None, None]
-        self.Lt, self.tiles = bchol(BMP(P, efx), bt, refine)
+        self.Lt, self.tiles = graphs.run(("bchol", L, nb, npad, bt, refine, efx),
+                                         lambda ins: bchol(BMP(ins[0], efx), bt, refine), [P])
 
     def _to_bmp(self, B):
         from .batched import BMP
@@ -520,24 +521,31 @@ class Chol:
             return MPF(r.m[:, 0], r.e[0])
         return f(B)
 
+    def _solve(self, lower, B):
+        """L^-1 B (lower) or L^-T B on batched B, replayed as a CUDA graph for repeated shapes"""
+        from .batched import btrsm_left, btrsm_left_T
+        state = []
+        sk = graphs._flatten((self.Lt, self.tiles), state)
+
+        def fn(ins):
+            Bm, Be, k = ins[0], ins[1], ins[2]
+            Lt, tiles = graphs._rebuild(sk, iter(ins[3:]))
+            if lower:                                               # Lt^-1 (D B)
+                P = btrsm_left(Lt, self._to_bmp(MPF(Bm, Be).shift(-k[:, :, None])), tiles, self.bt,
+                               self.SOLVE_REFINE)
+                return self._from_bmp(P)
+            P = btrsm_left_T(Lt, self._to_bmp(MPF(Bm, Be)), tiles, self.bt, self.SOLVE_REFINE)
+            return self._from_bmp(P).shift(-k[:, :, None])            # D (Lt^-T B)
+        key = ("solve", lower, self.L, self.nb, self.n, self.npad, self.bt, self.SOLVE_REFINE, B.shape, sk)
+        return graphs.run(key, fn, [B.m.contiguous(), B.e.contiguous(), self.k] + state)
+
     def solve_lower(self, B):
         """L^-1 B = Lt^-1 (D B)"""
-        from .batched import btrsm_left
-
-        def f(B):
-            P = btrsm_left(self.Lt, self._to_bmp(B.shift(-self.k[:, :, None])), self.tiles, self.bt,
-                           self.SOLVE_REFINE)
-            return self._from_bmp(P)
-        return self._io(B, f)
+        return self._io(B, lambda B: self._solve(True, B))
 
     def solve_upper(self, B):
         """L^-T B = D (Lt^-T B)"""
-        from .batched import btrsm_left_T
-
-        def f(B):
-            P = btrsm_left_T(self.Lt, self._to_bmp(B), self.tiles, self.bt, self.SOLVE_REFINE)
-            return self._from_bmp(P).shift(-self.k[:, :, None])
-        return self._io(B, f)
+        return self._io(B, lambda B: self._solve(False, B))
 
     def solve(self, B):
         """A^-1 B"""

@@ -509,3 +509,45 @@ def test_tile_kernels_vs_oracle(sb, L, ill):
     _lib.call("sdpv_trinv_tiles", _lib.ptr(cu(Lw.view(np.int32))), _lib.ptr(RINV), _lib.ptr(X), _lib.ptr(S), nb, 32,
               WL, LF, _lib.stream())
     assert np.array_equal(np_(X).view(np.uint32), RX)
+
+
+def test_chol_graph_replay_matches_eager(sb):
+    """Chol + solves replayed from CUDA graphs (same shapes, new data each call) give the eager bits,
+    and a result stays valid while the same graph runs again."""
+    from sdpvibe_b200 import graphs
+    from sdpvibe_b200.mpf import MPF, Chol
+    rng = np.random.default_rng(77)
+    L, nb, n, nr = 26, 3, 70, 5
+
+    def case():
+        vals, exps = [], []
+        for b in range(nb):
+            G = rng.integers(-40, 41, size=(n, n)).astype(object)
+            A = G.dot(G.T) + np.eye(n, dtype=object) * (50 * n)
+            vals += [int(v) for v in A.reshape(-1)]
+            exps += [int(x) for x in rng.integers(-5, 6, size=n * n)]
+        m, e = O.mpf_norm(O.to_limbs(vals, L), np.array(exps, np.int64), L)
+        Bm, Be = _normal_mpf_np(rng, L, (nb, n, nr), -20, 20)
+        return MPF(cu(m.reshape(L, nb, n, n)), cu(e.reshape(nb, n, n))), MPF(cu(Bm), cu(Be))
+    cases = [case() for _ in range(3)]
+    graphs.clear()
+    graphs.ENABLED = False
+    try:
+        eager = []
+        for A, B in cases:
+            ch = Chol(A)
+            eager.append((np_(ch.Lt.limbs), ch.solve_lower(B), ch.solve(B)))
+    finally:
+        graphs.ENABLED = True
+    kept = []
+    for (A, B), (lt, lo, x) in zip(cases, eager):
+        ch = Chol(A)
+        got_lo, got_x = ch.solve_lower(B), ch.solve(B)
+        assert np.array_equal(np_(ch.Lt.limbs), lt)
+        for got, ref in ((got_lo, lo), (got_x, x)):
+            assert np.array_equal(np_(got.m), np_(ref.m)) and np.array_equal(np_(got.e), np_(ref.e))
+        kept.append((got_x, x))
+    for got, ref in kept:                           # earlier results untouched by later replays
+        assert np.array_equal(np_(got.m), np_(ref.m)) and np.array_equal(np_(got.e), np_(ref.e))
+    assert len(graphs._cache) >= 3
+    graphs.clear()
