@@ -31,6 +31,7 @@ constexpr int kStages = 3;
 constexpr u32 kSlice = 128 * 128;            // one operand slice: 128 rows x 128 bytes
 constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue warps
 
+constexpr int kMaxG = 128;                  // moduli per launch (more are split over launches)
 constexpr int kStg = 130;                   // staging row pitch (int16): 65 words, conflict-free by row
 
 struct GemmSmem {
@@ -39,6 +40,8 @@ struct GemmSmem {
   u64 full[kStages], empty[kStages], acc_full, tmem_empty;
   u32 tmem_slot;
   int abort;
+  float tminv[kMaxG];                       // this launch's moduli, staged once per CTA
+  int16_t tmod[kMaxG], tc14[kMaxG];
 };
 
 // Named barrier 1 over the 256 epilogue threads; the _or form returns the OR of pred over them.
@@ -70,7 +73,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
-                    const int32_t* __restrict__ c14s, int g0, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
+                    const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, unsigned* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   GemmSmem& S = *reinterpret_cast<GemmSmem*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
@@ -91,6 +94,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     tmem_alloc(&S.tmem_slot, 512);
     tmem_relinquish();
   }
+  for (int g = tid; g < G; g += kThreads) {              // moduli < 2^15
+    S.tmod[g] = (int16_t)mods[g0 + gofs + g];
+    S.tc14[g] = (int16_t)c14s[g0 + gofs + g];
+    S.tminv[g] = minvs[g0 + gofs + g];
+  }
   __syncthreads();
   tc_fence_after();
   const u32 tmem = S.tmem_slot;
@@ -101,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       u32 kbg = 0;                              // k-blocks issued by this CTA so far (ring position)
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
         const i64 t = item % tiles, bg = item / tiles;
-        const int b = (int)(bg % nb), g = (int)(bg / nb);
+        const int b = (int)(bg % nb), g = gofs + (int)(bg / nb);       // modulus plane of the operands
         int tm, tn;
         tile_of((int)t, mode, ntn, tm, tn);
         const int m0 = tm * 128, n0 = tn * 128;
@@ -175,9 +183,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       int tm, tn;
       tile_of((int)t, mode, ntn, tm, tn);
       const int m0 = tm * 128, n0 = tn * 128;
-      const int gg = g0 + g;
-      const int m = mods[gg], c14 = c14s[gg];
-      const float minv = minvs[gg];
+      const int gg = g0 + gofs + g;
+      const int m = S.tmod[g], c14 = S.tc14[g];
+      const float minv = S.tminv[g];
       const i64 rowbase = (i64)gg * nb * M + (i64)b * M + m0;       // acc row of tile row 0
       const int nrow = (int)(M - m0 < 128 ? M - m0 : 128), ncol = (int)(N - n0 < 128 ? N - n0 : 128);
       const int rrow = q * 32 + lane;
@@ -363,13 +371,18 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
   if (tiles > 0x7fffffff) return SDPV_EINVAL;
-  const i64 nitems = tiles * nb * G;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);     // one resident CTA per SM, items looped
-  rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-      mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, nb, M, N, KC, mode, ntn, tiles, nitems,
-      fresh, sdpv::device_error_word());
-  return sdpv::launch_status();
+  for (int gofs = 0; gofs < G; gofs += kMaxG) {        // at most kMaxG moduli per launch
+    const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
+    const i64 nitems = tiles * nb * Gl;
+    const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);   // one resident CTA per SM, items looped
+    rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+        mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, tiles,
+        nitems, fresh, sdpv::device_error_word());
+    const int st = sdpv::launch_status();
+    if (st != SDPV_OK) return st;
+  }
+  return SDPV_OK;
 }
