@@ -30,9 +30,11 @@ struct CrtSmemHead {
 };
 
 constexpr int kNmax = 320;                  // moduli tables staged in shared memory (n <= 320)
+constexpr int kEmax = 640;                  // CRT digits staged in shared memory (E <= 640)
 struct CrtTables {
   int m[kNmax], inv[kNmax];
   float minv[kNmax];
+  int md[kEmax];
 };
 
 // Dynamic shared memory: [head (1 KB)] [Yh: ktc slices] [Yl: ktc slices] [Ct: Epad/128 * ktc slices]
@@ -47,7 +49,7 @@ __global__ void __launch_bounds__(kThreads)
   uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   CrtSmemHead& H = *reinterpret_cast<CrtSmemHead*>(base);
   CrtTables& TB = *reinterpret_cast<CrtTables*>(base + 64);
-  uint8_t* Yh = base + 4096;
+  uint8_t* Yh = base + 8192;
   uint8_t* Yl = Yh + (size_t)ktc * kSlice;
   uint8_t* Ct = Yl + (size_t)ktc * kSlice;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -69,6 +71,7 @@ __global__ void __launch_bounds__(kThreads)
     TB.inv[g] = g < n ? invs[g] : 0;
     TB.minv[g] = g < n ? minvs[g] : 1.f;
   }
+  for (int t = tid; t < kEmax; t += kThreads) TB.md[t] = t < E ? md[t] : 0;
   __syncthreads();
   tc_fence_after();
   const u32 tmem = H.tmem_slot;
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(kThreads)
           i64 v = carry;
 #pragma unroll
           for (int u = 0; u < 4; u++) {
-            i64 z = 128 * (i64)(int)zh[j + u] + (i64)(int)zl[j + u] - kq * (i64)md[t0 + u];
+            i64 z = 128 * (i64)(int)zh[j + u] + (i64)(int)zl[j + u] - kq * (i64)TB.md[t0 + u];
             v += z << (8 * u);
           }
           const u32 wv = (u32)v;
@@ -214,8 +217,8 @@ template <int MODE>
 int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rpb,
                const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st) {
   const CtxDev& d = c->d;
-  if (d.n > kNmax) return SDPV_EINVAL;
-  size_t smem = 1024 + 4096 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
+  if (d.n > kNmax || d.E > kEmax) return SDPV_EINVAL;
+  size_t smem = 1024 + 8192 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
   if (smem > 227 * 1024) return SDPV_EINVAL;
   static bool attr_set[64] = {};
   static size_t attr_val[64] = {};

@@ -168,7 +168,9 @@ def main():
         rexp = torch.zeros(a.M, dtype=torch.int64, device=dev)
         cexp = torch.zeros(a.N, dtype=torch.int64, device=dev)
         ts = _events(lambda: R.crt_norm(acc, a.N, 0, a.N, a.M, rexp, cexp, a.L - 1), a.reps, a.warmup)
-        out.update(ms=min(ts), ms_mean=float(np.mean(ts)), entries_per_s=a.M * a.N / (min(ts) * 1e-3))
+        tb = _events(lambda: R.crt_block(acc, a.N, 0, a.N, a.M), a.reps, a.warmup)
+        out.update(ms=min(ts), ms_mean=float(np.mean(ts)), entries_per_s=a.M * a.N / (min(ts) * 1e-3),
+                   ms_block=min(tb), block_entries_per_s=a.M * a.N / (min(tb) * 1e-3))
     else:
         L = a.L
 
