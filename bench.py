@@ -10,7 +10,11 @@ x 4 digit products x 2 ops x N(N+1)/2 x R per step, divided by the step time.  A
 mp-MAC/s.  `value` times the step with inputs resident in HBM; `e2e` times the same step through the
 public API with pinned host inputs copied in and Q copied out inside the timed region.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+The line also carries `sdp_solver`: the metric's other half, SDPB iterations (s/iteration) of the 768-bit
+Ising-structured SDP (300 blocks, N = 1000, L = 26) on the same GPU (`--workload solver` prints it as
+its own line; `--workload cholsolve` measures the batched Cholesky + solve configuration).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}] [--workload ...]
 Under torchrun each rank runs one replica (the Gram step has no cross-GPU exchange in scope);
 rank 0 prints one JSON line.
 """
@@ -322,6 +326,11 @@ def run_b200(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(R, os.cpu_count() or 1)
+    if world == 1 and not args.no_solver:
+        # the metric's other half: SDPB iterations of the 768-bit Ising-structured SDP on the same GPU
+        sv = solver_measurement(5, 1, local_rank)
+        line["sdp_solver"] = {k: sv[k] for k in ("metric", "value", "unit", "steps", "warmup", "per_iteration_s",
+                                                  "config", "kernel_s_per_iter", "gpu_launches", "clocks")}
     print(json.dumps(line), flush=True)
 
 
@@ -442,6 +451,12 @@ def run_solver(args, rank, world, local_rank):
     """SDPB iterations on the Ising-structured synthetic SDP: 300 blocks (dims 1/2/3 = 180/90/30,
     degree d ~ U[20,40], K = d+1), N = 1000, L = 26 (the 768-bit precision rule).  A step is one
     iteration; `--warmup` first iterations are excluded; metric s/iteration (lower is better)."""
+    line = solver_measurement(args.steps, args.warmup, local_rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def solver_measurement(steps, warmup, local_rank, world=1):
     import torch
     import mpmath as mp
     from sdpvibe_b200 import _trace
@@ -464,16 +479,14 @@ def run_solver(args, rank, world, local_rank):
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
              "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
     tr = _trace.Trace(timed=names)              # graph replays are timed whole, as "graph_replay"
-    warm = max(args.warmup, 1)
-    total_it = warm + args.steps
+    warm = max(warmup, 1)
+    total_it = warm + steps
     with ClockSampler(local_rank) as clk, tr:
         torch.cuda.synchronize()
         start = torch.cuda.Event(enable_timing=True)
         start.record()
         sol.run(max_iter=total_it, record=rec)
         torch.cuda.synchronize()
-    if rank != 0:
-        return
     ev = [start] + [m[1] for m in marks]
     per_it = [ev[i].elapsed_time(ev[i + 1]) * 1e-3 for i in range(len(ev) - 1)]
     timed = per_it[warm:]
@@ -495,7 +508,7 @@ def run_solver(args, rank, world, local_rank):
             "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / total_it for k in sorted(tr.events)},
             "gpu_launches": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
             "eig_refined": sol.eig_refined, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -505,6 +518,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-solver", action="store_true", help="gram: skip the SDP s/iteration measurement")
     ap.add_argument("--workload", choices=("gram", "cholsolve", "solver"), default="gram",
                     help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "
                          "solver: SDPB iterations (s/iter)")
