@@ -155,6 +155,12 @@ int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL,
 int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
                      int WL, int LF, void* stream);
 
+/* Triangular solve L y = v for nvec vectors of 32 entries with one factored 32 x 32 tile (Lt lower, RINV its
+ * pivot reciprocals), wide fixed point; V (nvec, 32, WL) is overwritten by y.  Replaces basecase.trsv_tile's
+ * trsv_warp (sdpvibe/basecase.py:228-245, 310-331). */
+int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* V, int64_t nvec, int bt, int WL, int LF,
+                    void* stream);
+
 /* Allocation-free sdpv_trinv_tiles, for callers that cannot allocate device memory at the point of the call
  * (their process has handed all device memory to another allocator, or the calling code must not allocate).
  * No counterpart in the reference.  The product scratch is a fixed 16 MiB array inside the library image

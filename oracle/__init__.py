@@ -243,6 +243,17 @@ def trinv_tiles(Lw, RINV, BT, WL, LF):
     return X
 
 
+def trsv_tiles(Lt, RINV, V, BT, WL, LF):
+    """basecase.py:228-245: y with L y = v for each vector of V (nvec, BT, WL) (one factored tile Lt
+    (BT, BT, WL), pivot reciprocals RINV (BT, WL)) -> Y (nvec, BT, WL)."""
+    Lt = _c(Lt, np.uint32); RINV = _c(RINV, np.uint32)
+    Y = np.array(V, np.uint32, copy=True)
+    nvec = Y.shape[0]
+    lib().or_trsv_tiles(_p(Lt), _p(RINV), _p(Y), ctypes.c_int64(nvec), ctypes.c_int(BT), ctypes.c_int(WL),
+                        ctypes.c_int(LF))
+    return Y
+
+
 def to_limbs(values, L):
     """Python ints -> (L, n) int32 limb planes (two's complement)."""
     return np.array([[((v >> (32 * k)) + (1 << 31)) % (1 << 32) - (1 << 31) for v in values]

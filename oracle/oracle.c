@@ -549,3 +549,21 @@ void or_trinv_tiles(const u32* Lt, const u32* RINV, u32* X, i64 nb, int BT, int 
     or_trinv_tile(Lt + (size_t)b * BT * BT * WL, RINV + (size_t)b * BT * WL, X + (size_t)b * BT * BT * WL, BT, WL,
                   LF);
 }
+
+/* basecase.py:228-245 (trsv_warp): solve L y = v for nvec vectors of BT entries with one factored tile
+ * (upper part of Lt ignored): for j in order, y_j = v_j r_j, then v_i -= l_ij y_j for i > j.  V (nvec, BT,
+ * WL) is overwritten by y. */
+void or_trsv_tiles(const u32* Lt, const u32* RINV, u32* V, i64 nvec, int BT, int WL, int LF) {
+  u32 p[256], t[256];
+  for (i64 w = 0; w < nvec; w++) {
+    u32* v = V + (size_t)w * BT * WL;
+    for (int j = 0; j < BT; j++) {
+      or_mulfx(p, v + (size_t)j * WL, RINV + (size_t)j * WL, 0, WL, LF);
+      for (int k = 0; k < WL; k++) v[(size_t)j * WL + k] = p[k];
+      for (int i = j + 1; i < BT; i++) {
+        or_mulfx(t, Lt + ((size_t)i * BT + j) * WL, p, 0, WL, LF);
+        sub_words(v + (size_t)i * WL, t, WL);
+      }
+    }
+  }
+}

@@ -145,7 +145,7 @@ def bchol_tile(A, LI=24, threads=256):
     LF, WL = L, L + LI
     F = 32 * LF
     Ws = brescale(A, -F, WL).limbs                                 # (WL, nb, b, b)
-    Lw, X = tile_factor(_soa_to_aos(Ws), WL, LF)                   # (nb, b, b, WL) each
+    Lw, X, _ = tile_factor(_soa_to_aos(Ws), WL, LF)                # (nb, b, b, WL) each
     Lout = brescale(BMP(_aos_to_soa(Lw), -F), e, L)
     Xs = _aos_to_soa(X)
     top = bitlen_words(Xs.reshape(WL, -1)).view(nb, b * b).amax(1) - F

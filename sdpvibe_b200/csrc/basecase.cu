@@ -666,6 +666,36 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
   }
 }
 
+
+// ---- batched triangular solve L y = v with one factored tile (sdpvibe/basecase.py:228-245): one warp per
+// vector, lane i owns v_i; for each j, lane j forms y_j = v_j r_j and broadcasts it, lanes i > j subtract
+// l_ij y_j.  V (nvec, 32, WL) is overwritten by y.
+__global__ void __launch_bounds__(kThreads) trsv_tiles_kernel(const u32* __restrict__ Lt, const u32* __restrict__ RINV,
+                                                              u32* __restrict__ V, i64 nvec, int WL, int LF) {
+  __shared__ u32 sp[kThreads / 32][WMAX];
+  const i64 w = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, ws = threadIdx.x >> 5;
+  if (w >= nvec) return;                                         // the whole warp leaves together
+  u32* vi = V + ((size_t)w * BT + lane) * WL;
+  for (int j = 0; j < BT; j++) {
+    if (lane == j) {
+      fx_mul(vi, vi, RINV + (size_t)j * WL, 0, WL, LF);
+      for (int k = 0; k < WL; k++) sp[ws][k] = vi[k];
+    }
+    __syncwarp();
+    if (lane > j) {
+      u32 t[WMAX];
+      fx_mul(t, Lt + ((size_t)lane * BT + j) * WL, sp[ws], 0, WL, LF);
+      i64 br = 0;
+      for (int k = 0; k < WL; k++) {
+        const i64 d = (i64)vi[k] - (i64)t[k] + br;
+        vi[k] = (u32)d;
+        br = d >> 32;
+      }
+    }
+    __syncwarp();
+  }
+}
 }  // namespace
 
 namespace {
@@ -759,5 +789,15 @@ extern "C" int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV
   int st = trinv_scratch_address(&scratch);
   if (st != SDPV_OK) return st;
   trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, scratch, WL, LF);
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* V, int64_t nvec, int bt, int WL,
+                               int LF, void* stream) {
+  if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || nvec < 0) return SDPV_EINVAL;
+  if (nvec == 0) return SDPV_OK;
+  const i64 blocks = (nvec * 32 + kThreads - 1) / kThreads;
+  if (blocks > 0x7fffffff) return SDPV_EINVAL;
+  trsv_tiles_kernel<<<(unsigned)blocks, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, V, nvec, WL, LF);
   return sdpv::launch_status();
 }

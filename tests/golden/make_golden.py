@@ -338,6 +338,56 @@ def case_basecase():
         save(f"basecase_L{L}", A=Am.limbs, L=Lg.limbs, Le=Lg.exp, X=Xg.limbs, Xe=Xg.exp)
 
 
+def _equilibrated_spd(rng, n, spread, L):
+    """tests/test_linalg.py:30-48 construction: A = V diag(2^-e_k) V^T (exact integers, e_k spread over
+    `spread` bits), equilibrated by powers of two, fixed point with exponent fx_exp(L) (diagonal < 1)."""
+    FX = -linalg.fx_exp(L)
+    V = [[rng.randint(-8, 8) for _ in range(n)] for _ in range(n)]
+    ek = [int(round(k * spread / (n - 1))) for k in range(n)]
+    emax = max(ek)
+    A = [[sum(V[i][k] * V[j][k] << (emax - ek[k]) for k in range(n)) for j in range(n)] for i in range(n)]
+    sh = [(A[i][i].bit_length() - 1) // 2 for i in range(n)]
+    out = []
+    for i in range(n):
+        row = []
+        for j in range(n):
+            s = FX - sh[i] - sh[j] - 1
+            v = A[i][j]
+            row.append(v << s if s >= 0 else (v + (1 << (-s - 1))) >> (-s))
+        out.append(row)
+    return mpmat.from_ints(out, -FX, L)
+
+
+def case_linalg():
+    # sdpvibe/linalg.py on one matrix: chol (substitution and tile-inverse panels, refinement), trsm_left
+    # (gemm and substitution leaves), chol_inv + trsm, and basecase.trsv_tile
+    rng = random.Random(29)
+    L, n, m = 8, 96, 5
+    A = _equilibrated_spd(rng, n, 60, L)
+    Bv = [[rng.randrange(-(1 << 200), 1 << 200) for _ in range(m)] for _ in range(n)]
+    B = mpmat.from_ints(Bv, -200, L)
+    B = mpmat.MP(B.limbs, torch.tensor([rng.randint(-6, 6) for _ in range(m)], dtype=torch.int64) - 200)
+    out = dict(Am=A.limbs, Ae=A.uniform_exp(), Bm=B.limbs, Be=B.exp)
+    Ls, ts = linalg.chol(A, tile_inverses=True, panel_leaf="subst")
+    out.update(Ls=Ls.limbs, Ls_e=Ls.uniform_exp())
+    Lg, tg = linalg.chol(A, tile_inverses=True, panel_leaf="gemm", refine=1)
+    out.update(Lg=Lg.limbs, Lg_e=Lg.uniform_exp())
+    for leaf in ("gemm", "subst"):
+        P = linalg.trsm_left(Ls, B, ts, leaf=leaf)
+        out.update({f"P_{leaf}_m": P.limbs, f"P_{leaf}_e": P.exp})
+    Lc, Xc = linalg.chol_inv(A)
+    out.update(Lc=Lc.limbs, Lc_e=Lc.uniform_exp(), Xc=Xc.limbs, Xc_e=Xc.uniform_exp())
+    P2 = linalg.trsm(Xc, B)
+    out.update(P2_m=P2.limbs, P2_e=P2.exp)
+    Vt = mpmat.from_ints([[rng.randrange(-(1 << 180), 1 << 180) for _ in range(32)] for _ in range(7)], 0, L)
+    ve = torch.tensor([rng.randint(-10, 10) for _ in range(7)], dtype=torch.int64)
+    Y, ye = basecase.trsv_tile(ts[0], Vt.limbs, ve)
+    Yf, yfe = basecase.trsv_tile(ts[0], Vt.limbs, ve, out_exp=-(32 * L - 40))
+    out.update(Vm=Vt.limbs, ve=ve, Ym=Y, ye=ye, Yfm=Yf, yfe=yfe,
+               t0_Lw=ts[0].Lw, t0_RINV=ts[0].RINV)
+    save("linalg_n96", **out)
+
+
 CASES = {k[5:]: v for k, v in globals().items() if k.startswith("case_")}
 
 if __name__ == "__main__":

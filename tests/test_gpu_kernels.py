@@ -551,3 +551,50 @@ def test_chol_graph_replay_matches_eager(sb):
         assert np.array_equal(np_(got.m), np_(ref.m)) and np.array_equal(np_(got.e), np_(ref.e))
     assert len(graphs._cache) >= 3
     graphs.clear()
+
+
+def test_trsv_tiles_vs_oracle(sb):
+    """sdpv_trsv_tiles (substitution with one factored tile, one warp per vector) against the oracle."""
+    from sdpvibe_b200 import _lib
+    rng = np.random.default_rng(5)
+    for L in (8, 26):
+        WL, LF = L + 24, L
+        W = _spd_tiles(rng, 1, L, False)
+        RA, RR = O.chol_tiles(W, 32, WL, LF)
+        tri = np.tril(np.ones((32, 32), bool))
+        Lw = np.where(tri[None, :, :, None], RA, 0).astype(np.uint32)[0]
+        V = rng.integers(0, 1 << 32, size=(9, 32, WL), dtype=np.uint64).astype(np.uint32)
+        V[..., LF + 1:] = np.where(V[..., LF:LF + 1] >> 31, np.uint32(0xffffffff), np.uint32(0))   # |v| < 2^32
+        ref = O.trsv_tiles(Lw, RR[0], V, 32, WL, LF)
+        Vd = cu(V.view(np.int32))
+        _lib.call("sdpv_trsv_tiles", _lib.ptr(cu(Lw.view(np.int32))), _lib.ptr(cu(RR[0].view(np.int32))),
+                  _lib.ptr(Vd), V.shape[0], 32, WL, LF, _lib.stream())
+        assert np.array_equal(np_(Vd).view(np.uint32), ref)
+
+
+@pytest.mark.skipif("linalg_n96" not in golden_names("linalg"), reason="fixture not generated")
+def test_linalg_golden(sb):
+    """linalg.chol (both panel leaves, refinement), trsm_left (both leaves), chol_inv + trsm and
+    basecase.trsv_tile bit-exact against the reference's own linalg run (tests/golden: linalg_n96)."""
+    from sdpvibe_b200 import linalg, basecase
+    from sdpvibe_b200.mpmat import MP
+    g = golden("linalg_n96")
+    A = MP(cu(g["Am"]), int(g["Ae"]))
+    B = MP(cu(g["Bm"]), cu(g["Be"]))
+    Ls, ts = linalg.chol(A, tile_inverses=True, panel_leaf="subst")
+    assert np.array_equal(np_(Ls.limbs), g["Ls"]) and Ls.uniform_exp() == int(g["Ls_e"])
+    Lg, _ = linalg.chol(A, tile_inverses=True, panel_leaf="gemm", refine=1)
+    assert np.array_equal(np_(Lg.limbs), g["Lg"]) and Lg.uniform_exp() == int(g["Lg_e"])
+    for leaf in ("gemm", "subst"):
+        P = linalg.trsm_left(Ls, B, ts, leaf=leaf)
+        assert np.array_equal(np_(P.limbs), g[f"P_{leaf}_m"]) and np.array_equal(np_(P.exp), g[f"P_{leaf}_e"]), leaf
+    Lc, Xc = linalg.chol_inv(A)
+    assert np.array_equal(np_(Lc.limbs), g["Lc"]) and Lc.uniform_exp() == int(g["Lc_e"])
+    assert np.array_equal(np_(Xc.limbs), g["Xc"]) and Xc.uniform_exp() == int(g["Xc_e"])
+    P2 = linalg.trsm(Xc, B)
+    assert np.array_equal(np_(P2.limbs), g["P2_m"]) and np.array_equal(np_(P2.exp), g["P2_e"])
+    assert np.array_equal(np_(ts[0].Lw).view(np.uint32), g["t0_Lw"].view(np.uint32))
+    Y, ye = basecase.trsv_tile(ts[0], cu(g["Vm"]), cu(g["ve"]))
+    assert np.array_equal(np_(Y), g["Ym"]) and np.array_equal(np_(ye), g["ye"])
+    Yf, yfe = basecase.trsv_tile(ts[0], cu(g["Vm"]), cu(g["ve"]), out_exp=-(32 * 8 - 40))
+    assert np.array_equal(np_(Yf), g["Yfm"]) and np.array_equal(np_(yfe), g["yfe"])
