@@ -288,11 +288,27 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_kernel(const u32* __rest
 // from shared-memory magnitudes.  Every product is the same truncated product (same columns, same kept
 // words), and sums of products are exact in WL words, so the results are bit-identical to the kernels above.
 constexpr int FW = 64;                    // fast path: WL <= FW
+constexpr int kThreadsS = 512;            // shared-memory kernels: 16 warps per tile
+constexpr int kWarpsS = kThreadsS / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct WarpScratch {                      // per-warp product scratch
   u32 xa[FW], xb[FW], acc[FW];
 };
+
+// c += d (96-bit)
+__device__ __forceinline__ void add96(u32& c0, u32& c1, u32& c2, u32 d0, u32 d1, u32 d2) {
+  asm("add.cc.u32 %0, %0, %3;\n\t"
+      "addc.cc.u32 %1, %1, %4;\n\t"
+      "addc.u32 %2, %2, %5;"
+      : "+r"(c0), "+r"(c1), "+r"(c2)
+      : "r"(d0), "r"(d1), "r"(d2));
+}
+
+// Exact 96-bit sum of x[i] y[k - i] over i0 <= i <= i1, added to (c0, c1, c2): two interleaved
+// accumulators (independent carry chains) and the loads of four terms issued ahead of their products.
+__device__ __forceinline__ void column96(u32& c0, u32& c1, u32& c2, const u32* x, const u32* y, int k, int i0,
+                                         int i1);
 
 __device__ __forceinline__ void mac96(u32& c0, u32& c1, u32& c2, u32 x, u32 y) {
   asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
@@ -300,6 +316,22 @@ __device__ __forceinline__ void mac96(u32& c0, u32& c1, u32& c2, u32 x, u32 y) {
       "addc.u32 %2, %2, 0;"
       : "+r"(c0), "+r"(c1), "+r"(c2)
       : "r"(x), "r"(y));
+}
+
+__device__ __forceinline__ void column96(u32& c0, u32& c1, u32& c2, const u32* x, const u32* y, int k, int i0,
+                                         int i1) {
+  u32 d0 = 0, d1 = 0, d2 = 0;
+  int i = i0;
+  for (; i + 3 <= i1; i += 4) {
+    const u32 a0 = x[i], a1 = x[i + 1], a2 = x[i + 2], a3 = x[i + 3];
+    const u32 b0 = y[k - i], b1 = y[k - i - 1], b2 = y[k - i - 2], b3 = y[k - i - 3];
+    mac96(c0, c1, c2, a0, b0);
+    mac96(d0, d1, d2, a1, b1);
+    mac96(c0, c1, c2, a2, b2);
+    mac96(d0, d1, d2, a3, b3);
+  }
+  for (; i <= i1; i++) mac96(c0, c1, c2, x[i], y[k - i]);
+  add96(c0, c1, c2, d0, d1, d2);
 }
 
 // Carry into this lane of a 32-lane digit chain: g = this lane's digit overflowed (carry out whatever
@@ -366,10 +398,7 @@ __device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScra
   for (int q0 = 0; q0 < ncol; q0 += 32) {
     const int q = q0 + lane, k = kmin + q;
     u32 c0 = 0, c1 = 0, c2 = 0;
-    if (q < ncol && k <= kmax) {
-      const int i0 = max(la, k - tb), i1 = min(ta, k - lb);
-      for (int i = i0; i <= i1; i++) mac96(c0, c1, c2, s.xa[i], s.xb[k - i]);
-    }
+    if (q < ncol && k <= kmax) column96(c0, c1, c2, s.xa, s.xb, k, max(la, k - tb), min(ta, k - lb));
     u32 c1u = __shfl_up_sync(kFull, c1, 1), c2u = __shfl_up_sync(kFull, c2, 2);
     if (lane == 0) c1u = p_c1;
     if (lane == 0) c2u = p_c2a;
@@ -434,8 +463,7 @@ __device__ void fx_rmw(u32* dst, const u32* x, int tx, const u32* y, int ty, boo
     }
   };
   for (int k = kmin; k <= kmax; k++) {
-    const int i0 = max(0, k - ty), i1 = min(tx, k);
-    for (int i = i0; i <= i1; i++) mac96(c0, c1, c2, x[i], y[k - i]);
+    column96(c0, c1, c2, x, y, k, max(0, k - ty), min(tx, k));
     if (k >= LF) emit(c0);
     c0 = c1;
     c1 = c2;
@@ -484,21 +512,21 @@ __device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arit
 }
 
 __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
-  return (size_t)(528 + 32) * WL * 4 + 8 * sizeof(WarpScratch) + 5 * FW * 4 + 64;
+  return (size_t)(528 + 32) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 5 * FW * 4 + 64;
 }
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
-  return (size_t)(528 + 32 + 288) * WL * 4 + 8 * sizeof(WarpScratch) + 2 * 528 + 64;
+  return (size_t)(528 + 32 + 288) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
 }
 
 __device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
 
-__global__ void __launch_bounds__(kThreads) chol_tiles_smem_kernel(u32* __restrict__ A, u32* __restrict__ RINV,
+__global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restrict__ A, u32* __restrict__ RINV,
                                                                    int WL, int LF, unsigned* __restrict__ err) {
   extern __shared__ __align__(16) u32 sm[];
   u32* T = sm;                                                   // lower triangle, entry (i, j) at tri(i, j)
   u32* colmag = T + 528 * WL;                                    // |l_ik| of the current column
   WarpScratch* ws = reinterpret_cast<WarpScratch*>(colmag + 32 * WL);
-  u32* nw = reinterpret_cast<u32*>(ws + 8);
+  u32* nw = reinterpret_cast<u32*>(ws + kWarpsS);
   u32 *sd = nw, *sr = nw + FW, *st1 = nw + 2 * FW, *st2 = nw + 3 * FW, *sone = nw + 4 * FW;
   uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * FW);
   uint8_t* coltop = colsign + 32;
@@ -508,7 +536,7 @@ __global__ void __launch_bounds__(kThreads) chol_tiles_smem_kernel(u32* __restri
   for (int i = 0; i < BT; i++) {
     const u32* src = G + (size_t)i * BT * WL;
     u32* dst = T + (size_t)tri(i, 0) * WL;
-    for (int w = tid; w < (i + 1) * WL; w += kThreads) dst[w] = src[w];
+    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[w];
   }
   __syncthreads();
   for (int k = 0; k < BT; k++) {
@@ -537,13 +565,13 @@ __global__ void __launch_bounds__(kThreads) chol_tiles_smem_kernel(u32* __restri
       for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
     }
     __syncthreads();
-    for (int i = k + 1 + warp; i < BT; i += 8) {                 // l_ik = a_ik * r_k
+    for (int i = k + 1 + warp; i < BT; i += kWarpsS) {           // l_ik = a_ik * r_k
       u32* aik = T + (size_t)tri(i, k) * WL;
       wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WL, colsign + i, coltop + i);
     }
     __syncthreads();
     const int m = BT - k - 1, npairs = m * (m + 1) / 2;
-    for (int p = tid; p < npairs; p += kThreads) {               // a_ij -= l_ik l_jk, k < j <= i
+    for (int p = tid; p < npairs; p += kThreadsS) {               // a_ij -= l_ik l_jk, k < j <= i
       int ii = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
       while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
       while (ii * (ii + 1) / 2 > p) ii--;
@@ -556,14 +584,14 @@ __global__ void __launch_bounds__(kThreads) chol_tiles_smem_kernel(u32* __restri
   for (int i = 0; i < BT; i++) {
     u32* dst = G + (size_t)i * BT * WL;
     const u32* src = T + (size_t)tri(i, 0) * WL;
-    for (int w = tid; w < (i + 1) * WL; w += kThreads) dst[w] = src[w];
+    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[w];
   }
 }
 
 // Number of partial-sum slots of column k in row i when each slot takes up to c products.
 __device__ __forceinline__ int nslots(int i, int k, int c) { return (i - k + c - 1) / c; }
 
-__global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* __restrict__ Lt,
+__global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* __restrict__ Lt,
                                                                     const u32* __restrict__ RINV,
                                                                     u32* __restrict__ X, int WL, int LF) {
   extern __shared__ __align__(16) u32 sm[];
@@ -571,7 +599,7 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
   u32* Lrow = Xm + 528 * WL;                                     // |l_ij|, j < i, of the current row
   u32* part = Lrow + 32 * WL;                                    // partial sums (two's complement)
   WarpScratch* ws = reinterpret_cast<WarpScratch*>(part + 288 * WL);
-  uint8_t* xs = reinterpret_cast<uint8_t*>(ws + 8);             // signs, tops of x
+  uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of x
   uint8_t* xt = xs + 528;
   uint8_t* ls = xt + 528;                                        // signs, tops of the row of L
   uint8_t* lt = ls + 32;
@@ -588,7 +616,7 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
     }
   }
   for (int i = 1; i < BT; i++) {
-    for (int j = warp; j <= i; j += 8) {
+    for (int j = warp; j <= i; j += kWarpsS) {
       int top, sg;
       if (j < i) {
         sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lrow + (size_t)j * WL, WL, top);
@@ -609,7 +637,7 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
     const int c = (i * (i + 1) / 2 + kThreads - 1) / kThreads;
     int total = 0;
     for (int k = 0; k < i; k++) total += nslots(i, k, c);
-    for (int slot = tid; slot < total; slot += kThreads) {
+    for (int slot = tid; slot < total; slot += kThreadsS) {
       int k = 0, r = slot;
       while (r >= nslots(i, k, c)) r -= nslots(i, k, c), k++;
       const int j0 = k + r * c, j1 = min(i, j0 + c);
@@ -622,7 +650,7 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
     }
     __syncthreads();
     // x_ik = -(sum of the partials) * r_i
-    for (int k = warp; k < i; k += 8) {
+    for (int k = warp; k < i; k += kWarpsS) {
       int base = 0;
       for (int kk = 0; kk < k; kk++) base += nslots(i, kk, c);
       const int n = nslots(i, k, c);
@@ -651,7 +679,7 @@ __global__ void __launch_bounds__(kThreads) trinv_tiles_smem_kernel(const u32* _
     }
     __syncthreads();
   }
-  for (int e = warp; e < BT * BT; e += 8) {                      // two's complement out; upper part zero
+  for (int e = warp; e < BT * BT; e += kWarpsS) {                      // two's complement out; upper part zero
     const int i = e / BT, k = e % BT;
     u32* dst = XG + (size_t)e * WL;
     if (k > i) {
@@ -721,7 +749,7 @@ extern "C" int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int 
   if (WL <= FW) {
     int st = smem_attributes();
     if (st != SDPV_OK) return st;
-    chol_tiles_smem_kernel<<<(unsigned)ntiles, kThreads, chol_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+    chol_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, chol_smem_bytes(WL), sdpv::as_stream(stream)>>>(
         A, RINV, WL, LF, sdpv::device_error_word());
     return sdpv::launch_status();
   }
@@ -737,7 +765,7 @@ extern "C" int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32
   if (WL <= FW) {                                   // shared-memory kernel: S is not used
     int st = smem_attributes();
     if (st != SDPV_OK) return st;
-    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreads, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
         Lt, RINV, X, WL, LF);
     return sdpv::launch_status();
   }
