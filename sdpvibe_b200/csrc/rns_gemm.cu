@@ -69,12 +69,52 @@ __device__ __forceinline__ void tile_of(int t, int mode, int ntn, int& tm, int& 
   }
 }
 
+// Epilogue arithmetic of one thread's row (TMEM lane quarter q, column half ch): (hh mod m) 2^14 + (hx mod m)
+// 2^7 + ll + old -> canonical residue, two per u32.  TMEM is released (tmem_empty) once both 32-column
+// chunks are in registers.
+__device__ __forceinline__ void epi_compute(u32 tmem, int q, int ch, int lane, int m, int c14, float minv,
+                                            const u32 (&olds)[2][16], u32 (&outp)[2][16], u64* tmem_empty) {
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    u32 hh[32], hx[32], ll[32];
+    u32 base = tmem + ((u32)(q * 32) << 16) + 64 * ch + 32 * c;
+    tmem_ld32(base, hh);
+    tmem_ld32(base + 128, hx);
+    tmem_ld32(base + 256, ll);
+    tmem_ld_wait();
+    if (c == 1) {                                       // accumulators read: the next item's MMAs may start
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_empty);
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < 16; j2++) {
+      u32 pair = 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = 2 * j2 + h;
+        // (hh mod m) and (hx mod m) as |r| <= m/2 + m/300 representatives, then the canonical residue
+        const int old = (int)(int16_t)(olds[c][j2] >> (16 * h));
+        int a = (int)hh[j], x = (int)hx[j];
+        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+        int v = ra * c14 + rx * 128 + (int)ll[j] + old;
+        int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+        r += (r < 0) ? m : 0;
+        r -= (r >= m) ? m : 0;
+        pair |= ((u32)r & 0xffffu) << (16 * h);
+      }
+      outp[c][j2] = pair;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
-                    i64 tiles, i64 nitems, bool fresh, unsigned* __restrict__ err) {
+                    i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   GemmSmem& S = *reinterpret_cast<GemmSmem*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -109,10 +149,20 @@ __global__ void __launch_bounds__(kThreads, 1)
       u32 kbg = 0;                              // k-blocks issued by this CTA so far (ring position)
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
         const i64 t = item % tiles, bg = item / tiles;
-        const int b = (int)(bg % nb), g = gofs + (int)(bg / nb);       // modulus plane of the operands
-        int tm, tn;
-        tile_of((int)t, mode, ntn, tm, tn);
-        const int m0 = tm * 128, n0 = tn * 128;
+        int b, g, m0, n0;
+        if (pack > 1) {                           // packed: tile t holds blocks t*pack .. (rows stacked)
+          b = 0;
+          g = gofs + (int)bg;
+          m0 = (int)(t * pack * M);
+          n0 = (int)(t * pack * N);
+        } else {
+          b = (int)(bg % nb);
+          g = gofs + (int)(bg / nb);              // modulus plane of the operands
+          int tm, tn;
+          tile_of((int)t, mode, ntn, tm, tn);
+          m0 = tm * 128;
+          n0 = tn * 128;
+        }
         for (int kb = 0; kb < nk; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
@@ -177,7 +227,58 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3, ch = (warp - 2) >> 2, ew = warp - 2;
     const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
     u32 li = 0;
-    for (i64 item = blockIdx.x; item < nitems; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && pack > 1; item += gridDim.x, li++) {
+      // packed small blocks: tile rows are the stacked rows of blocks t*pack .. t*pack + nbt - 1, tile
+      // columns their stacked B rows; only the diagonal sub-blocks are outputs (staged, coalesced)
+      const i64 t = item % tiles;
+      const int g = (int)(item / tiles);
+      const int gg = g0 + gofs + g;
+      const int m = S.tmod[g], c14 = S.tc14[g];
+      const float minv = S.tminv[g];
+      const i64 b0 = t * pack;
+      const int nbt = (int)(nb - b0 < pack ? nb - b0 : pack);
+      const int nrow = nbt * (int)M;
+      const i64 rowbase = (i64)gg * nb * M + b0 * M;               // acc row of tile row 0
+      const int rrow = q * 32 + lane;
+      u32 olds[2][16];
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j = 0; j < 16; j++) olds[c][j] = 0;
+      if (!fresh) {
+        epi_sync();
+        for (int r = ew; r < nrow; r += 8) {
+          const int bi = r / (int)M;
+          const int16_t* src = acc + (rowbase + r) * ldc;
+          for (int j = lane; j < N; j += 32) S.stg[r][bi * N + j] = src[j];
+        }
+        epi_sync();
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            olds[c][j] = *reinterpret_cast<const u32*>(&S.stg[rrow][64 * ch + 32 * c + 2 * j]);
+      }
+      const bool ok_me = mbar_wait(&S.acc_full, li & 1, err);
+      const bool fail = epi_sync_or(!ok_me);
+      if (fail) break;
+      tc_fence_after();
+      u32 outp[2][16];
+      epi_compute(tmem, q, ch, lane, m, c14, minv, olds, outp, &S.tmem_empty);
+      epi_sync();
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j2 = 0; j2 < 16; j2++)
+          *reinterpret_cast<u32*>(&S.stg[rrow][64 * ch + 32 * c + 2 * j2]) = outp[c][j2];
+      epi_sync();
+      for (int r = ew; r < nrow; r += 8) {
+        const int bi = r / (int)M;
+        int16_t* dst = acc + (rowbase + r) * ldc;
+        for (int j = lane; j < N; j += 32) dst[j] = S.stg[r][bi * N + j];
+      }
+    }
+    for (i64 item = blockIdx.x; item < nitems && pack <= 1; item += gridDim.x, li++) {
       const i64 t = item % tiles, bg = item / tiles;
       const int b = (int)(bg % nb), g = (int)(bg / nb);
       int tm, tn;
@@ -248,39 +349,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (fail) break;
       tc_fence_after();
       u32 outp[2][16];
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        u32 hh[32], hx[32], ll[32];
-        u32 base = tmem + ((u32)(q * 32) << 16) + 64 * ch + 32 * c;
-        tmem_ld32(base, hh);
-        tmem_ld32(base + 128, hx);
-        tmem_ld32(base + 256, ll);
-        tmem_ld_wait();
-        if (c == 1) {                                   // accumulators read: the next item's MMAs may start
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&S.tmem_empty);
-        }
-#pragma unroll
-        for (int j2 = 0; j2 < 16; j2++) {
-          u32 pair = 0;
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            const int j = 2 * j2 + h;
-            // (hh mod m) and (hx mod m) as |r| <= m/2 + m/300 representatives, then the canonical residue
-            const int old = (int)(int16_t)(olds[c][j2] >> (16 * h));
-            int a = (int)hh[j], x = (int)hx[j];
-            int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-            int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
-            int v = ra * c14 + rx * 128 + (int)ll[j] + old;
-            int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-            r += (r < 0) ? m : 0;
-            r -= (r >= m) ? m : 0;
-            pair |= ((u32)r & 0xffffu) << (16 * h);
-          }
-          outp[c][j2] = pair;
-        }
-      }
+      epi_compute(tmem, q, ch, lane, m, c14, minv, olds, outp, &S.tmem_empty);
       if (vec) {
         if (rrow < nrow) {
 #pragma unroll
@@ -357,9 +426,17 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   if (ldc < N) return SDPV_EINVAL;
   if (M == 0 || N == 0 || KC == 0) return SDPV_OK;
   if (((uintptr_t)Ahi | (uintptr_t)Alo | (uintptr_t)Bhi | (uintptr_t)Blo) & 15) return SDPV_EINVAL;
+  // Small blocks (M, N <= 64, not syrk) are packed: pack blocks share one 128 x 128 tile (their stacked rows
+  // against their stacked B rows; only the diagonal sub-blocks are kept), so fewer, fuller tiles run.
+  int pack = 1;
+  if (mode == 0 && nb > 1 && M <= 64 && N <= 64) {
+    i64 p = 128 / M < 128 / N ? 128 / M : 128 / N;
+    pack = (int)(p < nb ? p : nb);
+  }
   CUtensorMap mAh, mAl, mBh, mBl;
-  if (!make_map(&mAh, Ahi, KC, M, nb, G, a_stride) || !make_map(&mAl, Alo, KC, M, nb, G, a_stride) ||
-      !make_map(&mBh, Bhi, KC, N, nb, G, b_stride) || !make_map(&mBl, Blo, KC, N, nb, G, b_stride))
+  const i64 ra = pack > 1 ? M * nb : M, rb = pack > 1 ? N * nb : N, nbm = pack > 1 ? 1 : nb;
+  if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
+      !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride))
     return SDPV_EINVAL;
   size_t smem = sizeof(GemmSmem) + 1024;
   static std::once_flag attr;
@@ -370,17 +447,18 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
+  if (pack > 1) tiles = (nb + pack - 1) / pack;
   if (tiles > 0x7fffffff) return SDPV_EINVAL;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   for (int gofs = 0; gofs < G; gofs += kMaxG) {        // at most kMaxG moduli per launch
     const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
-    const i64 nitems = tiles * nb * Gl;
+    const i64 nitems = tiles * (pack > 1 ? 1 : nb) * Gl;
     const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);   // one resident CTA per SM, items looped
     rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
         mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, tiles,
-        nitems, fresh, sdpv::device_error_word());
+        nitems, fresh, pack, sdpv::device_error_word());
     const int st = sdpv::launch_status();
     if (st != SDPV_OK) return st;
   }

@@ -184,7 +184,11 @@ def _rand_residues(rng, T, G, rows, K):
 
 @pytest.mark.parametrize("L,nb,M,N,K,syrk", [(24, 1, 256, 256, 256, False), (26, 1, 300, 129, 1024, False),
                                               (27, 1, 274, 274, 2000, True), (24, 3, 70, 45, 48, False),
-                                              (10, 5, 33, 33, 16, True), (26, 2, 130, 7, 4096, False)])
+                                              (10, 5, 33, 33, 16, True), (26, 2, 130, 7, 4096, False),
+                                              # small blocks packed several to a tile
+                                              (26, 7, 21, 5, 48, False), (26, 5, 64, 64, 128, False),
+                                              (24, 9, 33, 60, 32, False), (34, 4, 32, 42, 48, False),
+                                              (26, 13, 1, 9, 16, False)])
 def test_rns_gemm_random(sb, L, nb, M, N, K, syrk):
     from sdpvibe_b200.mpmat import ctx
     rng = np.random.default_rng(M * N + K)
@@ -598,3 +602,23 @@ def test_linalg_golden(sb):
     assert np.array_equal(np_(Y), g["Ym"]) and np.array_equal(np_(ye), g["ye"])
     Yf, yfe = basecase.trsv_tile(ts[0], cu(g["Vm"]), cu(g["ve"]), out_exp=-(32 * 8 - 40))
     assert np.array_equal(np_(Yf), g["Yfm"]) and np.array_equal(np_(yfe), g["yfe"])
+
+
+@pytest.mark.parametrize("nb,M,N,K", [(1, 200, 130, 64), (6, 32, 42, 32), (3, 100, 7, 48)])
+def test_rns_gemm_fresh_overwrites(sb, nb, M, N, K):
+    """fresh mode: the accumulator's previous content is ignored (overwritten with the product residues)."""
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(nb + M + N)
+    L = 26
+    T = O.tables(L)
+    R = ctx(L)
+    Ah, Al = _rand_residues(rng, T, T.n, nb * M, K)
+    Bh, Bl = _rand_residues(rng, T, T.n, nb * N, K)
+    acc = cu((rng.integers(0, 30000, size=(T.n, nb * M, N))).astype(np.int16))      # garbage
+    R.accumulate(cu(Ah), cu(Al), cu(Bh), cu(Bl), acc, 0, nb=nb, fresh=True)
+    got = np_(acc)
+    zero = np.zeros((T.n, M, N), np.int16)
+    for b in range(nb):
+        sl = slice(b * M, (b + 1) * M)
+        ref = O.accumulate(T, Ah[:, sl], Al[:, sl], Bh[:, b * N:(b + 1) * N], Bl[:, b * N:(b + 1) * N], zero, 0)
+        assert np.array_equal(got[:, sl], ref)
