@@ -36,8 +36,8 @@ METRIC = "768-bit SDP s/iter & residue-GEMM INT8 TOPS, fused vs plain, 1 B200, b
 NBLOCKS, MLO, MHI, NCOLS, L, NCHUNK = 400, 20, 120, 274, 26, 4
 N_MOD = 128                       # moduli of the accumulator context (L + 1 = 27 limbs)
 # DRAM bytes (read + write) of one syrk launch per chunk row, from the ncu capture of
-# `kernel_bench --kernel syrk --N 274 --K 7000 --L 27` (509.1 MB read + 12.2 MB written / 7000 rows).
-SYRK_DRAM_BYTES_PER_ROW = (509.113088e6 + 12.194816e6) / 7000
+# `kernel_bench --kernel syrk --N 274 --K 7000 --L 27` (524.8 MB read + 14.0 MB written / 7000 rows).
+SYRK_DRAM_BYTES_PER_ROW = (524.783104e6 + 13.99424e6) / 7000
 
 
 def workload_shape(seed=0):
