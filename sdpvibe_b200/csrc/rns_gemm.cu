@@ -112,6 +112,8 @@ __device__ __forceinline__ void epi_compute(u32 tmem, int q, int ch, int lane, i
 __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                    const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
+                    int nfull,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
@@ -150,7 +152,12 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
         const i64 t = item % tiles, bg = item / tiles;
         int b, g, m0, n0;
-        if (pack > 1) {                           // packed: tile t holds blocks t*pack .. (rows stacked)
+        if (tailTB) {                             // syrk tail: A row block t against the last < 64 rows
+          b = (int)(bg % nb);
+          g = gofs + (int)(bg / nb);
+          m0 = (int)t * 128;
+          n0 = nfull;
+        } else if (pack > 1) {                    // packed: tile t holds blocks t*pack .. (rows stacked)
           b = 0;
           g = gofs + (int)bg;
           m0 = (int)(t * pack * M);
@@ -169,8 +176,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             *(volatile int*)&S.abort = 1;
             break;
           }
-          mbar_expect_tx(&S.full[s], 4 * kSlice);
           const int kx = kb * 128;
+          if (tailTB) {                           // [Bhi; Blo] of the tail rows back to back: 2 TB rows
+            mbar_expect_tx(&S.full[s], 2 * kSlice + 2 * tailTB * 128);
+            tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
+            tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
+            tma_load_4d(S.stage[s][2], &mTh, &S.full[s], kx, n0, b, g);
+            tma_load_4d(S.stage[s][2] + tailTB * 128, &mTl, &S.full[s], kx, n0, b, g);
+            continue;
+          }
+          mbar_expect_tx(&S.full[s], 4 * kSlice);
           tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
           tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
           tma_load_4d(S.stage[s][2], &mBh, &S.full[s], kx, n0, b, g);
@@ -180,7 +195,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const u32 idesc = idesc_i8(128, 256), idesc128 = idesc_i8(128, 128);
+      // tail items: N = 2 TB over [Bhi; Blo] (hh | hl at column 0, (hl + lh) | ll at column TB)
+      const int TB = tailTB ? tailTB : 128;
+      const u32 idesc = idesc_i8(128, 2 * TB), idesc128 = idesc_i8(128, TB);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
         // the epilogue must have read the previous item's accumulators out of TMEM
@@ -202,12 +219,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int ks = 0; ks < 4; ks++) {
             u64 bd = sdesc_sw128(bh + 32 * ks);
             if ((kb | ks) == 0) {
-              mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                             // hh | hl
-              mma_i8(tmem + 256, sdesc_sw128(al), sdesc_sw128(bh + kSlice), idesc128, 0u);  // ll
-              mma_i8(tmem + 128, sdesc_sw128(al), bd, idesc128, 1u);                        // hl += lh
+              mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                                   // hh | hl
+              mma_i8(tmem + 2 * TB, sdesc_sw128(al), sdesc_sw128(bh + TB * 128), idesc128, 0u);   // ll
+              mma_i8(tmem + TB, sdesc_sw128(al), bd, idesc128, 1u);                               // hl += lh
             } else {
               mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
-              mma_i8(tmem + 128, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+              mma_i8(tmem + TB, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
             }
           }
           mma_commit(&S.empty[s]);
@@ -227,6 +244,49 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3, ch = (warp - 2) >> 2, ew = warp - 2;
     const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
     u32 li = 0;
+    for (i64 item = blockIdx.x; item < nitems && tailTB; item += gridDim.x, li++) {
+      // syrk tail: entry (A row i, tail row j) = Q[nfull + j][i], written transposed into the lower triangle;
+      // a warp's lanes are consecutive i, so the accesses of one tail row coalesce
+      const i64 t = item % tiles, bg = item / tiles;
+      const int b = (int)(bg % nb), g = (int)(bg / nb);
+      const int gg = g0 + gofs + g;
+      const int m = S.tmod[g], c14 = S.tc14[g];
+      const float minv = S.tminv[g];
+      const i64 i = t * 128 + q * 32 + lane;                        // A row (output column)
+      const int tail = (int)(N - nfull);
+      int16_t* colp = acc + ((i64)gg * nb * M + (i64)b * M + nfull) * ldc + i;
+      int old[16];
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int j = 16 * ch + u;
+        old[u] = (i < M && j < tail && nfull + j >= i && !fresh) ? (int)colp[(i64)j * ldc] : 0;
+      }
+      const bool ok_me = mbar_wait(&S.acc_full, li & 1, err);
+      const bool fail = epi_sync_or(!ok_me);
+      if (fail) break;
+      tc_fence_after();
+      u32 hh[32], hx[32], ll[32];
+      const u32 base = tmem + ((u32)(q * 32) << 16);
+      tmem_ld32(base, hh);
+      tmem_ld32(base + tailTB, hx);
+      tmem_ld32(base + 2 * tailTB, ll);
+      tmem_ld_wait();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.tmem_empty);
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int j = 16 * ch + u;
+        int a = (int)hh[j], x = (int)hx[j];
+        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+        int v = ra * c14 + rx * 128 + (int)ll[j] + old[u];
+        int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+        r += (r < 0) ? m : 0;
+        r -= (r >= m) ? m : 0;
+        if (i < M && j < tail && nfull + j >= i) colp[(i64)j * ldc] = (int16_t)r;
+      }
+    }
     for (i64 item = blockIdx.x; item < nitems && pack > 1; item += gridDim.x, li++) {
       // packed small blocks: tile rows are the stacked rows of blocks t*pack .. t*pack + nbt - 1, tile
       // columns their stacked B rows; only the diagonal sub-blocks are outputs (staged, coalesced)
@@ -278,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = lane; j < N; j += 32) dst[j] = S.stg[r][bi * N + j];
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && pack <= 1; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && pack <= 1 && !tailTB; item += gridDim.x, li++) {
       const i64 t = item % tiles, bg = item / tiles;
       const int b = (int)(bg % nb), g = (int)(bg / nb);
       int tm, tn;
@@ -391,12 +451,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // 4-D int8 map over (K, rows, nb, G) with 128 x 128 boxes and 128-byte swizzle; gstride = bytes between
 // the planes of consecutive moduli (>= K*rows*nb).
-bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G, i64 gstride) {
+bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G, i64 gstride, int box_rows = 128) {
   sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
   if (!fn) return false;
   cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nb, (cuuint64_t)G};
   cuuint64_t strides[3] = {(cuuint64_t)K, (cuuint64_t)(K * rows), (cuuint64_t)gstride};
-  cuuint32_t box[4] = {128, 128, 1, 1};
+  cuuint32_t box[4] = {128, (cuuint32_t)box_rows, 1, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -446,21 +506,35 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   });
   if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
+  // syrk whose last row block has at most 32 rows: full lower tiles over the first nfull rows, then one
+  // item per A row block against those rows (N = 64 products, stored transposed) -- not 128 x 128 tiles
+  // that are mostly padding
+  const int nfull = (int)(N / 128) * 128, tailTB = (mode == 1 && N > 128 && N - nfull > 0 && N - nfull <= 32) ? 32 : 0;
+  if (tailTB) ntm = nfull / 128;
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
   if (pack > 1) tiles = (nb + pack - 1) / pack;
+  CUtensorMap mTh = mBh, mTl = mBl;
+  if (tailTB && (!make_map(&mTh, Bhi, KC, rb, nbm, G, b_stride, tailTB) ||
+                 !make_map(&mTl, Blo, KC, rb, nbm, G, b_stride, tailTB)))
+    return SDPV_EINVAL;
   if (tiles > 0x7fffffff) return SDPV_EINVAL;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   for (int gofs = 0; gofs < G; gofs += kMaxG) {        // at most kMaxG moduli per launch
     const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
-    const i64 nitems = tiles * (pack > 1 ? 1 : nb) * Gl;
-    const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);   // one resident CTA per SM, items looped
-    rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-        mAh, mAl, mBh, mBl, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, tiles,
-        nitems, fresh, pack, sdpv::device_error_word());
-    const int st = sdpv::launch_status();
-    if (st != SDPV_OK) return st;
+    for (int part = 0; part < (tailTB ? 2 : 1); part++) {
+      const int tb = part ? tailTB : 0;
+      const i64 ptiles = part ? nfull / 128 + 1 : tiles;
+      const i64 nitems = ptiles * (pack > 1 ? 1 : nb) * Gl;
+      if (nitems == 0) continue;
+      const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
+      rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
+          KC, mode, ntn, ptiles, nitems, fresh, pack, sdpv::device_error_word());
+      const int st = sdpv::launch_status();
+      if (st != SDPV_OK) return st;
+    }
   }
   return SDPV_OK;
 }

@@ -188,7 +188,10 @@ def _rand_residues(rng, T, G, rows, K):
                                               # small blocks packed several to a tile
                                               (26, 7, 21, 5, 48, False), (26, 5, 64, 64, 128, False),
                                               (24, 9, 33, 60, 32, False), (34, 4, 32, 42, 48, False),
-                                              (26, 13, 1, 9, 16, False)])
+                                              (26, 13, 1, 9, 16, False),
+                                              # syrk with a short last row block (tail items), and without
+                                              (27, 2, 150, 150, 64, True), (26, 1, 160, 160, 128, True),
+                                              (26, 1, 161, 161, 32, True), (27, 1, 290, 290, 48, True)])
 def test_rns_gemm_random(sb, L, nb, M, N, K, syrk):
     from sdpvibe_b200.mpmat import ctx
     rng = np.random.default_rng(M * N + K)
