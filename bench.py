@@ -241,10 +241,26 @@ def run_b200(args, rank, world, local_rank):
             acc.add(c)
         return acc.result()
 
+    copy_stream = torch.cuda.Stream(device=dev)
+    dbuf = [(torch.empty(hm.shape, dtype=hm.dtype, device=dev), torch.empty(he.shape, dtype=he.dtype, device=dev))
+            for hm, he in pinned]
+
     def step_e2e():
+        # host -> device copies of chunk c + 1 on a copy stream while chunk c is accumulated
+        main = torch.cuda.current_stream()
+        ready = []
+        for (hm, he), (dm, de) in zip(pinned, dbuf):
+            ev = torch.cuda.Event()
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_stream(main)             # the previous step is done with the buffers
+                dm.copy_(hm, non_blocking=True)
+                de.copy_(he, non_blocking=True)
+                ev.record(copy_stream)
+            ready.append(ev)
         acc = mpf.GramAcc(NCOLS, L)
-        for hm, he in pinned:
-            acc.add(mpf.MPF(hm.to(dev, non_blocking=True), he.to(dev, non_blocking=True)))
+        for (dm, de), ev in zip(dbuf, ready):
+            main.wait_event(ev)
+            acc.add(mpf.MPF(dm, de))
         Q = acc.result()
         out_m.copy_(Q.m, non_blocking=True)
         out_e.copy_(Q.e, non_blocking=True)
