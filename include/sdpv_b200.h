@@ -155,6 +155,12 @@ int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL,
 int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
                      int WL, int LF, void* stream);
 
+/* Eigenvalues of nb symmetric float64 n x n matrices A (nb, n, n) (n <= 128), ascending into w (nb, n), with an
+ * error bound per matrix in err (nb) and the sweep count in sweeps (nb, may be NULL): batched cyclic Jacobi.
+ * The device counterpart of the host LAPACK call in the step length (sdpvibe/solver.py:1064-1093, the
+ * eigvalsh of the scaled float64 copy, and _eig_err 1001-1004). */
+int sdpv_eig_sym_f64(const double* A, int64_t nb, int n, double* w, double* err, int* sweeps, void* stream);
+
 /* Triangular solve L y = v for nvec vectors of 32 entries with one factored 32 x 32 tile (Lt lower, RINV its
  * pivot reciprocals), wide fixed point; V (nvec, 32, WL) is overwritten by y.  Replaces basecase.trsv_tile's
  * trsv_warp (sdpvibe/basecase.py:228-245, 310-331). */

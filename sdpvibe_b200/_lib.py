@@ -44,6 +44,7 @@ _SIGS = {
     "sdpv_trinv_tiles": [_P, _P, _P, _P, _L, _I, _I, _I, _P],
     "sdpv_trinv_tiles_noalloc": [_P, _P, _P, _L, _I, _I, _I, _P],
     "sdpv_trsv_tiles": [_P, _P, _P, _L, _I, _I, _I, _P],
+    "sdpv_eig_sym_f64": [_P, _L, _I, _P, _P, _P, _P],
     "sdpv_get_error": [ctypes.POINTER(ctypes.c_uint), _P],
 }
 

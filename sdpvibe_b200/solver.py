@@ -151,15 +151,46 @@ def _mpf_from_float(V, L):
     return F.from_float(V, L)
 
 
-def _scaled_float(M):
-    """(per block scale s, ok mask, symmetric float64 copy of M * 2^-s): s is the largest entry top of
-    each block (0 for all-zero blocks), so the copy is O(1) and cannot overflow"""
+EIG_DEVICE = os.environ.get("SDPV_EIG", "device") != "host"    # min_eig's float64 eigenvalues on the GPU
+EIG_DEVICE_NMAX = 128
+
+
+def _scaled(M):
+    """(per block scale s, ok mask, M * 2^-s as an MPF): s is the largest entry top of each block (0 for
+    all-zero blocks), so the float64 copy is O(1) and cannot overflow"""
     tp = F._top(M)
     s = tp.reshape(tp.shape[0], -1).amax(1)
     ok = s > EZ // 2
     s = torch.where(ok, s, torch.zeros_like(s))
-    Mf = M.shift(-s[:, None, None]).to_float()
+    return s, ok, M.shift(-s[:, None, None])
+
+
+def _scaled_float(M):
+    """(s, ok, symmetric float64 copy of M * 2^-s on the host)"""
+    s, ok, Ms = _scaled(M)
+    Mf = Ms.to_float()
     return s, ok, (Mf + np.swapaxes(Mf, 1, 2)) / 2
+
+
+def _device_float(A):
+    """float64 values of an MPF on the device (the formula of MPF.to_float)"""
+    L = A.L
+    top = A.m[-1].double() * 2.0 ** 32 + (A.m[-2].double() % 2.0 ** 32) if L > 1 else A.m[-1].double()
+    sc = (A.e + 32 * (L - 2)).clamp(-1100, 1100).double()
+    return torch.where(A.e == EZ, torch.zeros_like(top), top * torch.pow(2.0, sc))
+
+
+def _eig_min_device(Ms):
+    """(lambda_min (nb,), error bound (nb,)) of the symmetric float64 copies of the blocks of Ms, by the
+    batched Jacobi kernel (sdpv_eig_sym_f64), returned to the host"""
+    from . import _lib
+    Af = _device_float(Ms)
+    Af = ((Af + Af.transpose(1, 2)) / 2).contiguous()
+    nb, n, _ = Af.shape
+    w = torch.empty((nb, n), dtype=torch.float64, device=Af.device)
+    err = torch.empty((nb,), dtype=torch.float64, device=Af.device)
+    _lib.call("sdpv_eig_sym_f64", _lib.ptr(Af), nb, n, _lib.ptr(w), _lib.ptr(err), None, _lib.stream())
+    return w[:, 0].cpu().numpy(), err.cpu().numpy()
 
 
 def refine_min_eig(A, gamma, levels=64):
@@ -210,15 +241,21 @@ def refine_min_eig(A, gamma, levels=64):
 
 def min_eig(chols, dMs, lam=None, gamma=None, stats=None):
     """min over blocks of lambda_min(L^-1 dM L^-T), combined with lam (sdpvibe/solver.py:1064-1093).
-    The eigenvalues come from a float64 copy of each block (LAPACK on the host, as the reference);
-    with gamma (stepLengthReduction) the blocks whose float64 error bound could move the step length by
-    more than EIG_TOL are recomputed in multiprecision (refine_min_eig), counted in stats."""
+    The eigenvalues come from a float64 copy of each block: on the GPU by the batched Jacobi kernel with
+    its own error bound (EIG_DEVICE, blocks up to 128), else LAPACK on the host with the reference's bound
+    (n + 2) eps ||M||_F, which reproduces the reference's steps bit for bit.  With gamma
+    (stepLengthReduction) the blocks whose error bound could move the step length by more than EIG_TOL
+    are recomputed in multiprecision (refine_min_eig), counted in stats."""
     for ch, D in zip(chols, dMs):
         T = ch.solve_lower(D)
         M = ch.solve_lower(T.T)                                     # L^-1 dM L^-T (dM symmetric)
-        s, ok, Mf = _scaled_float(M)
-        ev = np.linalg.eigvalsh(Mf)[:, 0]
-        err = _eig_err(Mf)
+        if EIG_DEVICE and M.shape[-1] <= EIG_DEVICE_NMAX:
+            s, ok, Ms = _scaled(M)
+            ev, err = _eig_min_device(Ms)
+        else:
+            s, ok, Mf = _scaled_float(M)
+            ev = np.linalg.eigvalsh(Mf)[:, 0]
+            err = _eig_err(Mf)
         flag = []
         for q in torch.nonzero(ok).reshape(-1).tolist():
             sc = mp.mpf(2) ** int(s[q])

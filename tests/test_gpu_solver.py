@@ -3,11 +3,12 @@
 tests/golden/solver_tiny.npz holds a tiny SDP (4 blocks of dims 1, 1, 2, 3; N = 5; L = 8) and, for its
 first iterations, what the reference's Solver.run produced (tests/golden/make_solver_golden.py): the
 printed scalars, the step lengths, y, and each chunk's corrector direction.  The GPU run must reproduce
-them bit for bit.  The step lengths depend on float64 eigenvalues from LAPACK on the host; both runs
-use numpy's, on bit-identical input matrices."""
+them bit for bit when the step-length eigenvalues come from LAPACK on the host, as in the reference (both
+runs use numpy's, on bit-identical input matrices), and to 1e-13 relative with the GPU eigenvalue kernel.""" 
 import mpmath as mp
 import numpy as np
 import pytest
+import torch
 
 from conftest import golden
 
@@ -32,8 +33,11 @@ def _sdp_from_fixture(g):
     return SDP(blocks, (g["b_m"], g["b_e"]), 0, L), L
 
 
-def test_solver_iterates_match_reference():
+def test_solver_iterates_match_reference(monkeypatch):
+    """with the step-length eigenvalues from LAPACK on the host, as the reference: bit-identical"""
+    from sdpvibe_b200 import solver
     from sdpvibe_b200.solver import Solver, fmt_big
+    monkeypatch.setattr(solver, "EIG_DEVICE", False)
     g = golden("solver_tiny")
     iters = int(g["iters_done"])
     sdp, L = _sdp_from_fixture(g)
@@ -74,3 +78,35 @@ def test_solver_ising_like_small_runs():
     for row in log:
         assert 0 < row["P_step"] <= 1 and 0 < row["D_step"] <= 1
         assert mp.isfinite(row["pobj"]) and mp.isfinite(row["dobj"])
+
+
+def test_solver_iterates_device_eigenvalues_near_reference():
+    """with the step-length eigenvalues from the GPU Jacobi kernel: the float64 lambda_min may differ from
+    LAPACK's in the last bits, so the steps (and the iterates after them) agree to 1e-13 relative"""
+    from sdpvibe_b200 import solver
+    from sdpvibe_b200.mpf import MPF
+    from sdpvibe_b200.solver import Solver
+    assert solver.EIG_DEVICE
+    g = golden("solver_tiny")
+    iters = int(g["iters_done"])
+    sdp, L = _sdp_from_fixture(g)
+    sol = Solver(sdp, L)
+    worst = [0.0]
+
+    def close(M, key):
+        got = M.to_mp().reshape(-1)
+        ref = MPF(torch.from_numpy(g[key + "_m"]).cuda(), torch.from_numpy(g[key + "_e"]).cuda()).to_mp().reshape(-1)
+        scale = max(abs(v) for v in ref) or mp.mpf(1)
+        d = max(abs(a - b) for a, b in zip(got, ref)) / scale
+        worst[0] = max(worst[0], float(d))
+        assert d <= mp.mpf("1e-13"), (key, float(d))
+
+    def rec(it, s, info):
+        for k, v in zip(("aP", "aD"), s.last_steps[:2]):
+            man, ex = str(g[f"it{it}_{k}"]).split("*2^")
+            ref = mp.mpf(int(man)) * mp.mpf(2) ** int(ex)
+            assert abs(v / ref - 1) <= mp.mpf("1e-13"), (it, k)
+        close(s.y, f"it{it}_y")
+        for gi, o in enumerate(s.st):
+            close(o["dc"]["dx"], f"it{it}_g{gi}_dx")
+    sol.run(max_iter=iters, record=rec)

@@ -86,11 +86,40 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("eig", ["host", "device"])
 @pytest.mark.parametrize("n", [40, 144])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_min_eig_exact_spectra(name, n):
+def test_min_eig_exact_spectra(name, n, eig, monkeypatch):
+    """host: LAPACK with the reference's bound (the reference's refined-block counts); device: the Jacobi
+    kernel with its own, wider bound (as many refinements or more, the same step accuracy).  n = 144 is
+    beyond the device kernel's 128 and runs on the host in both modes."""
+    from sdpvibe_b200 import solver
+    monkeypatch.setattr(solver, "EIG_DEVICE", eig == "device")
     make, refined = CASES[name]
-    _run(make(n), refined)
+    _run(make(n), refined if eig == "host" or n > solver.EIG_DEVICE_NMAX else None)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 21, 42, 63, 64, 100, 128])
+def test_eig_sym_f64_kernel(n):
+    """sdpv_eig_sym_f64 against LAPACK: every eigenvalue within the kernel's bound plus LAPACK's."""
+    from sdpvibe_b200 import _lib
+    rng = np.random.default_rng(n)
+    nb = 5
+    A = rng.standard_normal((nb, n, n)) * 2.0 ** rng.integers(-3, 4, size=(nb, 1, 1))
+    A[1] = A[1] @ A[1].transpose() if n > 1 else A[1]                 # semidefinite, clustered small ones
+    A = (A + np.swapaxes(A, 1, 2)) / 2
+    A[2] = np.diag(np.arange(n, dtype=np.float64))                      # already diagonal
+    Ad = torch.from_numpy(A).cuda()
+    w = torch.empty((nb, n), dtype=torch.float64, device="cuda")
+    err = torch.empty((nb,), dtype=torch.float64, device="cuda")
+    sw = torch.empty((nb,), dtype=torch.int32, device="cuda")
+    _lib.call("sdpv_eig_sym_f64", _lib.ptr(Ad), nb, n, _lib.ptr(w), _lib.ptr(err), _lib.ptr(sw), _lib.stream())
+    ref = np.linalg.eigvalsh(A)
+    lap = (n + 2) * 2.0 ** -52 * np.sqrt((A * A).sum(axis=(1, 2)))
+    wd, ed = w.cpu().numpy(), err.cpu().numpy()
+    assert (sw.cpu().numpy() < 40).all()
+    assert np.all(np.abs(wd - ref) <= (ed + lap)[:, None])
+    assert np.all(np.diff(wd, axis=1) >= 0)
 
 
 def test_min_eig_matrix_matches_oracle():
