@@ -293,9 +293,18 @@ def run_b200(args, rank, world, local_rank):
 
     for _ in range(max(args.warmup, 3)):
         step()
-    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
+    # The step has no host decision (GramAcc decides its flushes on the device), so it is recorded once as a
+    # CUDA graph and the timed steps replay it; a separate eager pass times every kernel for the breakdown.
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        step()
+    for _ in range(2):
+        graph.replay()
     with ClockSampler(local_rank) as clk:
-        ms = timed(step, args.steps, tr)
+        ms = timed(graph.replay, args.steps)
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
+    ms_eager = timed(step, args.steps, tr)
     for _ in range(2):
         step_e2e()
     ms_e2e = timed(step_e2e, args.steps)
@@ -336,7 +345,8 @@ def run_b200(args, rank, world, local_rank):
         "kernel_ms_per_step": {k: sum(tr.kernel_ms(k)) / args.steps for k in sorted(tr.timed)},
         "e2e": {"value": world * algorithmic_ops(R) / (ms_e2e / args.steps * 1e-3) / 1e12, "unit": "TOPS",
                 "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": tr.total_launches,
+        "ms_per_step_eager": ms_eager / args.steps,
+        "gpu_launches": tr.total_launches, "gpu_launches_per_step": tr.total_launches // args.steps,
         "launches_by_entry": dict(tr.launches),
         "clocks": clk.summary(),
     }
@@ -452,7 +462,8 @@ def run_cholsolve(args, rank, world, local_rank):
             "kernel_ms_per_step": kms, "top_kernel": top,
             "e2e": {"value": world * macs / (ms_e2e / args.steps * 1e-3), "unit": "mp-MAC/s",
                     "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": tr.total_launches // args.steps, "launches_by_entry": dict(tr.launches),
+            "gpu_launches": tr.total_launches, "gpu_launches_per_step": tr.total_launches // args.steps,
+            "launches_by_entry": dict(tr.launches),
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cholsolve_cpu_baseline(ns, os.cpu_count() or 1)
@@ -522,7 +533,8 @@ def solver_measurement(steps, warmup, local_rank, world=1):
             "last_row": {k: (mp.nstr(v, 6) if isinstance(v, mp.mpf) else v) for k, v in last.items()},
             "phase_s_per_iter": {k: v / total_it for k, v in sol.timer.totals().items()},
             "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / total_it for k in sorted(tr.events)},
-            "gpu_launches": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
+            "gpu_launches": tr.total_launches * len(timed) // max(1, total_it),
+            "gpu_launches_per_step": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
             "eig_refined": sol.eig_refined, "clocks": clk.summary()}
     return line
 

@@ -155,6 +155,13 @@ int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL,
 int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
                      int WL, int LF, void* stream);
 
+/* sdpv_crt_norm that runs only if *pred (a device int32) is nonzero, so that a caller can decide on the device
+ * whether a partial Gram sum must be reconstructed (GramAcc's flush, sdpvibe/mpf.py:557-616) without a host
+ * synchronisation.  When *pred is zero, O and eO are left untouched. */
+int sdpv_crt_norm_if(const sdpv_ctx* ctx, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                     int64_t rows, int64_t rows_per_block, const int64_t* rowexp, const int64_t* colexp, int L,
+                     int32_t* O, int64_t* eO, const int32_t* pred, void* stream);
+
 /* Eigenvalues of nb symmetric float64 n x n matrices A (nb, n, n) (n <= 128), ascending into w (nb, n), with an
  * error bound per matrix in err (nb) and the sweep count in sweeps (nb, may be NULL): batched cyclic Jacobi.
  * The device counterpart of the host LAPACK call in the step length (sdpvibe/solver.py:1064-1093, the

@@ -40,6 +40,7 @@ _SIGS = {
     "sdpv_rns_gemm": [_P, _P, _P, _P, _P, _L, _L, _P, _L, _I, _I, _L, _L, _L, _L, _I, _P],
     "sdpv_crt_block": [_P, _P, _L, _L, _L, _L, _L, _P, _P, _P],
     "sdpv_crt_norm": [_P, _P, _L, _L, _L, _L, _L, _L, _P, _P, _I, _P, _P, _P],
+    "sdpv_crt_norm_if": [_P, _P, _L, _L, _L, _L, _L, _L, _P, _P, _I, _P, _P, _P, _P],
     "sdpv_chol_tiles": [_P, _P, _L, _I, _I, _I, _P],
     "sdpv_trinv_tiles": [_P, _P, _P, _P, _L, _I, _I, _I, _P],
     "sdpv_trinv_tiles_noalloc": [_P, _P, _P, _L, _I, _I, _I, _P],

@@ -44,7 +44,9 @@ __global__ void __launch_bounds__(kThreads)
                const int64_t* __restrict__ rowexp, const int64_t* __restrict__ colexp, int L, int n, int E, int W,
                int ktc, int Epad, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                const int32_t* __restrict__ invs, const int32_t* __restrict__ md, const uint8_t* __restrict__ ct,
-               int32_t* __restrict__ out, int64_t* __restrict__ out2, unsigned* __restrict__ err) {
+               int32_t* __restrict__ out, int64_t* __restrict__ out2, const int32_t* __restrict__ pred,
+               unsigned* __restrict__ err) {
+  if (pred && *pred == 0) return;                      // predicated launch: nothing to do this time
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   CrtSmemHead& H = *reinterpret_cast<CrtSmemHead*>(base);
@@ -215,7 +217,8 @@ __global__ void __launch_bounds__(kThreads)
 
 template <int MODE>
 int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rpb,
-               const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st) {
+               const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st,
+               const int32_t* pred = nullptr) {
   const CtxDev& d = c->d;
   if (d.n > kNmax || d.E > kEmax) return SDPV_EINVAL;
   size_t smem = 1024 + 8192 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
@@ -238,7 +241,7 @@ int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i6
   if (gx > ntiles) gx = ntiles;
   crt_kernel<MODE><<<(unsigned)gx, kThreads, smem, st>>>(acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, d.n, d.E,
                                                           d.W, d.ktc, d.Epad, d.mods, d.minv, d.inv, d.md, d.ct, out,
-                                                          out2, device_error_word());
+                                                          out2, pred, device_error_word());
   return launch_status();
 }
 
@@ -261,4 +264,15 @@ extern "C" int sdpv_crt_norm(const sdpv_ctx* c, const int16_t* acc, int64_t ldg,
   if (rows == 0 || w == 0) return SDPV_OK;
   return launch_crt<1>(c, acc, ldg, N, j0, w, rows, rows_per_block, rowexp, colexp, L, O, eO,
                        sdpv::as_stream(stream));
+}
+
+extern "C" int sdpv_crt_norm_if(const sdpv_ctx* c, const int16_t* acc, int64_t ldg, int64_t N, int64_t j0, int64_t w,
+                                int64_t rows, int64_t rows_per_block, const int64_t* rowexp, const int64_t* colexp,
+                                int L, int32_t* O, int64_t* eO, const int32_t* pred, void* stream) {
+  if (!c || !pred || N < 0 || j0 < 0 || w < 0 || j0 + w > N || rows < 0 || rows_per_block < 1 || L < 1 || L > 160 ||
+      c->d.W > 160)
+    return SDPV_EINVAL;
+  if (rows == 0 || w == 0) return SDPV_OK;
+  return launch_crt<1>(c, acc, ldg, N, j0, w, rows, rows_per_block, rowexp, colexp, L, O, eO,
+                       sdpv::as_stream(stream), pred);
 }

@@ -394,7 +394,11 @@ class GramAcc:
     """Q = sum over chunks of P_c^T P_c, accumulated exactly in residues (lower-triangle tiles only)
     against running column reference exponents E_j, reconstructed by one CRT
     (sdpvibe/mpf.py:536-630).  A column that outgrows its HEAD bits of headroom forces a flush (CRT of
-    the partial sum, added in MPF).  Only the lower triangle of the result is defined."""
+    the partial sum, added in MPF).  Only the lower triangle of the result is defined.
+
+    The flush decision is taken on the device (a predicated CRT and selections instead of a host branch),
+    so ``add`` never waits for the GPU and a whole accumulation can be captured in a CUDA graph; the
+    arithmetic, and so every bit of the result, is that of the host-branch formulation."""
     HEAD = 28
 
     def __init__(self, N, L, E_ref=None):
@@ -403,8 +407,13 @@ class GramAcc:
         self.E = E_ref.clone() if E_ref is not None else torch.full((N,), EZ, dtype=torch.int64, device=dev)
         self.Tmax = torch.full((N,), EZ, dtype=torch.int64, device=dev)
         self.acc = None
-        self.part = None
-        self.flushes = 0
+        self.part = None                       # partial sum of flushed chunks, valid where _has != 0
+        self._has = torch.zeros((), dtype=torch.int32, device=dev)
+        self._nflush = torch.zeros((), dtype=torch.int64, device=dev)
+
+    @property
+    def flushes(self):
+        return int(self._nflush)
 
     def add(self, P):
         """P: MPF (rows, N)."""
@@ -413,10 +422,11 @@ class GramAcc:
         live = tp > EZ // 2
         self.Tmax = torch.maximum(self.Tmax, tp)
         known = self.E > EZ // 2
-        if bool((live & known & (tp > self.E + self.HEAD)).any()):
-            self._flush()
-            self.E = torch.where(live & (tp > self.E), tp, self.E)
-            known = self.E > EZ // 2
+        f = (live & known & (tp > self.E + self.HEAD)).any()         # flush?  (device bool)
+        if self.acc is not None:
+            self._flush_if(f)
+        self.E = torch.where(f & live & (tp > self.E), tp, self.E)
+        known = self.E > EZ // 2
         self.E = torch.where(live & ~known, tp, self.E)
         rows = P.shape[0]
         # columns aligned to E_j - NB in L+1 limbs and transposed to (N, rows), one kernel
@@ -428,19 +438,28 @@ class GramAcc:
             from .mpmat import residue_product
             residue_product(R, X, None, self.acc, syrk=True)
 
-    def _crt(self):
+    def _crt(self, pred=None):
         L, N, R = self.L, self.N, self.R
         rE = torch.where(self.E > EZ // 2, self.E - NBITS(L), torch.zeros_like(self.E))
-        Om, Oe = R.crt_norm(self.acc, self.acc.shape[2], 0, N, N, rE, rE[None, :], L)
+        Om, Oe = R.crt_norm(self.acc, self.acc.shape[2], 0, N, N, rE, rE[None, :], L, pred=pred)
         return MPF(Om.view(L, N, N), Oe.view(N, N))
 
+    def _flush_if(self, f):
+        """where f: part += CRT(acc) (part = CRT(acc) if empty), acc = 0, one more flush"""
+        fi = f.to(torch.int32)
+        q = self._crt(pred=fi)
+        if self.part is None:
+            self.part = q
+        else:
+            self.part = _select(self._has != 0, add(self.part, q), q, f, self.part)
+        self._has = self._has | fi
+        self.acc.masked_fill_(f, 0)
+        self._nflush += fi
+
     def _flush(self):
-        if self.acc is None:
-            return
-        q = self._crt()
-        self.part = q if self.part is None else add(self.part, q)
-        self.acc = None
-        self.flushes += 1
+        if self.acc is not None:
+            self._flush_if(torch.ones((), dtype=torch.bool, device=dev))
+            self.acc = None
 
     def next_reference(self, margin=4):
         return torch.where(self.Tmax > EZ // 2, self.Tmax + margin, self.Tmax)
@@ -454,7 +473,18 @@ class GramAcc:
             return self.part
         q = self._crt()
         self.acc = None
-        return q if self.part is None else add(self.part, q)
+        if self.part is None:
+            return q
+        h = self._has != 0
+        s = add(self.part, q)
+        return MPF(torch.where(h, s.m, q.m), torch.where(h, s.e, q.e))
+
+
+def _select(h, a, b, f, old):
+    """f ? (h ? a : b) : old, entrywise on MPF (h, f device bools)"""
+    m = torch.where(f, torch.where(h, a.m, b.m), old.m)
+    e = torch.where(f, torch.where(h, a.e, b.e), old.e)
+    return MPF(m, e)
 
 
 # ------------------------------------------------------------------ Cholesky (equilibrated, batched)

@@ -105,15 +105,19 @@ class RNS:
                   _lib.ptr(bl), _lib.stream())
         return Wd, bl, B
 
-    def crt_norm(self, acc, N, j0, w, rows, rowexp, colexp, L, rows_per_block=None):
+    def crt_norm(self, acc, N, j0, w, rows, rowexp, colexp, L, rows_per_block=None, pred=None):
         """CRT fused with MPF renormalisation: entry (r, jj) gets exponent
-        rowexp[r] + colexp[r // rows_per_block, j0 + jj]; returns (m (L, rows*w), e (rows*w,))."""
+        rowexp[r] + colexp[r // rows_per_block, j0 + jj]; returns (m (L, rows*w), e (rows*w,)).
+        pred (device int32 scalar): run only where it is nonzero (the outputs are undefined otherwise)."""
         B = rows * w
         O = torch.empty((L, B), dtype=torch.int32, device=acc.device)
         eO = torch.empty((B,), dtype=torch.int64, device=acc.device)
-        _lib.call("sdpv_crt_norm", self._h, _lib.ptr(acc), acc.stride(0), N, j0, w, rows, rows_per_block or rows,
-                  _lib.ptr(rowexp.contiguous()), _lib.ptr(colexp.contiguous()), L, _lib.ptr(O), _lib.ptr(eO),
-                  _lib.stream())
+        args = (self._h, _lib.ptr(acc), acc.stride(0), N, j0, w, rows, rows_per_block or rows,
+                _lib.ptr(rowexp.contiguous()), _lib.ptr(colexp.contiguous()), L, _lib.ptr(O), _lib.ptr(eO))
+        if pred is None:
+            _lib.call("sdpv_crt_norm", *args, _lib.stream())
+        else:
+            _lib.call("sdpv_crt_norm_if", *args, _lib.ptr(pred), _lib.stream())
         return O, eO
 
 
