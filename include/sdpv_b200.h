@@ -155,6 +155,12 @@ int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL,
 int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int bt,
                      int WL, int LF, void* stream);
 
+/* sdpv_mpf_add that runs only if *pred (a device int32) is nonzero; O may alias A (in-place accumulation).
+ * With sdpv_crt_norm_if it lets GramAcc add a flushed partial sum without a host decision
+ * (sdpvibe/mpf.py:612-616). */
+int sdpv_mpf_add_if(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
+                    int sgn, int32_t* O, int64_t* eO, const int32_t* pred, void* stream);
+
 /* sdpv_crt_norm that runs only if *pred (a device int32) is nonzero, so that a caller can decide on the device
  * whether a partial Gram sum must be reconstructed (GramAcc's flush, sdpvibe/mpf.py:557-616) without a host
  * synchronisation.  When *pred is zero, O and eO are left untouched. */

@@ -161,11 +161,12 @@ __global__ void mpf_mul_kernel(int L, i64 n, const int32_t* __restrict__ A, cons
 }
 
 template <int LMAX>
-__global__ void mpf_add_kernel(int L, i64 n, const int32_t* __restrict__ A, const i64* __restrict__ eA,
+__global__ void mpf_add_kernel(int L, i64 n, const int32_t* A, const i64* eA,
                                const int32_t* __restrict__ Bm, const i64* __restrict__ eB, int sgn,
-                               int32_t* __restrict__ O, i64* __restrict__ eO) {
+                               int32_t* O, i64* eO, const int32_t* __restrict__ pred) {
   i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (pred && *pred == 0) return;                      // predicated launch: O / eO untouched
   u32 a[LMAX], b[LMAX], wa[LMAX + 2], wb[LMAX + 2], r[LMAX];
   for (int k = 0; k < L; k++) {
     a[k] = (u32)A[(i64)k * n + i];
@@ -305,7 +306,17 @@ extern "C" int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* e
   if (L < 1 || L > 160 || n < 0) return SDPV_EINVAL;
   if (n == 0) return SDPV_OK;
   cudaStream_t st = sdpv::as_stream(stream);
-  SDPV_LMAX_DISPATCH(L, mpf_add_kernel, L, n, A, eA, Bm, eB, sgn, O, eO);
+  SDPV_LMAX_DISPATCH(L, mpf_add_kernel, L, n, A, eA, Bm, eB, sgn, O, eO, (const int32_t*)nullptr);
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_mpf_add_if(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm,
+                               const int64_t* eB, int sgn, int32_t* O, int64_t* eO, const int32_t* pred,
+                               void* stream) {
+  if (L < 1 || L > 160 || n < 0 || !pred) return SDPV_EINVAL;
+  if (n == 0) return SDPV_OK;
+  cudaStream_t st = sdpv::as_stream(stream);
+  SDPV_LMAX_DISPATCH(L, mpf_add_kernel, L, n, A, eA, Bm, eB, sgn, O, eO, pred);
   return sdpv::launch_status();
 }
 

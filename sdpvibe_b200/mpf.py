@@ -396,7 +396,8 @@ class GramAcc:
     (sdpvibe/mpf.py:536-630).  A column that outgrows its HEAD bits of headroom forces a flush (CRT of
     the partial sum, added in MPF).  Only the lower triangle of the result is defined.
 
-    The flush decision is taken on the device (a predicated CRT and selections instead of a host branch),
+    The flush decision is taken on the device (a predicated CRT and a predicated in-place MPF add instead
+    of a host branch),
     so ``add`` never waits for the GPU and a whole accumulation can be captured in a CUDA graph; the
     arithmetic, and so every bit of the result, is that of the host-branch formulation."""
     HEAD = 28
@@ -407,8 +408,7 @@ class GramAcc:
         self.E = E_ref.clone() if E_ref is not None else torch.full((N,), EZ, dtype=torch.int64, device=dev)
         self.Tmax = torch.full((N,), EZ, dtype=torch.int64, device=dev)
         self.acc = None
-        self.part = None                       # partial sum of flushed chunks, valid where _has != 0
-        self._has = torch.zeros((), dtype=torch.int32, device=dev)
+        self.part = None                       # sum of the flushed partial sums (zero until the first flush)
         self._nflush = torch.zeros((), dtype=torch.int64, device=dev)
 
     @property
@@ -445,21 +445,17 @@ class GramAcc:
         return MPF(Om.view(L, N, N), Oe.view(N, N))
 
     def _flush_if(self, f):
-        """where f: part += CRT(acc) (part = CRT(acc) if empty), acc = 0, one more flush"""
+        """where f (device bool): part += CRT(acc), acc = 0, one more flush.  part starts at zero, and
+        0 + q is q itself (q is normalised), so the first flush gives the reference's part = q."""
         fi = f.to(torch.int32)
         q = self._crt(pred=fi)
         if self.part is None:
-            self.part = q
-        else:
-            self.part = _select(self._has != 0, add(self.part, q), q, f, self.part)
-        self._has = self._has | fi
+            self.part = zeros((self.N, self.N), self.L)
+        n = self.N * self.N
+        _lib.call("sdpv_mpf_add_if", self.L, n, _lib.ptr(self.part.m), _lib.ptr(self.part.e), _lib.ptr(q.m),
+                  _lib.ptr(q.e), 1, _lib.ptr(self.part.m), _lib.ptr(self.part.e), _lib.ptr(fi), _lib.stream())
         self.acc.masked_fill_(f, 0)
         self._nflush += fi
-
-    def _flush(self):
-        if self.acc is not None:
-            self._flush_if(torch.ones((), dtype=torch.bool, device=dev))
-            self.acc = None
 
     def next_reference(self, margin=4):
         return torch.where(self.Tmax > EZ // 2, self.Tmax + margin, self.Tmax)
@@ -473,18 +469,7 @@ class GramAcc:
             return self.part
         q = self._crt()
         self.acc = None
-        if self.part is None:
-            return q
-        h = self._has != 0
-        s = add(self.part, q)
-        return MPF(torch.where(h, s.m, q.m), torch.where(h, s.e, q.e))
-
-
-def _select(h, a, b, f, old):
-    """f ? (h ? a : b) : old, entrywise on MPF (h, f device bools)"""
-    m = torch.where(f, torch.where(h, a.m, b.m), old.m)
-    e = torch.where(f, torch.where(h, a.e, b.e), old.e)
-    return MPF(m, e)
+        return q if self.part is None else add(self.part, q)
 
 
 # ------------------------------------------------------------------ Cholesky (equilibrated, batched)
