@@ -473,6 +473,49 @@ def run_cholsolve(args, rank, world, local_rank):
 CS_LIMBS_NOTE = "26 (832 bits); base tiles in WL = 50-word fixed point"
 
 
+# ------------------------------------------------------------------ objective sensitivity at the final iterate
+def run_sensitivity(args, rank, world, local_rank):
+    """The Ising-structured SDP after `--iters` solver iterations (default 20): linear response of the primal
+    objective along 64 Gaussian unit directions in (B, c) (numpy seed 1), one direction in memory at a time
+    (a direction over all chunks is 25830 x 1000 MPF entries).  Metric: device ms per direction."""
+    import torch
+    from sdpvibe_b200.solver import Solver
+    from sdpvibe_b200.synthetic import ising_like_sdp
+    from sdpvibe_b200.adjoint import objective_sensitivity, random_directions
+    import mpmath as mp
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    Ls, ndir = 26, 64
+    sdp, _ = ising_like_sdp(Ls)
+    sol = Solver(sdp, Ls)
+    iters = args.iters
+    sol.run(max_iter=iters)
+    rng_seed = 1
+    times, vals = [], []
+    for k in range(ndir):
+        d = random_directions(sdp, 1, seed=rng_seed + 1000 * k)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        v = objective_sensitivity(sol, d)[0]
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+        vals.append(v)
+        del d
+    if rank != 0:
+        return
+    ms = statistics.mean(times[1:])
+    line = {"metric": "objective sensitivity (linear response) per direction at the final iterate, ms",
+            "value": ms, "unit": "ms/direction", "n_gpus": world, "steps": ndir, "warmup": 1, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "832-bit MPF (L=26)",
+            "data": "synthetic",
+            "config": {"workload": f"sensitivity: ising_like SDP after {iters} iterations, {ndir} Gaussian unit "
+                                   "directions in (B, c) (numpy seed 1 + 1000 k), one at a time"},
+            "first_values": [mp.nstr(v, 12) for v in vals[:4]]}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ full solver iterations (SDP s/iter)
 def run_solver(args, rank, world, local_rank):
     """SDPB iterations on the Ising-structured synthetic SDP: 300 blocks (dims 1/2/3 = 180/90/30,
@@ -546,8 +589,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--iters", type=int, default=20, help="sensitivity: solver iterations before the sensitivities")
     ap.add_argument("--no-solver", action="store_true", help="gram: skip the SDP s/iteration measurement")
-    ap.add_argument("--workload", choices=("gram", "cholsolve", "solver"), default="gram",
+    ap.add_argument("--workload", choices=("gram", "cholsolve", "solver", "sensitivity"), default="gram",
                     help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "
                          "solver: SDPB iterations (s/iter)")
     args = ap.parse_args()
@@ -563,7 +607,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run = {"gram": run_b200, "cholsolve": run_cholsolve, "solver": run_solver}[args.workload]
+        run = {"gram": run_b200, "cholsolve": run_cholsolve, "solver": run_solver,
+               "sensitivity": run_sensitivity}[args.workload]
         run(args, rank, world, local_rank)
     finally:
         if world > 1:
