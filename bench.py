@@ -475,44 +475,92 @@ CS_LIMBS_NOTE = "26 (832 bits); base tiles in WL = 50-word fixed point"
 
 # ------------------------------------------------------------------ objective sensitivity at the final iterate
 def run_sensitivity(args, rank, world, local_rank):
-    """The Ising-structured SDP after `--iters` solver iterations (default 20): linear response of the primal
-    objective along 64 Gaussian unit directions in (B, c) (numpy seed 1), one direction in memory at a time
-    (a direction over all chunks is 25830 x 1000 MPF entries).  Metric: device ms per direction."""
+    """Objective sensitivity on the Ising-structured SDP (300 blocks, N = 1000, L = 26) after `--iters`
+    solver iterations (default 20): f(B, c) = c.(x + dx(B, c)), the primal objective after a Newton step
+    from the final iterate, differentiated by its adjoint (one adjoint solve with the Schur and Q factors,
+    then per direction one GEMM dB [y+dy, v] and dot products), along 64 Gaussian unit directions in (B, c)
+    from one numpy generator (seed 1), one direction in memory at a time (25830 x 1000 MPF entries).
+    value: device ms per direction (direction resident); e2e: per direction from the host float64 arrays
+    (conversion and copy inside).  The first `--fd-dirs` directions are checked against central differences
+    of f at L = 50 (1536-bit class precision, h = 2^-300), and the envelope value dc.x - x^T dB y is
+    reported beside each."""
     import torch
+    import mpmath as mp
     from sdpvibe_b200.solver import Solver
     from sdpvibe_b200.synthetic import ising_like_sdp
-    from sdpvibe_b200.adjoint import objective_sensitivity, random_directions
-    import mpmath as mp
+    from sdpvibe_b200.adjoint import NewtonObjective, iter_directions, direction_to_mpf, widen
+    from sdpvibe_b200.mpf import add
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    Ls, ndir = 26, 64
+    Ls, L2, ndir, hk = 26, 50, 64, 300
     sdp, _ = ising_like_sdp(Ls)
     sol = Solver(sdp, Ls)
     iters = args.iters
     sol.run(max_iter=iters)
-    rng_seed = 1
-    times, vals = [], []
-    for k in range(ndir):
-        d = random_directions(sdp, 1, seed=rng_seed + 1000 * k)
+
+    def timed(fn):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        v = objective_sensitivity(sol, d)[0]
+        r = fn()
         b.record()
         b.synchronize()
-        times.append(a.elapsed_time(b))
-        vals.append(v)
-        del d
+        return r, a.elapsed_time(b)
+    fo, t_setup = timed(lambda: NewtonObjective(sol))
+    f0, t_fwd = timed(fo.forward)
+    _, t_adj = timed(fo._adjoint)
+    times, e2e, vals, env = [], [], [], []
+    h2d = 0
+    for k, hd in enumerate(iter_directions(sdp, ndir, seed=1, host=True)):
+        h2d = sum(dB.nbytes + dc.nbytes for dB, dc in hd)
+        def through_host():
+            dd = direction_to_mpf(hd, Ls)
+            return dd, fo.directional([x for x, _ in dd], [y for _, y in dd])
+        (d, (da, de)), te = timed(through_host)
+        _, t = timed(lambda: fo.directional([x for x, _ in d], [y for _, y in d]))
+        times.append(t)
+        e2e.append(te)
+        vals.append(da)
+        env.append(de)
+        del d, hd
+    fd = []
+    t_fd = None
+    if args.fd_dirs > 0:
+        t0 = time.time()
+        hi = NewtonObjective(sol, L=L2)
+        with mp.workprec(32 * L2 + 64):
+            for k, d in enumerate(iter_directions(sdp, min(args.fd_dirs, ndir), seed=1)):   # the same directions
+                wd = [(widen(dB, L2).shift(-hk), widen(dc, L2).shift(-hk)) for dB, dc in d]
+                fp = hi.forward([add(g.B, dB) for g, (dB, _) in zip(hi.sdp.groups, wd)],
+                                [add(g.c, dc) for g, (_, dc) in zip(hi.sdp.groups, wd)])
+                fm = hi.forward([add(g.B, dB, -1) for g, (dB, _) in zip(hi.sdp.groups, wd)],
+                                [add(g.c, dc, -1) for g, (_, dc) in zip(hi.sdp.groups, wd)])
+                v = (fp - fm) * mp.mpf(2) ** (hk - 1)
+                fd.append(float(-mp.log10(abs(vals[k] - v) / abs(v))) if vals[k] != v else 999.0)
+        torch.cuda.synchronize()
+        t_fd = time.time() - t0
     if rank != 0:
         return
-    ms = statistics.mean(times[1:])
-    line = {"metric": "objective sensitivity (linear response) per direction at the final iterate, ms",
-            "value": ms, "unit": "ms/direction", "n_gpus": world, "steps": ndir, "warmup": 1, "ms_per_step": ms,
+    ms = statistics.mean(times)
+    rel_env = [float(abs(a - b) / abs(b)) if b else None for a, b in zip(vals, env)]
+    line = {"metric": "objective sensitivity (adjoint directional derivative) per direction at the final iterate",
+            "value": ms, "unit": "ms/direction", "n_gpus": world, "steps": ndir, "warmup": 0, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "832-bit MPF (L=26)",
             "data": "synthetic",
-            "config": {"workload": f"sensitivity: ising_like SDP after {iters} iterations, {ndir} Gaussian unit "
-                                   "directions in (B, c) (numpy seed 1 + 1000 k), one at a time"},
-            "first_values": [mp.nstr(v, 12) for v in vals[:4]]}
+            "config": {"workload": f"sensitivity: ising_like SDP (300 blocks, N 1000) after {iters} iterations; "
+                                   f"f = c.(x + dx), {ndir} Gaussian unit directions in (B, c) (numpy seed 1)",
+                       "inputs": "each direction 2.7 GB in MPF (larger than L2)"},
+            "e2e": {"value": statistics.mean(e2e), "unit": "ms/direction", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 5 * len(sdp.groups) * 8 * (Ls + 2)},
+            "setup_ms": t_setup, "forward_ms": t_fwd, "adjoint_solve_ms": t_adj,
+            "fd_check": {"L": L2, "h": f"2^-{hk}", "directions": len(fd),
+                         "min_digits": min(fd) if fd else None, "digits": fd, "seconds": t_fd},
+            "envelope_rel_diff": {"min": min(r for r in rel_env if r is not None),
+                                  "median": statistics.median(r for r in rel_env if r is not None),
+                                  "max": max(r for r in rel_env if r is not None)},
+            "objective_after_newton_step": mp.nstr(f0, 30),
+            "first_values": [mp.nstr(v, 20) for v in vals[:4]],
+            "first_envelope_values": [mp.nstr(v, 20) for v in env[:4]]}
     print(json.dumps(line), flush=True)
 
 
@@ -590,6 +638,7 @@ def main():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--iters", type=int, default=20, help="sensitivity: solver iterations before the sensitivities")
+    ap.add_argument("--fd-dirs", type=int, default=8, help="sensitivity: directions checked by finite differences")
     ap.add_argument("--no-solver", action="store_true", help="gram: skip the SDP s/iteration measurement")
     ap.add_argument("--workload", choices=("gram", "cholsolve", "solver", "sensitivity"), default="gram",
                     help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "

@@ -86,6 +86,10 @@ int sdpv_mpf_mul(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
 /* O = A + sgn*B entrywise.  Replaces mpf.add / mpf_add (sdpvibe/mpf.py:92-124, 326-331). */
 int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
                  int sgn, int32_t* O, int64_t* eO, void* stream);
+/* float64 values V (n) -> normalised MPF (L >= 2 limbs), exactly; zeros -> EZ; a non-finite value
+ * becomes zero and sets SDPV_ERRBIT_OVERFLOW.  Replaces the host frexp conversion of
+ * sdpvibe/solver.py:1012-1018 (the float64 -> mpf step of the step-length code). */
+int sdpv_mpf_from_f64(int L, int64_t n, const double* V, int32_t* O, int64_t* eO, void* stream);
 /* Normalise LI-limb integers with exponents eI to MPF with L limbs (LI <= 160).
  * Replaces mpf.normalize / mpf_norm (sdpvibe/mpf.py:127-140, 307-313). */
 int sdpv_mpf_norm(int L, int LI, int64_t n, const int32_t* X, const int64_t* eI, int32_t* O, int64_t* eO,

@@ -244,6 +244,48 @@ __global__ void mpf_norm_kernel(int L, int LI, i64 n, const int32_t* __restrict_
   eO[i] = eI[i] + s;
 }
 
+// float64 -> normalised MPF, exactly: the 53-bit significand (subnormals included) shifted to NB = 32L-2 bits
+// (NB >= 62 for L >= 2, so no rounding).  The normalised form is unique, so this equals normalising the
+// two-limb integer of frexp (sdpvibe/solver.py:1012-1018).  Zeros (either sign) -> m = 0, e = EZ; a
+// non-finite input -> zero and the overflow bit in the device error word.
+__global__ void from_f64_kernel(int L, i64 n, const double* __restrict__ V, int32_t* __restrict__ O,
+                                i64* __restrict__ eO, unsigned* __restrict__ err) {
+  i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const u64 bits = (u64)__double_as_longlong(__ldg(V + i));
+  const bool ng = bits >> 63;
+  const int bexp = (int)((bits >> 52) & 0x7ff);
+  u64 mant = bits & ((1ull << 52) - 1);
+  i64 ex = -1074;
+  if (bexp == 0x7ff) {
+    atomicOr(err, SDPV_ERRBIT_OVERFLOW);
+    mant = 0;
+  } else if (bexp) {
+    mant |= 1ull << 52;
+    ex = bexp - 1075;
+  }
+  if (!mant) {
+    for (int k = 0; k < L; k++) O[(i64)k * n + i] = 0;
+    eO[i] = SDPV_EZ;
+    return;
+  }
+  const int bl = 64 - __clzll((long long)mant);
+  const int sh = 32 * L - 2 - bl;                     // >= 9
+  const int q = sh >> 5;
+  const unsigned __int128 t = (unsigned __int128)mant << (sh & 31);
+  u32 carry = 1;
+  for (int k = 0; k < L; k++) {
+    const int j = k - q;
+    u32 w = (j >= 0 && j < 3) ? (u32)(t >> (32 * j)) : 0u;
+    if (ng) {
+      w = ~w + carry;
+      carry = carry && w == 0;
+    }
+    O[(i64)k * n + i] = (int32_t)w;
+  }
+  eO[i] = ex - sh;
+}
+
 inline unsigned blocks(i64 n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 #define SDPV_LMAX_DISPATCH(L, KERNEL, ...)                                     \
@@ -317,6 +359,13 @@ extern "C" int sdpv_mpf_add_if(int L, int64_t n, const int32_t* A, const int64_t
   if (n == 0) return SDPV_OK;
   cudaStream_t st = sdpv::as_stream(stream);
   SDPV_LMAX_DISPATCH(L, mpf_add_kernel, L, n, A, eA, Bm, eB, sgn, O, eO, pred);
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_mpf_from_f64(int L, int64_t n, const double* V, int32_t* O, int64_t* eO, void* stream) {
+  if (L < 2 || L > 160 || n < 0) return SDPV_EINVAL;
+  if (n == 0) return SDPV_OK;
+  from_f64_kernel<<<blocks(n), kThreads, 0, sdpv::as_stream(stream)>>>(L, n, V, O, eO, sdpv::device_error_word());
   return sdpv::launch_status();
 }
 

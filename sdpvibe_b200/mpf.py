@@ -198,14 +198,19 @@ def from_mp(vals, L, shape=None):
 
 # ------------------------------------------------------------------ elementwise kernels
 def from_float(V, L):
-    """float64 array -> MPF, exactly: 53-bit mantissas as two 32-bit limbs, then normalised
-    (sdpvibe/solver.py:1012-1018)."""
-    V = np.asarray(V, dtype=np.float64)
-    m, e = np.frexp(V)
-    mi = (m * 2.0 ** 53).astype(np.int64).reshape(-1)
-    w = np.stack([(mi & 0xFFFFFFFF).astype(np.uint32).view(np.int32), (mi >> 32).astype(np.int32)])
-    ein = np.where(mi != 0, e.reshape(-1).astype(np.int64) - 53, EZ)
-    return normalize(torch.from_numpy(w).to(dev), torch.from_numpy(ein).to(dev), L).reshape(*V.shape)
+    """float64 array (numpy, or a torch tensor on the device) -> MPF, exactly: the significand shifted to
+    NB bits on the device (sdpvibe/solver.py:1012-1018).  A non-finite value becomes zero and sets the
+    overflow bit of the device error word (``_lib.device_error_flags``)."""
+    if torch.is_tensor(V):
+        Vd = V.to(device=dev, dtype=torch.float64).contiguous()
+    else:
+        Vd = torch.from_numpy(np.ascontiguousarray(V, dtype=np.float64)).to(dev)
+    shape = tuple(Vd.shape)
+    n = Vd.numel()
+    O = torch.empty((L, n), dtype=torch.int32, device=dev)
+    eO = torch.empty((n,), dtype=torch.int64, device=dev)
+    _lib.call("sdpv_mpf_from_f64", L, n, _lib.ptr(Vd), _lib.ptr(O), _lib.ptr(eO), _lib.stream())
+    return MPF(O, eO).reshape(*shape)
 
 
 def normalize(Xw, ein, L):

@@ -444,6 +444,7 @@ def test_from_float_matches_oracle(sb):
     rs = np.random.default_rng(7)
     V = rs.standard_normal((3, 5, 5)) * 2.0 ** np.random.default_rng(8).integers(-900, 900, (3, 5, 5))
     V[0, 0, 0] = 0
+    V[1, 0, :] = [5e-324, -2.5e-310, -0.0, 1.7976931348623157e308, -1.0]      # subnormals, -0, extremes
     for L in (2, 26, 40):
         got = from_float(V, L)
         rm, re_ = OM.mpf_from_float(V, L)
