@@ -589,16 +589,21 @@ def solver_measurement(steps, warmup, local_rank, world=1):
     sol = Solver(sdp, Ls, timing=True)
     marks = []
 
+    warm = max(warmup, 1)
+    total_it = warm + steps
+
     def rec(it, s, info):
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
         marks.append((it, ev, info["row"]))
+        if it == warm:                          # phase and kernel tables over the timed iterations only
+            s.timer.marks.clear()
+            tr.launches.clear()
+            tr.events.clear()
     names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
              "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
-    tr = _trace.Trace(timed=names)              # graph replays are timed whole, as "graph_replay"
-    warm = max(warmup, 1)
-    total_it = warm + steps
+    tr = _trace.Trace(timed=names)              # graph replays are timed whole, one entry per graph key
     with ClockSampler(local_rank) as clk, tr:
         torch.cuda.synchronize()
         start = torch.cuda.Event(enable_timing=True)
@@ -622,10 +627,11 @@ def solver_measurement(steps, warmup, local_rank, world=1):
                        "l2": "working set of several GB; no flush"},
             "per_iteration_s": per_it, "build_s": t_build,
             "last_row": {k: (mp.nstr(v, 6) if isinstance(v, mp.mpf) else v) for k, v in last.items()},
-            "phase_s_per_iter": {k: v / total_it for k, v in sol.timer.totals().items()},
-            "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / total_it for k in sorted(tr.events)},
-            "gpu_launches": tr.total_launches * len(timed) // max(1, total_it),
-            "gpu_launches_per_step": tr.total_launches // max(1, total_it), "launches_by_entry": dict(tr.launches),
+            "tables_over": f"the {steps} timed iterations (plus the residue phase of the final evaluation)",
+            "phase_s_per_iter": {k: v / steps for k, v in sol.timer.totals().items()},
+            "kernel_s_per_iter": {k: sum(tr.kernel_ms(k)) * 1e-3 / steps for k in sorted(tr.events)},
+            "gpu_launches": tr.total_launches,
+            "gpu_launches_per_step": tr.total_launches // max(1, steps), "launches_by_entry": dict(tr.launches),
             "eig_refined": sol.eig_refined, "clocks": clk.summary()}
     return line
 

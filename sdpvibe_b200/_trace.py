@@ -54,9 +54,9 @@ def before(name):
     return None
 
 
-def replay(launches):
+def replay(launches, label="graph_replay"):
     """A CUDA graph of recorded library launches is about to be replayed: count them, and time the replay
-    as "graph_replay" when the active trace times anything.  Returns the end event to record, or None."""
+    under `label` when the active trace times anything.  Returns the end event to record, or None."""
     t = _active
     if t is None:
         return None
@@ -65,5 +65,5 @@ def replay(launches):
         return None
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    t.events["graph_replay"].append((a, b))
+    t.events[label].append((a, b))
     return b

@@ -515,7 +515,7 @@ __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
   return (size_t)(528 + 32) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 5 * FW * 4 + 64;
 }
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
-  return (size_t)(528 + 32 + 288) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
+  return (size_t)(528 + 32) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
 }
 
 __device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
@@ -539,45 +539,59 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
     for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[w];
   }
   __syncthreads();
-  for (int k = 0; k < BT; k++) {
+  // Pivot k (warp 0): r = d^-1/2 by the Newton schedule, l_kk = d r, r kept in sr and RINV.
+  auto pivot = [&](int k) {
     u32* akk = T + (size_t)tri(k, k) * WL;
-    if (warp == 0) {
-      for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
-      for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
-      __syncwarp();
-      if (lane == 0) {
-        if ((sd[WL - 1] >> 31) || (top_word(sd, WL) == 0 && sd[0] == 0)) atomicOr(err, SDPV_ERRBIT_NOTSPD);
-        fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
-      }
-      __syncwarp();
-      for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
-        int t = bits / 32 + 2;
-        if (t >= WL) t = 0;
-        wmul(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
-        wmul(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-        warp_addsub(st1, sone, st2, true, WL);
-        wmul(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-        warp_shr1(st2, WL);
-        warp_addsub(sr, sr, st2, false, WL);
-        if (t == 0) break;
-      }
-      wmul(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);   // l_kk = d * d^-1/2
-      for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
+    for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
+    for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
+    __syncwarp();
+    if (lane == 0) {
+      if ((sd[WL - 1] >> 31) || (top_word(sd, WL) == 0 && sd[0] == 0)) atomicOr(err, SDPV_ERRBIT_NOTSPD);
+      fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
     }
-    __syncthreads();
+    __syncwarp();
+    for (int bits = 100;; bits *= 2) {                             // r <- r + r (1 - d r^2) / 2
+      int t = bits / 32 + 2;
+      if (t >= WL) t = 0;
+      wmul(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+      wmul(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+      warp_addsub(st1, sone, st2, true, WL);
+      wmul(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+      warp_shr1(st2, WL);
+      warp_addsub(sr, sr, st2, false, WL);
+      if (t == 0) break;
+    }
+    wmul(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);     // l_kk = d * d^-1/2
+    for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
+  };
+  if (warp == 0) pivot(0);
+  __syncthreads();
+  // Step k: column k scaled by r_k; then, with one pivot of look-ahead, warp 0 updates a_{k+1,k+1} and runs
+  // pivot k+1's Newton chain while warps 1.. apply the rest of step k's trailing update.  Every entry gets
+  // the same truncated products as without look-ahead (their exact sum is order-free).
+  for (int k = 0; k < BT; k++) {
     for (int i = k + 1 + warp; i < BT; i += kWarpsS) {           // l_ik = a_ik * r_k
       u32* aik = T + (size_t)tri(i, k) * WL;
       wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WL, colsign + i, coltop + i);
     }
     __syncthreads();
-    const int m = BT - k - 1, npairs = m * (m + 1) / 2;
-    for (int p = tid; p < npairs; p += kThreadsS) {               // a_ij -= l_ik l_jk, k < j <= i
-      int ii = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
-      while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
-      while (ii * (ii + 1) / 2 > p) ii--;
-      const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
-      fx_rmw(T + (size_t)tri(i, j) * WL, colmag + (size_t)i * WL, coltop[i], colmag + (size_t)j * WL, coltop[j],
-             colsign[i] != colsign[j], WL, LF);
+    if (k == BT - 1) break;
+    if (warp == 0) {
+      u32* dn = T + (size_t)tri(k + 1, k + 1) * WL;                // a_{k+1,k+1} -= l_{k+1,k}^2
+      const u32* lk = colmag + (size_t)(k + 1) * WL;
+      wmul(lk, lk, 0, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+      warp_addsub(dn, dn, st1, true, WL);
+      pivot(k + 1);
+    } else {
+      const int m = BT - k - 1, npairs = m * (m + 1) / 2;
+      for (int p = 1 + tid - 32; p < npairs; p += kThreadsS - 32) {   // a_ij -= l_ik l_jk, k < j <= i, but (k+1, k+1)
+        int ii = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+        while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
+        while (ii * (ii + 1) / 2 > p) ii--;
+        const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
+        fx_rmw(T + (size_t)tri(i, j) * WL, colmag + (size_t)i * WL, coltop[i], colmag + (size_t)j * WL, coltop[j],
+               colsign[i] != colsign[j], WL, LF);
+      }
     }
     __syncthreads();
   }
@@ -588,92 +602,58 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
   }
 }
 
-// Number of partial-sum slots of column k in row i when each slot takes up to c products.
-__device__ __forceinline__ int nslots(int i, int k, int c) { return (i - k + c - 1) / c; }
-
+// X = L^-1 right-looking: slot (i, k) of Xm first accumulates sum_j l_ij x_jk (two's complement, exact
+// modulo 2^(32 WL)) as the rows j < i are finished; row j+1 is finished as x_{j+1,k} = -(its sum) r_{j+1}.
+// Step j forms all (31 - j)(j + 1) <= 256 products l_ij x_jk (i > j, k <= j) in one round of threads, so
+// the critical path is one product round and one warp product per row.  The products and the final
+// products are the reference's; only the order of the exact sums differs.
 __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* __restrict__ Lt,
                                                                     const u32* __restrict__ RINV,
                                                                     u32* __restrict__ X, int WL, int LF) {
   extern __shared__ __align__(16) u32 sm[];
-  u32* Xm = sm;                                                  // |x_ik|, lower triangle
-  u32* Lrow = Xm + 528 * WL;                                     // |l_ij|, j < i, of the current row
-  u32* part = Lrow + 32 * WL;                                    // partial sums (two's complement)
-  WarpScratch* ws = reinterpret_cast<WarpScratch*>(part + 288 * WL);
-  uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of x
+  u32* Xm = sm;                                                  // slots tri(i, k), lower triangle
+  u32* Lcol = Xm + 528 * WL;                                     // |l_ij| of the current column j, by row i
+  WarpScratch* ws = reinterpret_cast<WarpScratch*>(Lcol + 32 * WL);
+  uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of finished x
   uint8_t* xt = xs + 528;
-  uint8_t* ls = xt + 528;                                        // signs, tops of the row of L
+  uint8_t* ls = xt + 528;                                        // signs, tops of the column of L
   uint8_t* lt = ls + 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const u32* LG = Lt + (size_t)blockIdx.x * BT * BT * WL;
   const u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
   u32* XG = X + (size_t)blockIdx.x * BT * BT * WL;
-  if (warp == 0) {                                               // x_00 = r_0
+  for (int e = tid; e < 528 * WL; e += kThreadsS) Xm[e] = 0;
+  __syncthreads();
+  for (int i = warp; i < BT; i += kWarpsS) {                     // x_ii = r_i
     int top;
-    const int sg = load_mag(RI, Xm, WL, top);
+    const int sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WL, WL, top);
     if (lane == 0) {
-      xs[0] = (uint8_t)sg;
-      xt[0] = (uint8_t)top;
+      xs[tri(i, i)] = (uint8_t)sg;
+      xt[tri(i, i)] = (uint8_t)top;
     }
   }
-  for (int i = 1; i < BT; i++) {
-    for (int j = warp; j <= i; j += kWarpsS) {
-      int top, sg;
-      if (j < i) {
-        sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lrow + (size_t)j * WL, WL, top);
-        if (lane == 0) {
-          ls[j] = (uint8_t)sg;
-          lt[j] = (uint8_t)top;
-        }
-      } else {                                                   // x_ii = r_i
-        sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WL, WL, top);
-        if (lane == 0) {
-          xs[tri(i, i)] = (uint8_t)sg;
-          xt[tri(i, i)] = (uint8_t)top;
-        }
+  for (int j = 0; j < BT - 1; j++) {
+    for (int i = j + 1 + warp; i < BT; i += kWarpsS) {
+      int top;
+      const int sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WL, WL, top);
+      if (lane == 0) {
+        ls[i] = (uint8_t)sg;
+        lt[i] = (uint8_t)top;
       }
     }
     __syncthreads();
-    // partial sums of l_ij x_jk over runs of up to c consecutive j, for every k < i
-    const int c = (i * (i + 1) / 2 + kThreads - 1) / kThreads;
-    int total = 0;
-    for (int k = 0; k < i; k++) total += nslots(i, k, c);
-    for (int slot = tid; slot < total; slot += kThreadsS) {
-      int k = 0, r = slot;
-      while (r >= nslots(i, k, c)) r -= nslots(i, k, c), k++;
-      const int j0 = k + r * c, j1 = min(i, j0 + c);
-      u32* dst = part + (size_t)slot * WL;
-      for (int w = 0; w < WL; w++) dst[w] = 0;
-      for (int j = j0; j < j1; j++) {
-        const int e = tri(j, k);
-        fx_rmw(dst, Lrow + (size_t)j * WL, lt[j], Xm + (size_t)e * WL, xt[e], ls[j] == xs[e], WL, LF);
-      }
+    const int nk = j + 1, np = (BT - 1 - j) * nk;
+    for (int p = tid; p < np; p += kThreadsS) {                  // slot (i, k) += l_ij x_jk
+      const int i = j + 1 + p / nk, k = p % nk;
+      const int e = tri(j, k);
+      fx_rmw(Xm + (size_t)tri(i, k) * WL, Lcol + (size_t)i * WL, lt[i], Xm + (size_t)e * WL, xt[e], ls[i] == xs[e],
+             WL, LF);
     }
     __syncthreads();
-    // x_ik = -(sum of the partials) * r_i
-    for (int k = warp; k < i; k += kWarpsS) {
-      int base = 0;
-      for (int kk = 0; kk < k; kk++) base += nslots(i, kk, c);
-      const int n = nslots(i, k, c);
-      WarpScratch& s = ws[warp];
-      u32 carry = 0, hprev = 0;
-      for (int cc = 0; cc < 2; cc++) {
-        const int w = lane + 32 * cc;
-        u64 v = 0;
-        if (w < WL)
-          for (int q = 0; q < n; q++) v += part[(size_t)(base + q) * WL + w];
-        const u32 lo = (u32)v, h = (u32)(v >> 32);
-        u32 hu = __shfl_up_sync(kFull, h, 1);
-        if (lane == 0) hu = hprev;
-        hprev = __shfl_sync(kFull, h, 31);
-        const u32 e = lo + hu;
-        u32 cout;
-        const u32 cj = chain_carry(e < lo, e == kFull, carry, cout);
-        if (w < WL) s.acc[w] = e + cj;
-        carry = cout;
-      }
-      __syncwarp();
-      const int ei = tri(i, k);
-      wmul(s.acc, RI + (size_t)i * WL, 0, WL, LF, s, nullptr, Xm + (size_t)ei * WL, xs + ei, xt + ei);
+    for (int k = warp; k <= j; k += kWarpsS) {                   // x_{j+1,k} = -(sum) r_{j+1}
+      const int ei = tri(j + 1, k);
+      wmul(Xm + (size_t)ei * WL, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WL,
+           xs + ei, xt + ei);
       if (lane == 0) xs[ei] ^= 1;                                // the negation
       __syncwarp();
     }

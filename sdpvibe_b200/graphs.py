@@ -75,7 +75,7 @@ def run(key, fn, inputs):
         return result
     for s, t in zip(e.inputs, inputs):
         s.copy_(t)
-    end = _trace.replay(e.launches)
+    end = _trace.replay(e.launches, "graph " + " ".join(str(k) for k in key))
     e.graph.replay()
     if end is not None:
         end.record()

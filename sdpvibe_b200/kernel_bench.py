@@ -2,7 +2,7 @@
 
   python -m sdpvibe_b200.kernel_bench --kernel syrk --N 274 --K 7000 --L 27 --reps 20
   kernels: residues | gemm | syrk | crt | mpfgemm | bgemm (--nb stacked blocks) | cholsolve (batched
-  Cholesky + solve over uneven blocks)
+  Cholesky + solve over uneven blocks) | tiles (--nb 32 x 32 base tiles: factorisation and inverse)
 
 Inputs are seeded random limb planes / residues of the given shape; rates are algorithmic (the
 reference's operation counts: moduli x 4 digit products x 2 ops per multiply-add; decomposition
@@ -67,6 +67,45 @@ def cholsolve_buckets(cases, L, bt=32):
     return res
 
 
+def spd_tile_fx(L, seed=0):
+    """one 32 x 32 SPD tile G G^T + 2^30 I (G integer, |g| < 2^20) scaled below 1, in wide fixed point
+    (WL = L + 24 words, 32 L fraction bits), entry-major (32, 32, WL) int32"""
+    WL, F = L + 24, 32 * L
+    rng = np.random.default_rng(seed)
+    G = [[int(v) for v in row] for row in rng.integers(-(1 << 20), 1 << 20, size=(32, 32))]
+    A = [[sum(G[i][k] * G[j][k] for k in range(32)) + ((1 << 30) if i == j else 0) for j in range(32)]
+         for i in range(32)]
+    sh = F - (max(A[i][i] for i in range(32)).bit_length() + 1)
+    out = np.zeros((32, 32, WL), np.uint32)
+    for i in range(32):
+        for j in range(32):
+            u = (A[i][j] << sh) % (1 << (32 * WL))
+            out[i, j] = [(u >> (32 * w)) & 0xffffffff for w in range(WL)]
+    return out.view(np.int32)
+
+
+def _tiles(a):
+    from . import _lib
+    from .basecase import tile_factor
+    WL, LF = a.L + 24, a.L
+    W = torch.from_numpy(spd_tile_fx(a.L)).cuda()[None].expand(a.nb, 32, 32, WL).contiguous()
+    Lw, X, RINV = tile_factor(W, WL, LF)
+    work = W.clone()
+
+    def chol():
+        work.copy_(W)
+        _lib.call("sdpv_chol_tiles", _lib.ptr(work), _lib.ptr(RINV), a.nb, 32, WL, LF, _lib.stream())
+    Xo, scratch = torch.empty_like(Lw), torch.empty_like(Lw)
+
+    def inv():
+        _lib.call("sdpv_trinv_tiles", _lib.ptr(Lw), _lib.ptr(RINV), _lib.ptr(Xo), _lib.ptr(scratch), a.nb, 32, WL,
+                  LF, _lib.stream())
+    tc = _events(chol, a.reps, a.warmup)
+    ti = _events(inv, a.reps, a.warmup)
+    return dict(nb=a.nb, WL=WL, chol_ms=min(tc), chol_ms_mean=float(np.mean(tc)), trinv_ms=min(ti),
+                trinv_ms_mean=float(np.mean(ti)))
+
+
 def _cholsolve(a, rng):
     """batched Cholesky + 2 triangular solves (nrhs right-hand sides) over uneven SPD blocks"""
     from . import mpf, _trace
@@ -107,7 +146,8 @@ def main():
     from . import mpf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve", "bgemm"))
+    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve", "bgemm",
+                                                             "tiles"))
     ap.add_argument("--nb", type=int, default=1, help="bgemm: number of stacked blocks")
     ap.add_argument("--blocks", type=int, default=600, help="cholsolve: number of SPD blocks")
     ap.add_argument("--nmin", type=int, default=8)
@@ -162,6 +202,8 @@ def main():
                    items=((a.M + 127) // 128) * ((a.N + 127) // 128) * a.nb * R.n, ms_residues_A=min(tr))
     elif a.kernel == "cholsolve":
         out.update(_cholsolve(a, rng))
+    elif a.kernel == "tiles":
+        out.update(_tiles(a))
     elif a.kernel == "crt":
         m = torch.tensor(R.mods, dtype=torch.int64, device=dev)[:, None, None]
         acc = (torch.randint(0, 1 << 30, (R.n, a.M, a.N), device=dev) % m).to(torch.int16)
