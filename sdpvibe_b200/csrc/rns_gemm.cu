@@ -38,6 +38,7 @@ struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
   int16_t stg[128][kStg];                   // epilogue staging of one output tile (coalesced global I/O)
   u64 full[kStages], empty[kStages], acc_full, tmem_empty;
+  u64 nacc_full[2], ntmem_empty[2];          // narrow items: two TMEM buffers
   u32 tmem_slot;
   int abort;
   float tminv[kMaxG];                       // this launch's moduli, staged once per CTA
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
-                    int nfull,
+                    int nfull, int nmode, int nTB,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
@@ -129,6 +130,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     mbar_init(&S.acc_full, 1);
     mbar_init(&S.tmem_empty, 8);                // one arrival per epilogue warp
+    for (int u = 0; u < 2; u++) {
+      mbar_init(&S.nacc_full[u], 1);
+      mbar_init(&S.ntmem_empty[u], 8);
+    }
     S.abort = 0;
     mbar_fence_init();
   }
@@ -152,11 +157,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
         const i64 t = item % tiles, bg = item / tiles;
         int b, g, m0, n0;
-        if (tailTB) {                             // syrk tail: A row block t against the last < 64 rows
+        if (tailTB || nmode) {                    // syrk tail / narrow: big-side row block t against TB rows
           b = (int)(bg % nb);
           g = gofs + (int)(bg / nb);
           m0 = (int)t * 128;
-          n0 = nfull;
+          n0 = tailTB ? nfull : 0;
         } else if (pack > 1) {                    // packed: tile t holds blocks t*pack .. (rows stacked)
           b = 0;
           g = gofs + (int)bg;
@@ -177,12 +182,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           const int kx = kb * 128;
-          if (tailTB) {                           // [Bhi; Blo] of the tail rows back to back: 2 TB rows
-            mbar_expect_tx(&S.full[s], 2 * kSlice + 2 * tailTB * 128);
+          if (tailTB || nmode) {                  // [Bhi; Blo] of the TB small-side rows back to back
+            const int TB = tailTB ? tailTB : nTB;
+            mbar_expect_tx(&S.full[s], 2 * kSlice + 2 * TB * 128);
             tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
             tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
             tma_load_4d(S.stage[s][2], &mTh, &S.full[s], kx, n0, b, g);
-            tma_load_4d(S.stage[s][2] + tailTB * 128, &mTl, &S.full[s], kx, n0, b, g);
+            tma_load_4d(S.stage[s][2] + TB * 128, &mTl, &S.full[s], kx, n0, b, g);
             continue;
           }
           mbar_expect_tx(&S.full[s], 4 * kSlice);
@@ -194,7 +200,50 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
+    if (lane == 0 && nmode) {
+      // narrow items: as the tail items, N = 2 TB over [Bhi; Blo], in two TMEM buffers (256 columns apart)
+      // so that an item's MMAs run while the epilogue still reads the previous item
+      const int TB = nTB;
+      const u32 idesc = idesc_i8(128, 2 * TB), idescT = idesc_i8(128, TB);
+      u32 kbg = 0, li = 0;
+      for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
+        const u32 buf = li & 1;
+        if (li >= 2 && !mbar_wait(&S.ntmem_empty[buf], ((li >> 1) - 1) & 1, err)) {
+          *(volatile int*)&S.abort = 1;
+          break;
+        }
+        tc_fence_after();
+        const u32 tb = tmem + buf * 256;
+        bool ok = true;
+        for (int kb = 0; kb < nk; kb++, kbg++) {
+          const u32 s = kbg % kStages;
+          if (!mbar_wait(&S.full[s], (kbg / kStages) & 1, err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
+          const int nks = (int)min((i64)4, (KC - kb * 128 + 31) / 32);     // K steps past KC are zero
+          for (int ks = 0; ks < nks; ks++) {
+            u64 bd = sdesc_sw128(bh + 32 * ks);
+            if ((kb | ks) == 0) {
+              mma_i8(tb + 0, sdesc_sw128(ah), bd, idesc, 0u);                                  // hh | hl
+              mma_i8(tb + 2 * TB, sdesc_sw128(al), sdesc_sw128(bh + TB * 128), idescT, 0u);    // ll
+              mma_i8(tb + TB, sdesc_sw128(al), bd, idescT, 1u);                                // hl += lh
+            } else {
+              mma_i8(tb + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
+              mma_i8(tb + TB, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+            }
+          }
+          mma_commit(&S.empty[s]);
+        }
+        if (!ok) {
+          *(volatile int*)&S.abort = 1;
+          break;
+        }
+        mma_commit(&S.nacc_full[buf]);
+      }
+    } else if (lane == 0) {
       // tail items: N = 2 TB over [Bhi; Blo] (hh | hl at column 0, (hl + lh) | ll at column TB)
       const int TB = tailTB ? tailTB : 128;
       const u32 idesc = idesc_i8(128, 2 * TB), idesc128 = idesc_i8(128, TB);
@@ -215,8 +264,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           tc_fence_after();
           u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
-#pragma unroll
-          for (int ks = 0; ks < 4; ks++) {
+          const int nks = (int)min((i64)4, (KC - kb * 128 + 31) / 32);     // K steps past KC are zero
+          for (int ks = 0; ks < nks; ks++) {
             u64 bd = sdesc_sw128(bh + 32 * ks);
             if ((kb | ks) == 0) {
               mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                                   // hh | hl
@@ -244,6 +293,52 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3, ch = (warp - 2) >> 2, ew = warp - 2;
     const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
     u32 li = 0;
+    for (i64 item = blockIdx.x; item < nitems && nmode; item += gridDim.x, li++) {
+      // narrow items: TMEM lane = big-side row r, columns = the TB small-side entries; nmode 1: C[r][j]
+      // (A is the big side), nmode 2: C[j][r] (B is the big side; a warp's lanes are consecutive r, so each
+      // output row's stores coalesce).  Each thread takes half of the TB columns.
+      const i64 t = item % tiles, bg = item / tiles;
+      const int b = (int)(bg % nb), g = (int)(bg / nb);
+      const int gg = g0 + gofs + g;
+      const int m = S.tmod[g], c14 = S.tc14[g];
+      const float minv = S.tminv[g];
+      const u32 buf = li & 1;
+      const int TB = nTB, half = nTB >> 1;
+      const i64 r = t * 128 + q * 32 + lane;
+      const i64 big = nmode == 1 ? M : N, small = nmode == 1 ? N : M;
+      const i64 rowA = (i64)gg * nb * M + (i64)b * M;                  // acc row of block row 0
+      int16_t* bp = nmode == 1 ? acc + (rowA + r) * ldc : acc + rowA * ldc + r;
+      const i64 js = nmode == 1 ? 1 : ldc;
+      const int j0 = ch * half;
+      const bool ok_me = mbar_wait(&S.nacc_full[buf], (li >> 1) & 1, err);
+      const bool fail = epi_sync_or(!ok_me);
+      if (fail) break;
+      tc_fence_after();
+      u32 hh[32], hx[32], ll[32];
+      const u32 base = tmem + buf * 256 + ((u32)(q * 32) << 16) + j0;
+      tmem_ld32(base, hh);
+      tmem_ld32(base + TB, hx);
+      tmem_ld32(base + 2 * TB, ll);
+      tmem_ld_wait();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
+#pragma unroll
+      for (int u = 0; u < 32; u++) {
+        const int j = j0 + u;
+        if (u >= half) break;
+        int a = (int)hh[u], x = (int)hx[u];
+        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+        const bool in = r < big && j < small;
+        const int o = (!fresh && in) ? (int)bp[j * js] : 0;                // old residue (rare: K chunks)
+        int v = ra * c14 + rx * 128 + (int)ll[u] + o;
+        int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+        rr += (rr < 0) ? m : 0;
+        rr -= (rr >= m) ? m : 0;
+        if (in) bp[j * js] = (int16_t)rr;
+      }
+    }
     for (i64 item = blockIdx.x; item < nitems && tailTB; item += gridDim.x, li++) {
       // syrk tail: entry (A row i, tail row j) = Q[nfull + j][i], written transposed into the lower triangle;
       // a warp's lanes are consecutive i, so the accesses of one tail row coalesce
@@ -287,7 +382,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (i < M && j < tail && nfull + j >= i) colp[(i64)j * ldc] = (int16_t)r;
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && pack > 1; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && pack > 1 && !nmode; item += gridDim.x, li++) {
       // packed small blocks: tile rows are the stacked rows of blocks t*pack .. t*pack + nbt - 1, tile
       // columns their stacked B rows; only the diagonal sub-blocks are outputs (staged, coalesced)
       const i64 t = item % tiles;
@@ -338,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = lane; j < N; j += 32) dst[j] = S.stg[r][bi * N + j];
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && pack <= 1 && !tailTB; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && pack <= 1 && !tailTB && !nmode; item += gridDim.x, li++) {
       const i64 t = item % tiles, bg = item / tiles;
       const int b = (int)(bg % nb), g = (int)(bg / nb);
       int tm, tn;
@@ -493,11 +588,29 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
     i64 p = 128 / M < 128 / N ? 128 / M : 128 / N;
     pack = (int)(p < nb ? p : nb);
   }
+  // One side at most 64 rows, the other longer (not syrk, not packed): narrow items.  The long side fills the
+  // 128 MMA rows, the short side's TB rows (rounded up to 16) are the MMA's N = 2 TB as [hi; lo]; nmode 1:
+  // A is the long side, 2: B is (C stored transposed from the tile).
+  int nmode = 0, nTB = 0;
+  if (mode == 0 && pack <= 1) {
+    if (N <= 64 && M > 64) nmode = 1;
+    else if (M <= 64 && N > 64) nmode = 2;
+    if (nmode) nTB = (int)(((nmode == 1 ? N : M) + 15) / 16 * 16);
+  }
   CUtensorMap mAh, mAl, mBh, mBl;
   const i64 ra = pack > 1 ? M * nb : M, rb = pack > 1 ? N * nb : N, nbm = pack > 1 ? 1 : nb;
-  if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
-      !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride))
+  if (nmode == 2) {                                    // big side B into the A slots, A as the TB rows
+    if (!make_map(&mAh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mAl, Blo, KC, rb, nbm, G, b_stride) ||
+        !make_map(&mBh, Ahi, KC, ra, nbm, G, a_stride, nTB) || !make_map(&mBl, Alo, KC, ra, nbm, G, a_stride, nTB))
+      return SDPV_EINVAL;
+  } else if (nmode == 1) {
+    if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
+        !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride, nTB) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride, nTB))
+      return SDPV_EINVAL;
+  } else if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
+             !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride)) {
     return SDPV_EINVAL;
+  }
   size_t smem = sizeof(GemmSmem) + 1024;
   static std::once_flag attr;
   static cudaError_t attr_err = cudaSuccess;
@@ -513,6 +626,7 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   if (tailTB) ntm = nfull / 128;
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
   if (pack > 1) tiles = (nb + pack - 1) / pack;
+  if (nmode) tiles = ((nmode == 1 ? M : N) + 127) / 128;
   CUtensorMap mTh = mBh, mTl = mBl;
   if (tailTB && (!make_map(&mTh, Bhi, KC, rb, nbm, G, b_stride, tailTB) ||
                  !make_map(&mTl, Blo, KC, rb, nbm, G, b_stride, tailTB)))
@@ -530,7 +644,7 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       if (nitems == 0) continue;
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
       rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
+          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, nmode, nTB, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
           KC, mode, ntn, ptiles, nitems, fresh, pack, sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;

@@ -2,7 +2,9 @@
 
   python -m sdpvibe_b200.kernel_bench --kernel syrk --N 274 --K 7000 --L 27 --reps 20
   kernels: residues | gemm | syrk | crt | mpfgemm | bgemm (--nb stacked blocks) | cholsolve (batched
-  Cholesky + solve over uneven blocks) | tiles (--nb 32 x 32 base tiles: factorisation and inverse)
+  Cholesky + solve over uneven blocks) | tiles (--nb 32 x 32 base tiles: factorisation and inverse) |
+  solve (mpf.Chol of --nb SPD blocks of size --M, then L^-1 B with B (nb, M, N): per-kernel device time of
+  the eager sequence and the time of its CUDA-graph replay)
 
 Inputs are seeded random limb planes / residues of the given shape; rates are algorithmic (the
 reference's operation counts: moduli x 4 digit products x 2 ops per multiply-add; decomposition
@@ -106,6 +108,32 @@ def _tiles(a):
                 trinv_ms_mean=float(np.mean(ti)))
 
 
+def _solve(a):
+    from . import _trace, graphs, mpf
+    rng = np.random.default_rng(1)
+    n, nb, m = a.M, a.nb, a.N
+    G = rng.standard_normal((nb, n, n))
+    A = mpf.from_float(G @ np.swapaxes(G, 1, 2) + n * np.eye(n), a.L)
+    B = mpf.from_float(rng.standard_normal((nb, n, m)), a.L)
+    ch = mpf.Chol(A)
+    graphs.ENABLED = False
+    ch.solve_lower(B)
+    torch.cuda.synchronize()
+    names = [k for k in _lib_names() if k.startswith("sdpv_")]
+    with _trace.Trace(timed=names) as tr:
+        t_eager = _events(lambda: ch.solve_lower(B), 1, 0)[0]
+    kms = {k: round(sum(tr.kernel_ms(k)), 3) for k in sorted(tr.events, key=lambda k: -sum(tr.kernel_ms(k)))}
+    graphs.ENABLED = True
+    tg = _events(lambda: ch.solve_lower(B), a.reps, max(2, a.warmup))
+    return dict(nb=nb, n=n, m=m, eager_ms=t_eager, graph_ms=min(tg), launches=tr.total_launches,
+                launches_by_entry=dict(tr.launches), kernel_ms=kms)
+
+
+def _lib_names():
+    from . import _lib
+    return list(_lib._SIGS)
+
+
 def _cholsolve(a, rng):
     """batched Cholesky + 2 triangular solves (nrhs right-hand sides) over uneven SPD blocks"""
     from . import mpf, _trace
@@ -147,7 +175,7 @@ def main():
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve", "bgemm",
-                                                             "tiles"))
+                                                             "tiles", "solve"))
     ap.add_argument("--nb", type=int, default=1, help="bgemm: number of stacked blocks")
     ap.add_argument("--blocks", type=int, default=600, help="cholsolve: number of SPD blocks")
     ap.add_argument("--nmin", type=int, default=8)
@@ -204,6 +232,8 @@ def main():
         out.update(_cholsolve(a, rng))
     elif a.kernel == "tiles":
         out.update(_tiles(a))
+    elif a.kernel == "solve":
+        out.update(_solve(a))
     elif a.kernel == "crt":
         m = torch.tensor(R.mods, dtype=torch.int64, device=dev)[:, None, None]
         acc = (torch.randint(0, 1 << 30, (R.n, a.M, a.N), device=dev) % m).to(torch.int16)

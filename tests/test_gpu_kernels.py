@@ -191,7 +191,12 @@ def _rand_residues(rng, T, G, rows, K):
                                               (26, 13, 1, 9, 16, False),
                                               # syrk with a short last row block (tail items), and without
                                               (27, 2, 150, 150, 64, True), (26, 1, 160, 160, 128, True),
-                                              (26, 1, 161, 161, 32, True), (27, 1, 290, 290, 48, True)])
+                                              (26, 1, 161, 161, 32, True), (27, 1, 290, 290, 48, True),
+                                              # narrow items: one side <= 64 rows, the other longer
+                                              (26, 3, 32, 300, 32, False), (26, 4, 64, 1000, 64, False),
+                                              (24, 2, 17, 130, 208, False), (34, 2, 50, 90, 48, False),
+                                              (26, 1, 64, 129, 4096, False), (26, 1, 1, 300, 16, False),
+                                              (27, 3, 129, 33, 160, False), (26, 2, 300, 64, 16, False)])
 def test_rns_gemm_random(sb, L, nb, M, N, K, syrk):
     from sdpvibe_b200.mpmat import ctx
     rng = np.random.default_rng(M * N + K)
@@ -608,7 +613,8 @@ def test_linalg_golden(sb):
     assert np.array_equal(np_(Yf), g["Yfm"]) and np.array_equal(np_(yfe), g["yfe"])
 
 
-@pytest.mark.parametrize("nb,M,N,K", [(1, 200, 130, 64), (6, 32, 42, 32), (3, 100, 7, 48)])
+@pytest.mark.parametrize("nb,M,N,K", [(1, 200, 130, 64), (6, 32, 42, 32), (3, 100, 7, 48), (5, 32, 1000, 32),
+                                      (2, 48, 200, 96)])
 def test_rns_gemm_fresh_overwrites(sb, nb, M, N, K):
     """fresh mode: the accumulator's previous content is ignored (overwritten with the product residues)."""
     from sdpvibe_b200.mpmat import ctx
