@@ -119,6 +119,37 @@ __device__ __forceinline__ void shift_entry(Word word, int L, i64 s, int Lout, i
   }
 }
 
+// The same for s >= 0 (the alignment case: target >= exponent) in 32-bit arithmetic: one funnel shift and
+// one add with carry per output word.  s beyond 32 (L + 1) gives the same words as 32 (L + 1) (every word
+// read is the sign extension), so it is clamped.  s < 0 takes the general path.
+template <class Word>
+__device__ __forceinline__ void shift_entry32(Word word, int L, i64 s, int Lout, int32_t* __restrict__ out,
+                                              i64 ostride, unsigned* err) {
+  if (s < 0) {
+    shift_entry(word, L, s, Lout, out, ostride, err);
+    return;
+  }
+  const u32 ext = ((int32_t)word(L - 1) < 0) ? 0xffffffffu : 0u;
+  const int si = (int)(s > 32 * (i64)(L + 1) ? 32 * (i64)(L + 1) : s);
+  const int q = si >> 5, r = si & 31;
+  auto w = [&](int i) -> u32 { return i < L ? (u32)word(i) : ext; };
+  u32 carry = si > 0 ? (w((si - 1) >> 5) >> ((si - 1) & 31)) & 1u : 0u;
+  u32 lo = w(q), prev = 0;
+  for (int k = 0; k <= Lout; k++) {
+    const u32 hi = w(q + k + 1);
+    const u32 f = __funnelshift_r(lo, hi, r);
+    const u32 v = f + carry;
+    carry = v < f ? 1u : 0u;
+    lo = hi;
+    if (k < Lout) {
+      out[(i64)k * ostride] = (int32_t)v;
+      prev = v;
+    } else if (v != ((prev >> 31) ? 0xffffffffu : 0u)) {
+      atomicOr(err, SDPV_ERRBIT_OVERFLOW);
+    }
+  }
+}
+
 // No transpose: thread per entry (b, r, c); reference exponent per row (per_col = 0) or column.
 __global__ void align_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e, int L, i64 nb, i64 R, i64 C,
                              const i64* __restrict__ target, int per_col, int Lout, int32_t* __restrict__ out,
@@ -129,7 +160,7 @@ __global__ void align_kernel(const int32_t* __restrict__ m, const i64* __restric
   i64 b = idx / (R * C), rc = idx - b * R * C, r = rc / C, c = rc - r * C;
   i64 ev = e[idx];
   i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
-  shift_entry([&](int i) { return (u32)__ldg(m + (i64)i * n + idx); }, L, s, Lout, out + idx, n, err);
+  shift_entry32([&](int i) { return (u32)__ldg(m + (i64)i * n + idx); }, L, s, Lout, out + idx, n, err);
 }
 
 // Transpose: tiles of 16 rows x 32 columns staged with all limbs; out is (Lout, nb, C, R).
@@ -144,11 +175,14 @@ __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __rest
   const i64 b = blockIdx.z;
   const i64 r0 = (i64)blockIdx.x * TR, c0 = (i64)blockIdx.y * TC;
   const int tid = threadIdx.x;
-  for (int t = tid; t < L * TR * TC; t += kThreads) {       // all copies in flight at once
-    int l = t / (TR * TC), rr = (t / TC) % TR, cc = t % TC;
-    i64 r = r0 + rr, c = c0 + cc;
-    bool in = r < R && c < C;
-    cp_async4(&sm[(l * TR + rr) * (TC + 1) + cc], m + (in ? (i64)l * n + (b * R + r) * C + c : 0), in ? 4u : 0u);
+  for (int pos = tid; pos < TR * TC; pos += kThreads) {     // all copies in flight at once
+    const int rr = pos / TC, cc = pos % TC;
+    const i64 r = r0 + rr, c = c0 + cc;
+    const bool in = r < R && c < C;
+    const int32_t* src = m + (in ? (b * R + r) * C + c : 0);
+    u32* dst = &sm[rr * (TC + 1) + cc];
+    const u32 nb4 = in ? 4u : 0u;
+    for (int l = 0; l < L; l++, src += n, dst += TR * (TC + 1)) cp_async4(dst, src, nb4);
   }
   cp_async_commit();
   for (int t = tid; t < TR * TC; t += kThreads) {
@@ -166,7 +200,7 @@ __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __rest
     i64 ev = se[rr * TC + cc];
     i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
     const u32* base = sm + rr * (TC + 1) + cc;
-    shift_entry([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * R + r, n, err);
+    shift_entry32([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * R + r, n, err);
   }
 }
 
