@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           m0 = tm * 128;
           n0 = tn * 128;
         }
+        const bool diag = mode == 1 && !tailTB && !nmode && pack <= 1 && m0 == n0;   // syrk diagonal: B = A
         for (int kb = 0; kb < nk; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
@@ -191,9 +192,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_load_4d(S.stage[s][2] + TB * 128, &mTl, &S.full[s], kx, n0, b, g);
             continue;
           }
-          mbar_expect_tx(&S.full[s], 4 * kSlice);
+          mbar_expect_tx(&S.full[s], (diag ? 2 : 4) * kSlice);
           tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
           tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
+          if (diag) continue;                     // [Ahi; Alo] in slots 0, 1 serve as [Bhi; Blo]
           tma_load_4d(S.stage[s][2], &mBh, &S.full[s], kx, n0, b, g);
           tma_load_4d(S.stage[s][3], &mBl, &S.full[s], kx, n0, b, g);
         }
@@ -222,18 +224,25 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
-          const int nks = (int)min((i64)4, (KC - kb * 128 + 31) / 32);     // K steps past KC are zero
-          for (int ks = 0; ks < nks; ks++) {
-            u64 bd = sdesc_sw128(bh + 32 * ks);
+          const u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
+          const u64 dah = sdesc_sw128(ah), dal = sdesc_sw128(al), dbh = sdesc_sw128(bh);
+          auto step = [&](int ks) {
+            const u64 bd = dbh + 2 * ks;
             if ((kb | ks) == 0) {
-              mma_i8(tb + 0, sdesc_sw128(ah), bd, idesc, 0u);                                  // hh | hl
-              mma_i8(tb + 2 * TB, sdesc_sw128(al), sdesc_sw128(bh + TB * 128), idescT, 0u);    // ll
-              mma_i8(tb + TB, sdesc_sw128(al), bd, idescT, 1u);                                // hl += lh
+              mma_i8(tb + 0, dah, bd, idesc, 0u);                                              // hh | hl
+              mma_i8(tb + 2 * TB, dal, sdesc_sw128(bh + TB * 128), idescT, 0u);                // ll
+              mma_i8(tb + TB, dal, bd, idescT, 1u);                                            // hl += lh
             } else {
-              mma_i8(tb + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
-              mma_i8(tb + TB, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+              mma_i8(tb + 0, dah + 2 * ks, bd, idesc, 1u);
+              mma_i8(tb + TB, dal + 2 * ks, bd, idesc, 1u);
             }
+          };
+          const i64 krem = KC - kb * 128;                                 // K steps past KC are zero
+          if (krem >= 128) {
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++) step(ks);
+          } else {
+            for (int ks = 0; ks < (int)((krem + 31) / 32); ks++) step(ks);
           }
           mma_commit(&S.empty[s]);
         }
@@ -249,6 +258,12 @@ __global__ void __launch_bounds__(kThreads, 1)
       const u32 idesc = idesc_i8(128, 2 * TB), idesc128 = idesc_i8(128, TB);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
+        bool diag = false;
+        if (mode == 1 && !tailTB && pack <= 1) {
+          int tm, tn;
+          tile_of((int)(item % tiles), mode, ntn, tm, tn);
+          diag = tm == tn;
+        }
         // the epilogue must have read the previous item's accumulators out of TMEM
         if (li > 0 && !mbar_wait(&S.tmem_empty, (li - 1) & 1, err)) {
           *(volatile int*)&S.abort = 1;
@@ -263,18 +278,27 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]), bh = smem_u32(S.stage[s][2]);
-          const int nks = (int)min((i64)4, (KC - kb * 128 + 31) / 32);     // K steps past KC are zero
-          for (int ks = 0; ks < nks; ks++) {
-            u64 bd = sdesc_sw128(bh + 32 * ks);
+          const u32 ah = smem_u32(S.stage[s][0]), al = smem_u32(S.stage[s][1]);
+          const u32 bh = diag ? ah : smem_u32(S.stage[s][2]);
+          // descriptors of K step ks: start address + 32 ks bytes = field + 2 ks (no carry out of the field)
+          const u64 dah = sdesc_sw128(ah), dal = sdesc_sw128(al), dbh = sdesc_sw128(bh);
+          auto step = [&](int ks) {
+            const u64 bd = dbh + 2 * ks;
             if ((kb | ks) == 0) {
-              mma_i8(tmem + 0, sdesc_sw128(ah), bd, idesc, 0u);                                   // hh | hl
-              mma_i8(tmem + 2 * TB, sdesc_sw128(al), sdesc_sw128(bh + TB * 128), idesc128, 0u);   // ll
-              mma_i8(tmem + TB, sdesc_sw128(al), bd, idesc128, 1u);                               // hl += lh
+              mma_i8(tmem + 0, dah, bd, idesc, 0u);                                              // hh | hl
+              mma_i8(tmem + 2 * TB, dal, sdesc_sw128(bh + TB * 128), idesc128, 0u);              // ll
+              mma_i8(tmem + TB, dal, bd, idesc128, 1u);                                          // hl += lh
             } else {
-              mma_i8(tmem + 0, sdesc_sw128(ah + 32 * ks), bd, idesc, 1u);
-              mma_i8(tmem + TB, sdesc_sw128(al + 32 * ks), bd, idesc, 1u);
+              mma_i8(tmem + 0, dah + 2 * ks, bd, idesc, 1u);
+              mma_i8(tmem + TB, dal + 2 * ks, bd, idesc, 1u);
             }
+          };
+          const i64 krem = KC - kb * 128;                                 // K steps past KC are zero
+          if (krem >= 128) {
+#pragma unroll
+            for (int ks = 0; ks < 4; ks++) step(ks);
+          } else {
+            for (int ks = 0; ks < (int)((krem + 31) / 32); ks++) step(ks);
           }
           mma_commit(&S.empty[s]);
         }
