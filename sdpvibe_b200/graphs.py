@@ -75,11 +75,17 @@ def run(key, fn, inputs):
         return result
     for s, t in zip(e.inputs, inputs):
         s.copy_(t)
-    end = _trace.replay(e.launches, "graph " + " ".join(str(k) for k in key))
+    end = _trace.replay(e.launches, _label(key))
     e.graph.replay()
     if end is not None:
         end.record()
     return _rebuild(e.skeleton, iter([t.clone() for t in e.outputs]))
+
+
+def _label(key):
+    """trace label of a graph: its key without the structure skeletons (plain values and integer shapes)"""
+    keep = [k for k in key if not isinstance(k, tuple) or all(isinstance(x, int) for x in k)]
+    return "graph " + " ".join(str(k) for k in keep)
 
 
 def clear():
