@@ -483,6 +483,18 @@ def fx_exp(L):
     return -(32 * L - 40)
 
 
+_FX_ONE = {}
+
+
+def _fx_one(L, efx):
+    """the fixed-point 1 (L limbs at exponent efx) on this device, made once"""
+    key = (L, efx, torch.cuda.current_device())
+    if key not in _FX_ONE:
+        one = from_mp([1], L, (1,))
+        _FX_ONE[key] = shift_round(one.m, torch.tensor([efx - int(one.e[0])], device=dev), L)[:, 0].clone()
+    return _FX_ONE[key]
+
+
 class Chol:
     """A = L L^T per block, with L = D^-1 Lt, D = diag(2^-k): Lt fixed point, k integer
     (sdpvibe/mpf.py:461-532).  A: MPF (n, n) or batched (nb, n, n); padded internally to a multiple of
@@ -490,7 +502,9 @@ class Chol:
 
     SOLVE_REFINE = int(os.environ.get("SDPB_GPU_SOLVE_REFINE", "0"))
 
-    def __init__(self, A, bt=32, refine=1):
+    def __init__(self, A, bt=32, refine=1, defer_check=False):
+        """defer_check: instead of raising here (one host synchronisation), leave the positivity flag of
+        the diagonal in self.bad (a device bool) for the caller to test later with others at once."""
         from .batched import BMP, bchol
         self.two_d = A.e.dim() == 2
         if self.two_d:
@@ -500,7 +514,9 @@ class Chol:
         self.nb, self.n, self.L, self.bt, self.refine = nb, n, L, bt, refine
         idx = torch.arange(n, device=dev)
         tpd = _top(A)[:, idx, idx]                                  # (nb, n)
-        if bool(((A.m[-1][:, idx, idx] < 0) | (tpd <= EZ // 2)).any()):          # one host sync
+        bad = ((A.m[-1][:, idx, idx] < 0) | (tpd <= EZ // 2)).any()
+        self.bad = bad
+        if not defer_check and bool(bad):                           # one host sync
             raise ValueError("matrix is not positive definite (diagonal)")
         k = torch.div(tpd + 1, 2, rounding_mode="floor")            # A_ii < 2^(2k)
         self.k = k
@@ -513,8 +529,7 @@ class Chol:
         P = torch.zeros((L, nb, npad, npad), dtype=torch.int32, device=dev)
         P[:, :, :n, :n] = Af
         if npad > n:
-            one = from_mp([1], L, (1,))
-            onefx = shift_round(one.m, torch.tensor([efx - int(one.e[0])], device=dev), L)[:, 0]
+            onefx = _fx_one(L, efx)
             ii = torch.arange(n, npad, device=dev)
             P[:, :, ii, ii] = onefx[:, None, None]
         self.Lt, self.tiles = graphs.run(("bchol", L, nb, npad, bt, refine, efx),

@@ -588,6 +588,36 @@ class Solver:
                 if lg2 > float(mp.log(cond[0], 2) if cond[0] > 0 else -1):
                     cond[0] = mp.mpf(2) ** mp.mpf(lg2)
                     cond[1] = name
+            # condition estimates and positivity flags stay on the device until the end of the iteration
+            # (read there in one transfer, applied in this order): no host synchronisation per factorisation
+            conds, bads = [], []
+
+            def chol(A):
+                ch = Chol(A, defer_check=True)
+                bads.append(ch.bad)
+                return ch
+
+            def resolve(extra=()):
+                """read the pending flags, estimates and `extra` tensors in one transfer; apply them in order"""
+                parts = [b.reshape(1).to(torch.float64) for b in bads] + [c.reshape(-1).to(torch.float64)
+                                                                          for c, _ in conds]
+                parts += [x.reshape(-1).to(torch.float64) for x in extra]
+                vals = torch.cat(parts).cpu().tolist() if parts else []
+                if any(vals[:len(bads)]):
+                    raise ValueError("matrix is not positive definite (diagonal)")
+                o = len(bads)
+                for c, name in conds:
+                    lg = vals[o:o + c.numel()]
+                    o += c.numel()
+                    z = max(range(len(lg)), key=lambda i: lg[i])
+                    upd_cond(lg[z], name(z))
+                out = []
+                for x in extra:
+                    out.append(vals[o:o + x.numel()])
+                    o += x.numel()
+                bads.clear()
+                conds.clear()
+                return out
             tm("residues")
             dobj = sdp.const + dot(sdp.b, self.y)
             psum = musum = mp.mpf(0)
@@ -603,12 +633,11 @@ class Solver:
                               X=[add(X, mul(d, aP)) for X, d in zip(xs["X"], dc["dX"])],
                               Y=[add(Y, mul(d, aD)) for Y, d in zip(xs["Y"], dc["dY"])])
                 psum += dot(g.c, xs["x"])
-                cX = [Chol(X) for X in xs["X"]]
-                cY = [Chol(Y) for Y in xs["Y"]]
+                cX = [chol(X) for X in xs["X"]]
+                cY = [chol(Y) for Y in xs["Y"]]
                 for tag, chs in (("X", cX), ("Y", cY)):
-                    lg = chol_log2_cond(chs[0], g.Xmask[0]).cpu().tolist()
-                    z = max(range(len(lg)), key=lambda i: lg[i])
-                    upd_cond(lg[z], f"{tag}_cholesky.block_{g.idx[z % g.nb]}_{z // g.nb}")
+                    conds.append((chol_log2_cond(chs[0], g.Xmask[0]),
+                                  lambda z, tag=tag, g=g: f"{tag}_cholesky.block_{g.idx[z % g.nb]}_{z // g.nb}"))
                 Vs = g.V
                 a, y_ = self.pairings(g, Vs, cX, xs["Y"])
                 d = -self.seg_diag(g, y_, [g.K])
@@ -627,6 +656,7 @@ class Solver:
                     musum += total(diag_of(M))
                 o["xs"], o["ch"] = xs, dict(X=cX, Y=cY)
                 o["res"] = dict(dres=dres, Pres=Pres, mXY=mXY)
+            resolve()
             update = None
             pobj = sdp.const + psum
             gap = abs(pobj - dobj) / max(abs(pobj) + abs(dobj), mp.mpf(1))
@@ -666,10 +696,8 @@ class Solver:
                 tm("schur: assemble S")
                 Sg = self.schur(g, o.pop("AXI"), o.pop("AY"))
                 tm("schur: chol(S)")
-                cs = Chol(Sg)
-                lg = chol_log2_cond(cs, g.xmask).cpu().tolist()
-                q = max(range(len(lg)), key=lambda i: lg[i])
-                upd_cond(lg[q], f"schur_complement_cholesky.block_{g.idx[q]}")
+                cs = chol(Sg)
+                conds.append((chol_log2_cond(cs, g.xmask), lambda q, g=g: f"schur_complement_cholesky.block_{g.idx[q]}"))
                 tm("schur: P = L^-1 B")
                 P = cs.solve_lower(g.B)
                 tm("schur: Q += P^T P")
@@ -677,8 +705,8 @@ class Solver:
                 Q = qg if Q is None else add(Q, qg)
                 o["cholS"], o["Pm"] = cs, P
             tm("chol(Q)")
-            cholQ = Chol(copy_lower_to_upper(Q))
-            Q_cond = mp.mpf(2) ** mp.mpf(float(chol_log2_cond(cholQ)[0]))
+            cholQ = chol(copy_lower_to_upper(Q))
+            q_lg = chol_log2_cond(cholQ)
             del Q
             dy, acc = self._direction(mu, pvec, cholQ, corr=False,
                                       beta=mp.mpf(0) if pd_feas else p["infeasibleCenteringParameter"])
@@ -706,6 +734,7 @@ class Solver:
             aP, aD = S(alphaP), S(alphaD)
             update = (aP, aD)
             self.y = add(self.y, mul(dy, aD))
+            Q_cond = mp.mpf(2) ** mp.mpf(resolve([q_lg])[0][0])
             row = dict(iteration=it, total_time=round(time.time() - t0, 3), iter_time=round(time.time() - ti, 3),
                        mu=mu, pobj=pobj, dobj=dobj, gap=gap, P_err=primal_err_P, p_err=primal_err_p, D_err=dual_err,
                        R_err=R_err, P_step=alphaP, D_step=alphaD, beta=beta_c, Q_cond=Q_cond,
