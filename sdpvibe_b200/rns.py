@@ -88,6 +88,8 @@ class RNS:
         N = M if syrk else Bhi.shape[1] // nb
         if syrk:
             Bhi, Blo = Ahi, Alo
+        if M == 0 or N == 0 or KC == 0:                 # nothing to add
+            return
         for t in (Ahi, Alo, Bhi, Blo):
             assert t.stride(2) == 1 and t.stride(1) == KC, "residue planes must have packed rows"
         _lib.call("sdpv_rns_gemm", self._h, _lib.ptr_strided(Ahi), _lib.ptr_strided(Alo), _lib.ptr_strided(Bhi),
