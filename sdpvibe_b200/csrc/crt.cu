@@ -112,8 +112,12 @@ __global__ void __launch_bounds__(kThreads)
           if (valid && g < n) {
             const int m = TB.m[g];
             const float mi = TB.minv[g];
-            y = mod_exact(av[16 * h + q] * TB.inv[g], m, mi);
+            // centred residue of x = a inv (0 <= x < 2^30): nearest quotient from the float estimate (off by
+            // at most one), then at most one correction each way into [-(m >> 1), m >> 1]
+            const int x = av[16 * h + q] * TB.inv[g];
+            y = x - __float2int_rn(__int2float_rn(x) * mi) * m;
             y -= (y > (m >> 1)) ? m : 0;
+            y += (y < -(m >> 1)) ? m : 0;
             ks += (float)y * mi;
           }
           int yl = ((y + 64) & 127) - 64, yh = (y - yl) >> 7;
@@ -128,6 +132,7 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
     const i64 kq = (i64)__float2int_rd(ks + 0.5f);
+    const int kq32 = (int)kq;                                          // |k| <= n / 2
     fence_proxy_async_smem();
     __syncthreads();
 
@@ -165,8 +170,9 @@ __global__ void __launch_bounds__(kThreads)
           i64 v = carry;
 #pragma unroll
           for (int u = 0; u < 4; u++) {
-            i64 z = 128 * (i64)(int)zh[j + u] + (i64)(int)zl[j + u] - kq * (i64)TB.md[t0 + u];
-            v += z << (8 * u);
+            // z = 128 Zh + Zl - k Md fits int32: |Zh| <= n 2^14 <= 320 2^14 < 2^23, |Zl| < 2^21, |k Md| < 2^15
+            const int z = 128 * (int)zh[j + u] + (int)zl[j + u] - kq32 * TB.md[t0 + u];
+            v += (i64)z * (i64)(1 << (8 * u));                       // one 32 x 32 -> 64 multiply-add
           }
           const u32 wv = (u32)v;
           if (MODE == 0) {
