@@ -597,7 +597,7 @@ def solver_measurement(steps, warmup, local_rank, world=1):
     sol = Solver(sdp, Ls, timing=True)
     marks = []
 
-    warm = max(warmup, 1)
+    warm = max(warmup, 3)                       # 1 records the graphs, 2-3 fill the chunk streams' pools
     total_it = warm + steps
 
     def rec(it, s, info):

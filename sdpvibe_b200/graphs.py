@@ -7,7 +7,8 @@ it is recorded once as a CUDA graph and replayed afterwards: the first call with
 (the library initialises its per-process state there) and then records the sequence on static copies of
 its inputs; later calls copy their inputs into those buffers, replay, and return copies of the static
 outputs (a result may be kept while the same graph runs again, e.g. the factors of X and of Y).  Replay
-gives the same bits as the eager run: the same kernels run on the same data.
+gives the same bits as the eager run: the same kernels run on the same data.  Replays of one graph from
+different streams are ordered by an event (its static buffers are shared).
 
 ``SDPV_GRAPHS=0`` turns the replay off (every call eager).
 """
@@ -50,7 +51,7 @@ def _rebuild(sk, it):
 
 
 class _Entry:
-    __slots__ = ("graph", "inputs", "outputs", "skeleton", "launches")
+    __slots__ = ("graph", "inputs", "outputs", "skeleton", "launches", "done")
 
 
 def run(key, fn, inputs):
@@ -68,18 +69,25 @@ def run(key, fn, inputs):
         with torch.cuda.graph(e.graph), _trace.Trace() as rec:     # counts the recorded launches
             static = fn(e.inputs)
         e.launches = rec.launches
+        e.done = None
         leaves = []
         e.skeleton = _flatten(static, leaves)
         e.outputs = leaves
         _cache[key] = e
         return result
+    if e.done is not None:                              # a replay issued on another stream must be over
+        torch.cuda.current_stream().wait_event(e.done)   # before its static buffers are written again
     for s, t in zip(e.inputs, inputs):
         s.copy_(t)
     end = _trace.replay(e.launches, _label(key))
     e.graph.replay()
     if end is not None:
         end.record()
-    return _rebuild(e.skeleton, iter([t.clone() for t in e.outputs]))
+    out = _rebuild(e.skeleton, iter([t.clone() for t in e.outputs]))
+    if e.done is None:
+        e.done = torch.cuda.Event()
+    e.done.record()
+    return out
 
 
 def _label(key):

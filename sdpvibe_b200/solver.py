@@ -478,6 +478,46 @@ class PhaseTimer:
         return out
 
 
+CONCURRENT = os.environ.get("SDPV_CONCURRENT", "1") != "0"
+
+
+class _ChunkStreams:
+    """Streams for independent per-chunk work.  Tensors made on a chunk stream and used afterwards on the
+    main stream are safe to free there: a chunk stream only runs new work after waiting for the main stream
+    at the next entry, so a freed block is never reused while the main stream still reads it."""
+
+    def __init__(self, solver, n):
+        self.solver, self.n = solver, n
+
+    def __enter__(self):
+        self.main = torch.cuda.current_stream()
+        if not CONCURRENT:
+            return lambda i: _NullCtx()
+        pool = getattr(self.solver, "_streams", None)
+        if pool is None or len(pool) < self.n:
+            pool = self.solver._streams = [torch.cuda.Stream() for _ in range(self.n)]
+        start = torch.cuda.Event()
+        start.record(self.main)
+        for st in pool[:self.n]:
+            st.wait_event(start)
+        self.pool = pool
+        return lambda i: torch.cuda.stream(pool[i])
+
+    def __exit__(self, *exc):
+        if CONCURRENT:
+            for st in self.pool[:self.n]:
+                self.main.wait_stream(st)
+        return False
+
+
+class _NullCtx:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *exc):
+        return False
+
+
 class Solver:
     """SDPB's Mehrotra predictor-corrector iteration (sdpvibe/solver.py:579-982) on one GPU with every
     chunk resident.  Per chunk the iteration keeps x, X, Y, their Cholesky factors, the residues, the
@@ -501,6 +541,13 @@ class Solver:
         self.y = F.zeros((sdp.N, 1), L)
         self.timer = PhaseTimer(timing)
         self.eig_refined = self.eig_unresolved = 0
+
+    # -- chunk concurrency
+    def _chunk_streams(self):
+        """context manager: inside it, `on(i)` runs chunk i's work on stream i (after everything issued before
+        on the current stream); on exit the current stream waits for all chunk streams.  SDPV_CONCURRENT=0
+        keeps every chunk on the current stream."""
+        return _ChunkStreams(self, len(self.sdp.groups))
 
     # -- per-chunk pieces (sdpvibe/solver.py:622-665)
     @staticmethod
@@ -623,39 +670,47 @@ class Solver:
             psum = musum = mp.mpf(0)
             dual_err = primal_err_P = mp.mpf(0)
             pvec = sdp.b
-            for gi, g in enumerate(G):
+            pgs = []
+            with self._chunk_streams() as on:                    # chunks concurrent, as in the Schur phase
+                for gi, g in enumerate(G):
+                    with on(gi):
+                        o = self.st[gi]
+                        xs = o["xs"]
+                        if update:
+                            aP, aD = update
+                            dc = o.pop("dc")
+                            xs = dict(x=add(xs["x"], mul(dc["dx"], aP)),
+                                      X=[add(X, mul(d, aP)) for X, d in zip(xs["X"], dc["dX"])],
+                                      Y=[add(Y, mul(d, aD)) for Y, d in zip(xs["Y"], dc["dY"])])
+                        cX = [chol(X) for X in xs["X"]]
+                        cY = [chol(Y) for Y in xs["Y"]]
+                        for tag, chs in (("X", cX), ("Y", cY)):
+                            conds.append((chol_log2_cond(chs[0], g.Xmask[0]),
+                                          lambda z, tag=tag, g=g: f"{tag}_cholesky.block_{g.idx[z % g.nb]}_{z // g.nb}"))
+                        Vs = g.V
+                        a, y_ = self.pairings(g, Vs, cX, xs["Y"])
+                        d = -self.seg_diag(g, y_, [g.K])
+                        o["AXI"], o["AY"] = a, y_
+                        B = g.B
+                        By = gemm(B, bexpand(self.y, g.nb))
+                        d = add(d, By, -1)
+                        dres = add(d, g.c)
+                        pgs.append(gemm(flat_rows(B), flat_rows(xs["x"]), transA=True))
+                        Ax = self.cmws(g, Vs, xs["x"])
+                        Pres = [masked(add(Ax[0], xs["X"][0], -1), mk2(g))]
+                        mXY = [masked(-gemm(X, Y), mk2(g)) for X, Y in zip(xs["X"], xs["Y"])]
+                        o["xs"], o["ch"] = xs, dict(X=cX, Y=cY)
+                        o["res"] = dict(dres=dres, Pres=Pres, mXY=mXY)
+            for gi, g in enumerate(G):                           # sums and host scalars in chunk order
                 o = self.st[gi]
-                xs = o["xs"]
-                if update:
-                    aP, aD = update
-                    dc = o.pop("dc")
-                    xs = dict(x=add(xs["x"], mul(dc["dx"], aP)),
-                              X=[add(X, mul(d, aP)) for X, d in zip(xs["X"], dc["dX"])],
-                              Y=[add(Y, mul(d, aD)) for Y, d in zip(xs["Y"], dc["dY"])])
-                psum += dot(g.c, xs["x"])
-                cX = [chol(X) for X in xs["X"]]
-                cY = [chol(Y) for Y in xs["Y"]]
-                for tag, chs in (("X", cX), ("Y", cY)):
-                    conds.append((chol_log2_cond(chs[0], g.Xmask[0]),
-                                  lambda z, tag=tag, g=g: f"{tag}_cholesky.block_{g.idx[z % g.nb]}_{z // g.nb}"))
-                Vs = g.V
-                a, y_ = self.pairings(g, Vs, cX, xs["Y"])
-                d = -self.seg_diag(g, y_, [g.K])
-                o["AXI"], o["AY"] = a, y_
-                B = g.B
-                By = gemm(B, bexpand(self.y, g.nb))
-                d = add(d, By, -1)
-                dres = add(d, g.c)
-                pvec = add(pvec, gemm(flat_rows(B), flat_rows(xs["x"]), transA=True), -1)
-                Ax = self.cmws(g, Vs, xs["x"])
-                Pres = [masked(add(Ax[0], xs["X"][0], -1), mk2(g))]
-                dual_err = max(dual_err, max_abs(dres))
-                primal_err_P = max([primal_err_P] + [max_abs(P) for P in Pres])
-                mXY = [masked(-gemm(X, Y), mk2(g)) for X, Y in zip(xs["X"], xs["Y"])]
-                for M in mXY:
+                res = o["res"]
+                psum += dot(g.c, o["xs"]["x"])
+                pvec = add(pvec, pgs[gi], -1)
+                dual_err = max(dual_err, max_abs(res["dres"]))
+                primal_err_P = max([primal_err_P] + [max_abs(P) for P in res["Pres"]])
+                for M in res["mXY"]:
                     musum += total(diag_of(M))
-                o["xs"], o["ch"] = xs, dict(X=cX, Y=cY)
-                o["res"] = dict(dres=dres, Pres=Pres, mXY=mXY)
+            del pgs
             resolve()
             update = None
             pobj = sdp.const + psum
@@ -689,21 +744,25 @@ class Solver:
             if mu > p["maxComplementarity"]:
                 self.result = result("maxComplementarity exceeded", it - 1)
                 break
-            # Schur complement, its Cholesky factor, Q = sum_g P_g^T P_g (all chunks resident: P kept)
-            Q = None
-            for gi, g in enumerate(G):
-                o = self.st[gi]
-                tm("schur: assemble S")
-                Sg = self.schur(g, o.pop("AXI"), o.pop("AY"))
-                tm("schur: chol(S)")
-                cs = chol(Sg)
-                conds.append((chol_log2_cond(cs, g.xmask), lambda q, g=g: f"schur_complement_cholesky.block_{g.idx[q]}"))
-                tm("schur: P = L^-1 B")
-                P = cs.solve_lower(g.B)
-                tm("schur: Q += P^T P")
-                qg = gemm(flat_rows(P), flat_rows(P), transA=True)
-                Q = qg if Q is None else add(Q, qg)
-                o["cholS"], o["Pm"] = cs, P
+            # Schur complement, its Cholesky factor, Q = sum_g P_g^T P_g (all chunks resident: P kept).  The
+            # chunks are independent until the sum: each runs on its own stream, the sum in chunk order.
+            tm("schur: S, chol(S), P = L^-1 B, P^T P")
+            qgs = []
+            with self._chunk_streams() as on:
+                for gi, g in enumerate(G):
+                    with on(gi):
+                        o = self.st[gi]
+                        Sg = self.schur(g, o.pop("AXI"), o.pop("AY"))
+                        cs = chol(Sg)
+                        conds.append((chol_log2_cond(cs, g.xmask),
+                                      lambda q, g=g: f"schur_complement_cholesky.block_{g.idx[q]}"))
+                        P = cs.solve_lower(g.B)
+                        qgs.append(gemm(flat_rows(P), flat_rows(P), transA=True))
+                        o["cholS"], o["Pm"] = cs, P
+            Q = qgs[0]
+            for qg in qgs[1:]:
+                Q = add(Q, qg)
+            del qgs
             tm("chol(Q)")
             cholQ = chol(copy_lower_to_upper(Q))
             q_lg = chol_log2_cond(cholQ)
@@ -765,31 +824,45 @@ class Solver:
             return g.Xmask[0][:, :, None] & g.Xmask[0][:, None, :]
         acc = dict(Rerr=mp.mpf(0), fr=mp.mpf(0), lamP=None, lamD=None)
         tm("direction (corrector) 1" if corr else "direction (predictor) 1")
+        tgs = []
+        with self._chunk_streams() as on:                        # chunks concurrent; sums in chunk order below
+            for gi, g in enumerate(G):
+                with on(gi):
+                    o = self.st[gi]
+                    xs, res, cX = o["xs"], o["res"], o["ch"]["X"]
+                    Rb = res["mXY"][0] if not corr else add(res["mXY"][0], gemm(o["dp"]["dX"][0], o["dp"]["dY"][0]), -1)
+                    Rb = add_diag(Rb, bm, g.Xmask[0])
+                    Z = symmetrize(cX[0].solve(add(gemm(res["Pres"][0], xs["Y"][0]), Rb, -1)))
+                    Vx = g.V["Vx"][0]
+                    VZV = gemm(Vx, gemm(Z, Vx), transA=True)
+                    rhs = add(-res["dres"], self.seg_diag(g, [VZV], [g.K]), -1)
+                    w = o["cholS"].solve_lower(rhs)
+                    o["dir"] = dict(R=[Rb], W=w)
+                    tgs.append(gemm(flat_rows(o["Pm"]), flat_rows(w), transA=True))
         dy = pvec
         for gi, g in enumerate(G):
-            o = self.st[gi]
-            xs, res, cX = o["xs"], o["res"], o["ch"]["X"]
             if not corr:
-                acc["Rerr"] = max([acc["Rerr"]] + [max_abs(add_diag(M, muS, g.Xmask[0])) for M in res["mXY"]])
-            Rb = res["mXY"][0] if not corr else add(res["mXY"][0], gemm(o["dp"]["dX"][0], o["dp"]["dY"][0]), -1)
-            Rb = add_diag(Rb, bm, g.Xmask[0])
-            Z = symmetrize(cX[0].solve(add(gemm(res["Pres"][0], xs["Y"][0]), Rb, -1)))
-            Vx = g.V["Vx"][0]
-            VZV = gemm(Vx, gemm(Z, Vx), transA=True)
-            rhs = add(-res["dres"], self.seg_diag(g, [VZV], [g.K]), -1)
-            w = o["cholS"].solve_lower(rhs)
-            o["dir"] = dict(R=[Rb], W=w)
-            dy = add(dy, gemm(flat_rows(o["Pm"]), flat_rows(w), transA=True), -1)
+                acc["Rerr"] = max([acc["Rerr"]] + [max_abs(add_diag(M, muS, g.Xmask[0]))
+                                                   for M in self.st[gi]["res"]["mXY"]])
+            dy = add(dy, tgs[gi], -1)
+        del tgs
         dy = cholQ.solve(dy)
         tm("direction (corrector) 2 + step length" if corr else "direction (predictor) 2")
-        for gi, g in enumerate(G):
+        with self._chunk_streams() as on:
+            for gi, g in enumerate(G):
+                with on(gi):
+                    o = self.st[gi]
+                    xs, res, cX, dr = o["xs"], o["res"], o["ch"]["X"], o.pop("dir")
+                    Pdy = gemm(o["Pm"], bexpand(dy, g.nb))
+                    dxg = o["cholS"].solve_upper(add(dr["W"], Pdy))
+                    Ad = self.cmws(g, g.V, dxg)
+                    dXg = [add(Ad[0], res["Pres"][0])]
+                    dYg = [masked(-symmetrize(cX[0].solve(add(gemm(dXg[0], xs["Y"][0]), dr["R"][0], -1))), mk2(g))]
+                    o["step"] = (dxg, dXg, dYg)
+        for gi, g in enumerate(G):                               # host scalars / step lengths in chunk order
             o = self.st[gi]
-            xs, res, cX, dr = o["xs"], o["res"], o["ch"]["X"], o.pop("dir")
-            Pdy = gemm(o["Pm"], bexpand(dy, g.nb))
-            dxg = o["cholS"].solve_upper(add(dr["W"], Pdy))
-            Ad = self.cmws(g, g.V, dxg)
-            dXg = [add(Ad[0], res["Pres"][0])]
-            dYg = [masked(-symmetrize(cX[0].solve(add(gemm(dXg[0], xs["Y"][0]), dr["R"][0], -1))), mk2(g))]
+            xs = o["xs"]
+            dxg, dXg, dYg = o.pop("step")
             if not corr:
                 acc["fr"] += dot(masked(add(xs["X"][0], dXg[0]), mk2(g)), masked(add(xs["Y"][0], dYg[0]), mk2(g)))
                 o["dp"] = dict(dX=dXg, dY=dYg)
