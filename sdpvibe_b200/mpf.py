@@ -585,3 +585,32 @@ class Chol:
     def solve(self, B):
         """A^-1 B"""
         return self.solve_upper(self.solve_lower(B))
+
+
+_BUCKET_STREAMS = []
+
+
+def chol_solve_many(pairs):
+    """[(A_b, B_b)] -> [A_b^-1 B_b] for independent batched systems (the reference's callers make one
+    Chol + solve per bucket of blocks of equal padded size).  Each system runs on its own CUDA stream, so
+    the latency-bound factorisations of different buckets overlap; the results are those of the same calls
+    made one after the other.  The positivity checks of all factorisations are read at the end, in one
+    transfer (ValueError as Chol raises it)."""
+    main = torch.cuda.current_stream()
+    while len(_BUCKET_STREAMS) < len(pairs):
+        _BUCKET_STREAMS.append(torch.cuda.Stream())
+    start = torch.cuda.Event()
+    start.record(main)
+    outs, bads = [], []
+    for (A, B), st in zip(pairs, _BUCKET_STREAMS):
+        st.wait_event(start)
+        with torch.cuda.stream(st):
+            ch = Chol(A, defer_check=True)
+            bads.append(ch.bad.reshape(1))
+            outs.append(ch.solve(B))
+    for st in _BUCKET_STREAMS[:len(pairs)]:
+        main.wait_stream(st)
+    if bads and bool(torch.cat(bads).any()):
+        raise ValueError("matrix is not positive definite (diagonal)")
+    return outs
+

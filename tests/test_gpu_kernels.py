@@ -474,6 +474,18 @@ def test_cholsolve_buckets_vs_oracle(sb):
             assert np.allclose(Ai @ xf, Bi, rtol=0, atol=1e-9)
 
 
+def test_chol_solve_many_matches_sequential(sb):
+    """the buckets' systems on concurrent streams give the bits of the same calls one after the other"""
+    from sdpvibe_b200 import mpf
+    from sdpvibe_b200.kernel_bench import cholsolve_inputs, cholsolve_buckets
+    buckets = cholsolve_buckets(cholsolve_inputs(40, 8, 160, 8, seed=4), 26)
+    seq = [mpf.Chol(A).solve(B) for _, _, A, B in buckets]
+    for _ in range(2):                                          # eager, then graph replays
+        got = mpf.chol_solve_many([(A, B) for _, _, A, B in buckets])
+        for X, Y in zip(got, seq):
+            assert torch.equal(X.m, Y.m) and torch.equal(X.e, Y.e)
+
+
 def _spd_tiles(rng, nb, L, ill):
     """nb random 32 x 32 SPD tiles in wide fixed point (WL = L + 24 words, F = 32 L fraction bits),
     entry-major (nb, 32, 32, WL) uint32; diagonal below 1.  ill: columns of the generator scaled by
