@@ -183,6 +183,12 @@ def _device_float(A):
 def _eig_min_device(Ms):
     """(lambda_min (nb,), error bound (nb,)) of the symmetric float64 copies of the blocks of Ms, by the
     batched Jacobi kernel (sdpv_eig_sym_f64), returned to the host"""
+    w, err = _eig_device(Ms)
+    return w.cpu().numpy(), err.cpu().numpy()
+
+
+def _eig_device(Ms):
+    """as _eig_min_device, the results left on the device"""
     from . import _lib
     Af = _device_float(Ms)
     Af = ((Af + Af.transpose(1, 2)) / 2).contiguous()
@@ -190,7 +196,7 @@ def _eig_min_device(Ms):
     w = torch.empty((nb, n), dtype=torch.float64, device=Af.device)
     err = torch.empty((nb,), dtype=torch.float64, device=Af.device)
     _lib.call("sdpv_eig_sym_f64", _lib.ptr(Af), nb, n, _lib.ptr(w), _lib.ptr(err), None, _lib.stream())
-    return w[:, 0].cpu().numpy(), err.cpu().numpy()
+    return w[:, 0], err
 
 
 def refine_min_eig(A, gamma, levels=64):
@@ -239,6 +245,18 @@ def refine_min_eig(A, gamma, levels=64):
     return out, len(unresolved)
 
 
+def min_eig_start(ch, D):
+    """the device part of min_eig for one factor: M = L^-1 dM L^-T, its scaling and (EIG_DEVICE) the
+    eigenvalue kernel, with nothing read back; min_eig_finish takes the results"""
+    T = ch.solve_lower(D)
+    M = ch.solve_lower(T.T)                                         # L^-1 dM L^-T (dM symmetric)
+    if EIG_DEVICE and M.shape[-1] <= EIG_DEVICE_NMAX:
+        s, ok, Ms = _scaled(M)
+        return M, s, ok, _eig_device(Ms)
+    s, ok, Mf = _scaled_float(M)
+    return M, s, ok, (np.linalg.eigvalsh(Mf)[:, 0], _eig_err(Mf))
+
+
 def min_eig(chols, dMs, lam=None, gamma=None, stats=None):
     """min over blocks of lambda_min(L^-1 dM L^-T), combined with lam (sdpvibe/solver.py:1064-1093).
     The eigenvalues come from a float64 copy of each block: on the GPU by the batched Jacobi kernel with
@@ -246,19 +264,18 @@ def min_eig(chols, dMs, lam=None, gamma=None, stats=None):
     (n + 2) eps ||M||_F, which reproduces the reference's steps bit for bit.  With gamma
     (stepLengthReduction) the blocks whose error bound could move the step length by more than EIG_TOL
     are recomputed in multiprecision (refine_min_eig), counted in stats."""
-    for ch, D in zip(chols, dMs):
-        T = ch.solve_lower(D)
-        M = ch.solve_lower(T.T)                                     # L^-1 dM L^-T (dM symmetric)
-        if EIG_DEVICE and M.shape[-1] <= EIG_DEVICE_NMAX:
-            s, ok, Ms = _scaled(M)
-            ev, err = _eig_min_device(Ms)
-        else:
-            s, ok, Mf = _scaled_float(M)
-            ev = np.linalg.eigvalsh(Mf)[:, 0]
-            err = _eig_err(Mf)
+    return min_eig_finish([min_eig_start(ch, D) for ch, D in zip(chols, dMs)], lam, gamma, stats)
+
+
+def min_eig_finish(pending, lam=None, gamma=None, stats=None):
+    """the host part of min_eig over the results of min_eig_start, in order"""
+    for M, s, ok, (ev, err) in pending:
+        if torch.is_tensor(ev):
+            ev, err = ev.cpu().numpy(), err.cpu().numpy()
+        s_h, ok_h = s.tolist(), ok.tolist()                        # one transfer each
         flag = []
-        for q in torch.nonzero(ok).reshape(-1).tolist():
-            sc = mp.mpf(2) ** int(s[q])
+        for q in (q for q in range(len(ok_h)) if ok_h[q]):
+            sc = mp.mpf(2) ** int(s_h[q])
             lq = mp.mpf(float(ev[q])) * sc
             if gamma is not None and not _resolved(lq, mp.mpf(float(err[q])) * sc, gamma):
                 flag.append(q)
@@ -859,6 +876,9 @@ class Solver:
                     dXg = [add(Ad[0], res["Pres"][0])]
                     dYg = [masked(-symmetrize(cX[0].solve(add(gemm(dXg[0], xs["Y"][0]), dr["R"][0], -1))), mk2(g))]
                     o["step"] = (dxg, dXg, dYg)
+                    if corr:                                     # the device part of the step lengths too
+                        o["eig"] = ([min_eig_start(c, D) for c, D in zip(o["ch"]["X"], dXg)],
+                                    [min_eig_start(c, D) for c, D in zip(o["ch"]["Y"], dYg)])
         for gi, g in enumerate(G):                               # host scalars / step lengths in chunk order
             o = self.st[gi]
             xs = o["xs"]
@@ -869,8 +889,9 @@ class Solver:
             else:
                 gm = p["stepLengthReduction"]
                 st = {}
-                lamP = min_eig(o["ch"]["X"], dXg, gamma=gm, stats=st)
-                lamD = min_eig(o["ch"]["Y"], dYg, gamma=gm, stats=st)
+                pend_P, pend_D = o.pop("eig")
+                lamP = min_eig_finish(pend_P, gamma=gm, stats=st)
+                lamD = min_eig_finish(pend_D, gamma=gm, stats=st)
                 for k, v in (("lamP", lamP), ("lamD", lamD)):
                     if v is not None:
                         acc[k] = v if acc[k] is None else min(acc[k], v)
