@@ -780,12 +780,23 @@ class Solver:
             for qg in qgs[1:]:
                 Q = add(Q, qg)
             del qgs
-            tm("chol(Q)")
-            cholQ = chol(copy_lower_to_upper(Q))
-            q_lg = chol_log2_cond(cholQ)
+            # chol(Q) on a stream of its own: the first half of the predictor does not need it, so the two
+            # overlap; _direction waits for it before its solve with Q
+            tm("chol(Q) + direction (predictor) 1")
+            main = torch.cuda.current_stream()
+            qstream = self._q_stream() if CONCURRENT else main
+            qstream.wait_stream(main)
+            with torch.cuda.stream(qstream):
+                cholQ = chol(copy_lower_to_upper(Q))
+                q_lg = chol_log2_cond(cholQ)
+                q_ready = torch.cuda.Event()
+                q_ready.record(qstream)
+            for t in (Q.m, Q.e):
+                t.record_stream(qstream)                       # freed below while the Q stream may read it
             del Q
             dy, acc = self._direction(mu, pvec, cholQ, corr=False,
-                                      beta=mp.mpf(0) if pd_feas else p["infeasibleCenteringParameter"])
+                                      beta=mp.mpf(0) if pd_feas else p["infeasibleCenteringParameter"],
+                                      q_ready=q_ready)
             R_err = acc["Rerr"]
             r = acc["fr"] / (mu * sdp.total_psd_rows)
             beta = r * r if r < 1 else r
@@ -830,7 +841,12 @@ class Solver:
         self._pending_update = update
         return self.result
 
-    def _direction(self, mu, pvec, cholQ, corr, beta):
+    def _q_stream(self):
+        if getattr(self, "_qs", None) is None:
+            self._qs = torch.cuda.Stream()
+        return self._qs
+
+    def _direction(self, mu, pvec, cholQ, corr, beta, q_ready=None):
         """predictor (corr=False) or corrector search direction (sdpvibe/solver.py:870-933): dy, and per
         chunk dp (predictor) or dc (corrector) with the step-length eigenvalues"""
         p, S, G = self.p, self.S, self.sdp.groups
@@ -840,7 +856,8 @@ class Solver:
         def mk2(g):
             return g.Xmask[0][:, :, None] & g.Xmask[0][:, None, :]
         acc = dict(Rerr=mp.mpf(0), fr=mp.mpf(0), lamP=None, lamD=None)
-        tm("direction (corrector) 1" if corr else "direction (predictor) 1")
+        if corr:
+            tm("direction (corrector) 1")
         tgs = []
         with self._chunk_streams() as on:                        # chunks concurrent; sums in chunk order below
             for gi, g in enumerate(G):
@@ -863,6 +880,8 @@ class Solver:
                                                    for M in self.st[gi]["res"]["mXY"]])
             dy = add(dy, tgs[gi], -1)
         del tgs
+        if q_ready is not None:
+            torch.cuda.current_stream().wait_event(q_ready)
         dy = cholQ.solve(dy)
         tm("direction (corrector) 2 + step length" if corr else "direction (predictor) 2")
         with self._chunk_streams() as on:
