@@ -86,6 +86,14 @@ int sdpv_mpf_mul(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
 /* O = A + sgn*B entrywise.  Replaces mpf.add / mpf_add (sdpvibe/mpf.py:92-124, 326-331). */
 int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
                  int sgn, int32_t* O, int64_t* eO, void* stream);
+/* Schur complement of one chunk: S (L, nb, P, P) / eS from the pairings AXI, AY (L, 2 nb, W, W) / (2 nb, W, W),
+ * W = dim K, P = K dim (dim + 1) / 2, in one launch with the reference's products and sums in its order
+ * (bit-exact); S symmetric, diagonal entries of rows with xmask (nb, P, bytes) false set to one_m / one_e
+ * (L <= 64).  Replaces the assembly of sdpvibe/solver.py:634-652 (elementwise mpf_mul / mpf_add over
+ * sub-blocks, fold over the parities, the 1/4 scale, copy of the lower triangle, padding diagonal). */
+int sdpv_schur_assemble(int L, int64_t nb, int P, int K, int dim, const int32_t* AXI, const int64_t* eAXI,
+                        const int32_t* AY, const int64_t* eAY, const uint8_t* xmask, const int32_t* one_m,
+                        int64_t one_e, int32_t* S, int64_t* eS, void* stream);
 /* float64 values V (n) -> normalised MPF (L >= 2 limbs), exactly; zeros -> EZ; a non-finite value
  * becomes zero and sets SDPV_ERRBIT_OVERFLOW.  Replaces the host frexp conversion of
  * sdpvibe/solver.py:1012-1018 (the float64 -> mpf step of the step-length code). */

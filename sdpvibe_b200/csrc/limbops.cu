@@ -124,40 +124,15 @@ __global__ void mpf_mul_kernel(int L, i64 n, const int32_t* __restrict__ A, cons
   i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   i64 ib = bscalar ? 0 : i, nbn = bscalar ? 1 : n;
-  u32 a[LMAX], b[LMAX], p[2 * LMAX], r[LMAX];
+  u32 a[LMAX], b[LMAX], r[LMAX];
   for (int k = 0; k < L; k++) {
     a[k] = (u32)A[(i64)k * n + i];
     b[k] = (u32)Bm[(i64)k * nbn + ib];
   }
-  bool na = a[L - 1] >> 31, nb = b[L - 1] >> 31;
-  if (na) neg_words(a, L);
-  if (nb) neg_words(b, L);
-  if (!bitlen_mag(a, L) || !bitlen_mag(b, L)) {
-    for (int k = 0; k < L; k++) O[(i64)k * n + i] = 0;
-    eO[i] = SDPV_EZ;
-    return;
-  }
-  // Product by output columns: 64-bit low/high partial sums per column, one carry pass.
-  u64 carry = 0, hprev = 0;
-  for (int k = 0; k < 2 * L - 1; k++) {
-    u64 slo = 0, shi = 0;
-    int x0 = k - L + 1 > 0 ? k - L + 1 : 0, x1 = k < L - 1 ? k : L - 1;
-    for (int x = x0; x <= x1; x++) {
-      u64 pr = (u64)a[x] * b[k - x];
-      slo += (u32)pr;
-      shi += pr >> 32;
-    }
-    u64 sum = slo + hprev + carry;
-    p[k] = (u32)sum;
-    carry = sum >> 32;
-    hprev = shi;
-  }
-  p[2 * L - 1] = (u32)(hprev + carry);
-  int s = bitlen_mag(p, 2 * L) - (32 * L - 2);
-  mag_shift(p, 2 * L, s, r, L);
-  if (na != nb) neg_words(r, L);
+  i64 er;
+  mpf_mul_dev<LMAX>(a, eA[i], b, eB[ib], L, r, er);
   for (int k = 0; k < L; k++) O[(i64)k * n + i] = (int32_t)r[k];
-  eO[i] = eA[i] + eB[ib] + s;
+  eO[i] = er;
 }
 
 template <int LMAX>
@@ -167,59 +142,15 @@ __global__ void mpf_add_kernel(int L, i64 n, const int32_t* A, const i64* eA,
   i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (pred && *pred == 0) return;                      // predicated launch: O / eO untouched
-  u32 a[LMAX], b[LMAX], wa[LMAX + 2], wb[LMAX + 2], r[LMAX];
+  u32 a[LMAX], b[LMAX], r[LMAX];
   for (int k = 0; k < L; k++) {
     a[k] = (u32)A[(i64)k * n + i];
     b[k] = (u32)Bm[(i64)k * n + i];
   }
-  bool na = a[L - 1] >> 31;
-  bool nbs = (b[L - 1] >> 31) ^ (sgn < 0);
-  if (a[L - 1] >> 31) neg_words(a, L);
-  if (b[L - 1] >> 31) neg_words(b, L);
-  i64 ea = eA[i], eb = eB[i];
-  if (!bitlen_mag(a, L)) ea = SDPV_EZ;
-  if (!bitlen_mag(b, L)) eb = SDPV_EZ;
-  if (ea == SDPV_EZ && eb == SDPV_EZ) {
-    for (int k = 0; k < L; k++) O[(i64)k * n + i] = 0;
-    eO[i] = SDPV_EZ;
-    return;
-  }
-  const int far = 32 * (L + 3);
-  i64 t = (ea > eb ? ea : eb) - 32;
-  i64 da = ea - t, db = eb - t;
-  int sa = (da < -(i64)far) ? far : (int)(-da);
-  int sb = (db < -(i64)far) ? far : (int)(-db);
-  if (ea == SDPV_EZ) {
-    for (int k = 0; k < L + 2; k++) wa[k] = 0;
-  } else {
-    mag_shift(a, L, sa, wa, L + 2);
-  }
-  if (eb == SDPV_EZ) {
-    for (int k = 0; k < L + 2; k++) wb[k] = 0;
-  } else {
-    mag_shift(b, L, sb, wb, L + 2);
-  }
-  if (na) neg_words(wa, L + 2);
-  if (nbs) neg_words(wb, L + 2);
-  u64 c = 0;
-  for (int k = 0; k < L + 2; k++) {
-    u64 v = (u64)wa[k] + wb[k] + c;
-    wa[k] = (u32)v;
-    c = v >> 32;
-  }
-  bool ns = wa[L + 1] >> 31;
-  if (ns) neg_words(wa, L + 2);
-  int bl = bitlen_mag(wa, L + 2);
-  if (!bl) {
-    for (int k = 0; k < L; k++) O[(i64)k * n + i] = 0;
-    eO[i] = SDPV_EZ;
-    return;
-  }
-  int s = bl - (32 * L - 2);
-  mag_shift(wa, L + 2, s, r, L);
-  if (ns) neg_words(r, L);
+  i64 er;
+  mpf_add_dev<LMAX>(a, eA[i], b, eB[i], sgn, L, r, er);
   for (int k = 0; k < L; k++) O[(i64)k * n + i] = (int32_t)r[k];
-  eO[i] = t + s;
+  eO[i] = er;
 }
 
 template <int LMAX>

@@ -594,6 +594,28 @@ class Solver:
         return [AXI], [AY]
 
     def schur(self, g, AXI, AY):
+        """S_pq = Tr(A_p X^-1 A_q Y) of the chunk from its pairings, in one launch (sdpv_schur_assemble:
+        the operations of schur_composed, fused, bit for bit)"""
+        from . import _lib
+        A, Yp = AXI[0], AY[0]
+        L, nb, P = self.L, g.nb, g.P
+        S = MPF(torch.empty((L, nb, P, P), dtype=torch.int32, device=dev),
+                torch.empty((nb, P, P), dtype=torch.int64, device=dev))
+        one, one_e = self._one()
+        _lib.call("sdpv_schur_assemble", L, nb, P, g.K, g.dim, _lib.ptr(A.m.contiguous()), _lib.ptr(A.e.contiguous()),
+                  _lib.ptr(Yp.m.contiguous()), _lib.ptr(Yp.e.contiguous()), _lib.ptr(g.xmask.contiguous()),
+                  _lib.ptr(one.m), one_e, _lib.ptr(S.m), _lib.ptr(S.e), _lib.stream())
+        return S
+
+    def _one(self):
+        """the MPF scalar 1 and its exponent (made once)"""
+        if getattr(self, "_one_c", None) is None:
+            o = self.S(1)
+            self._one_c = (o, int(o.e[0]))
+        return self._one_c
+
+    def schur_composed(self, g, AXI, AY):
+        """the reference's composition of the Schur complement out of elementwise MPF operations"""
         K = g.K
         if g.dim == 1:
             S = fold(mul(AXI[0], AY[0]), g.nb)

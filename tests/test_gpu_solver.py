@@ -110,3 +110,33 @@ def test_solver_iterates_device_eigenvalues_near_reference():
         for gi, o in enumerate(s.st):
             close(o["dc"]["dx"], f"it{it}_g{gi}_dx")
     sol.run(max_iter=iters, record=rec)
+
+
+@pytest.mark.parametrize("dims,K,L", [((1, 2, 3), 5, 8), ((2, 3), 9, 26), ((1, 4), 3, 12)])
+def test_schur_kernel_matches_composition(dims, K, L):
+    """the fused Schur assembly (sdpv_schur_assemble) gives the bits of the composed elementwise operations,
+    on random pairings with zeros and padding rows"""
+    from sdpvibe_b200 import mpf as F
+    from sdpvibe_b200.mpf import MPF
+    from sdpvibe_b200.solver import SDP, Solver
+    rng = np.random.default_rng(K + L)
+    blocks = []
+    for d in dims:
+        for kk in (K, K - 1):
+            npair = d * (d + 1) // 2
+            blocks.append(dict(dim=d, K=kk, Ve=rng.standard_normal((2, kk)), Vo=rng.standard_normal((1, kk)),
+                               c=rng.standard_normal((kk * npair, 1)), B=rng.standard_normal((kk * npair, 3))))
+    sdp = SDP(blocks, rng.standard_normal((3, 1)), 0, L)
+    sol = Solver(sdp, L)
+    for g in sdp.groups:
+        W = g.dim * g.K
+        shape = (2 * g.nb, W, W)
+
+        def sym():
+            v = rng.standard_normal(shape) * 2.0 ** rng.integers(-30, 30, size=shape)
+            v[rng.random(shape) < 0.1] = 0
+            return F.from_float((v + np.swapaxes(v, 1, 2)) / 2, L)
+        A, Y = sym(), sym()
+        got = sol.schur(g, [A], [Y])
+        ref = sol.schur_composed(g, [A], [Y])
+        assert torch.equal(got.m, ref.m) and torch.equal(got.e, ref.e), g.dim
