@@ -457,6 +457,16 @@ def fmt_big(v, digits):
     return f"{mant}e{sign}{ex.zfill(2)}"
 
 
+def chol_log2_cond_parts(ch):
+    """(max, min) over the diagonal of L (log2) of a factorisation (sdpvibe/solver.py:548-555)"""
+    L = ch.L
+    i = torch.arange(ch.n, device=dev)
+    d = ch.Lt.limbs[:, :, i, i]
+    top = d[-1].double() * 2.0 ** 32 + (d[-2].double() % 2.0 ** 32) if L > 1 else d[-1].double()
+    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.Lt.exp + 32 * (L - 2)) + ch.k.double()
+    return float(lg.max()), float(lg.min())
+
+
 def chol_log2_cond(ch, mask=None):
     """per block log2 of SDPB's Cholesky condition estimate (max / min diagonal of L)^2, over the rows
     where mask (nb, n) is True (sdpvibe/solver.py:563-576)"""
@@ -808,9 +818,15 @@ class Solver:
             main = torch.cuda.current_stream()
             qstream = self._q_stream() if CONCURRENT else main
             qstream.wait_stream(main)
+            qb = self._q_block(sdp.N)
             with torch.cuda.stream(qstream):
-                cholQ = chol(copy_lower_to_upper(Q))
-                q_lg = chol_log2_cond(cholQ)
+                if qb:                                         # tiled: ~Q/2 instead of ~9 Q at the peak
+                    from .blockchol import BlockChol
+                    cholQ, q_lg = BlockChol([Q], qb), None
+                    q_cond_lg = cholQ.log2_cond()
+                else:
+                    cholQ = chol(copy_lower_to_upper(Q))
+                    q_lg = chol_log2_cond(cholQ)
                 q_ready = torch.cuda.Event()
                 q_ready.record(qstream)
             for t in (Q.m, Q.e):
@@ -843,7 +859,11 @@ class Solver:
             aP, aD = S(alphaP), S(alphaD)
             update = (aP, aD)
             self.y = add(self.y, mul(dy, aD))
-            Q_cond = mp.mpf(2) ** mp.mpf(resolve([q_lg])[0][0])
+            if q_lg is None:
+                resolve()
+                Q_cond = mp.mpf(2) ** mp.mpf(q_cond_lg)
+            else:
+                Q_cond = mp.mpf(2) ** mp.mpf(resolve([q_lg])[0][0])
             row = dict(iteration=it, total_time=round(time.time() - t0, 3), iter_time=round(time.time() - ti, 3),
                        mu=mu, pobj=pobj, dobj=dobj, gap=gap, P_err=primal_err_P, p_err=primal_err_p, D_err=dual_err,
                        R_err=R_err, P_step=alphaP, D_step=alphaD, beta=beta_c, Q_cond=Q_cond,
@@ -862,6 +882,17 @@ class Solver:
                       flush=True)
         self._pending_update = update
         return self.result
+
+    def _q_block(self, N):
+        """tile size of the tiled Cholesky of Q, or 0 for the monolithic one (sdpvibe/solver.py:594-606):
+        SDPB_GPU_QBLOCK=<tile> forces it; else 2048 when the monolithic factorisation (about 9 N^2 MPF
+        entries) would take more than 35% of the GPU's memory and N > 2048"""
+        forced = int(os.environ.get("SDPB_GPU_QBLOCK", 0))
+        if forced:
+            return forced if forced < N else 0
+        E = 4 * self.L + 8
+        budget = torch.cuda.get_device_properties(torch.cuda.current_device()).total_memory
+        return 2048 if 9.0 * N * N * E > 0.35 * budget and N > 2048 else 0
 
     def _q_stream(self):
         if getattr(self, "_qs", None) is None:

@@ -323,6 +323,20 @@ def case_chol():
              lo_m=lo.m, lo_e=lo.e, up_m=up.m, up_e=up.e, x_m=xs.m, x_e=xs.e, **tiles)
 
 
+def case_blockchol():
+    # sdpvibe/blockchol.py: the tiled Cholesky of one N x N matrix (lower triangle valid) and its solves
+    from sdpvibe.blockchol import BlockChol
+    rng = random.Random(29)
+    L, N, b, nr = 8, 70, 32, 3
+    A = spd_blocks(rng, 1, N, L, 12)
+    Q = mpf.MPF(A.m[:, 0].contiguous(), A.e[0].contiguous())
+    ch = BlockChol([Q], b)
+    B = rmpf(rng, (N, nr), L, -20, 20)
+    lo, up, xs = ch.solve_lower(B), ch.solve_upper(B), ch.solve(B)
+    save("blockchol_n70_b32", Qm=A.m[:, 0], Qe=A.e[0], b=b, Bm=B.m, Be=B.e, lo_m=lo.m, lo_e=lo.e, up_m=up.m,
+         up_e=up.e, x_m=xs.m, x_e=xs.e, log2_cond=np.float64(ch.log2_cond()))
+
+
 def case_basecase():
     # sdpvibe/basecase.py:268-293 on single 32x32 tiles (equilibrated, fixed point)
     rng = random.Random(23)
