@@ -86,6 +86,20 @@ int sdpv_mpf_mul(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
 /* O = A + sgn*B entrywise.  Replaces mpf.add / mpf_add (sdpvibe/mpf.py:92-124, 326-331). */
 int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
                  int sgn, int32_t* O, int64_t* eO, void* stream);
+/* ---------------------------------------------------------------- binary SDP records (El::BigFloat over GMP limbs)
+ * Record: byte is_zero; unless zero, int32 size, int64 exp, nl 64-bit limbs; value = sign(size) M
+ * 2^(64 (exp - |size|)).  Replaces decode_bigfloats / encode_bigfloats (sdpvibe/_bigfloat.c:16-111).
+ * sdpv_bigfloat_index (host, no launch): offsets of n records from pos; SDPV_EINVAL if truncated/corrupt.
+ * sdpv_bigfloat_unpack: device records at offsets -> planar (L, n) limbs + exponents, mantissa rounded half
+ *   up to at most 32 L - 2 bits (L <= 64, nl <= 64).
+ * sdpv_bigfloat_pack: planar limbs + exponents -> device records at offsets (1 or 13 + 8 nl bytes each);
+ *   a mantissa wider than nl limbs sets SDPV_ERRBIT_OVERFLOW. */
+int sdpv_bigfloat_index(const uint8_t* buf, int64_t len, int64_t pos, int64_t n, int nl, int64_t* offsets,
+                        int64_t* end);
+int sdpv_bigfloat_unpack(const uint8_t* buf, const int64_t* offsets, int64_t n, int nl, int L, int32_t* out,
+                         int64_t* exps, void* stream);
+int sdpv_bigfloat_pack(const int32_t* m, const int64_t* e, int64_t n, int L, int nl, const int64_t* offsets,
+                       uint8_t* out, void* stream);
 /* Schur complement of one chunk: S (L, nb, P, P) / eS from the pairings AXI, AY (L, 2 nb, W, W) / (2 nb, W, W),
  * W = dim K, P = K dim (dim + 1) / 2, in one launch with the reference's products and sums in its order
  * (bit-exact); S symmetric, diagonal entries of rows with xmask (nb, P, bytes) false set to one_m / one_e

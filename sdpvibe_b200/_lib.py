@@ -37,6 +37,9 @@ _SIGS = {
     "sdpv_mpf_norm": [_I, _I, _L, _P, _P, _P, _P, _P],
     "sdpv_mpf_from_f64": [_I, _L, _P, _P, _P, _P],
     "sdpv_schur_assemble": [_I, _L, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _P, _P],
+    "sdpv_bigfloat_index": [_P, _L, _L, _L, _I, _P, _P],
+    "sdpv_bigfloat_unpack": [_P, _P, _L, _I, _I, _P, _P, _P],
+    "sdpv_bigfloat_pack": [_P, _P, _L, _I, _I, _P, _P, _P],
     "sdpv_top_max": [_P, _P, _I, _L, _L, _L, _I, _P, _P],
     "sdpv_align": [_P, _P, _I, _L, _L, _L, _P, _I, _I, _I, _P, _P],
     "sdpv_residues": [_P, _P, _L, _L, _L, _L, _I, _I, _P, _P, _L, _P],

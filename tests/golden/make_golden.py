@@ -337,6 +337,52 @@ def case_blockchol():
          up_e=up.e, x_m=xs.m, x_e=xs.e, log2_cond=np.float64(ch.log2_cond()))
 
 
+def case_bigfloat():
+    # sdpvibe/_bigfloat.c via sdpvibe/sdp_io.py: a block written by write_block_bin (boost binary archive of
+    # El::BigFloat records) and read back by read_block; plus raw records of every kind for the decoder
+    from sdpvibe import sdp_io
+    import struct
+    rng = random.Random(31)
+    for tag, (L, precision, dim, K, N, h) in {"L8_p200": (8, 200, 2, 3, 4, 2), "L26_p768": (26, 768, 1, 5, 3, 3)}.items():
+        npair = dim * (dim + 1) // 2
+        def host(shape, elo, ehi, zf=0.2):
+            A = rmpf(rng, shape, L, elo, ehi, zf)
+            return A.m.reshape(L, -1).T.contiguous().numpy(), A.e.reshape(-1).numpy()
+        blk = {"dim": dim, "K": K, "B": host((K * npair, N), -30, 30), "c": host((K * npair,), -10, 10),
+               "bilinear_bases_even": (h, host((h, K), -5, 5)), "bilinear_bases_odd": (0, None)}
+        path = os.path.join("/tmp", f"block_{tag}.bin")
+        sdp_io.write_block_bin(path, blk, precision, L, N)
+        raw = open(path, "rb").read()
+        r = sdp_io._BinReader(raw, L)
+        _, _, Bl, Be = r.matrix()
+        cl, ce = r.vector()
+        bases = [r.matrix(), r.matrix()]
+        save(f"bigfloat_block_{tag}", raw=np.frombuffer(raw, np.uint8), L=L, precision=precision, dim=dim, K=K, N=N,
+             h=h, Bl=Bl, Be=Be, cl=cl, ce=ce, hl=bases[0][2], he=bases[0][3], in_Bl=blk["B"][0], in_Be=blk["B"][1])
+    # raw records: zeros (flag), zero mantissa, short sizes, negative, rounding carries, limbs past size
+    for nl, L in ((4, 4), (13, 26), (3, 8)):
+        recs, n = bytearray(), 0
+        for kind in range(60):
+            if kind % 7 == 0:
+                recs += b"\x01"; n += 1; continue
+            asz = rng.randint(0, nl)
+            limbs = [rng.getrandbits(64) for _ in range(nl)]
+            if kind % 11 == 0:
+                limbs[:asz] = [(1 << 64) - 1] * asz                     # rounding carries through
+            size = -asz if rng.random() < 0.5 else asz
+            exp = rng.randint(-40, 40)
+            recs += b"\x00" + struct.pack("<iq", size, exp) + struct.pack(f"<{nl}Q", *limbs)
+            n += 1
+        buf = np.frombuffer(bytes(recs), np.uint8)
+        lim = np.empty((n, L), np.int32)
+        ex = np.empty(n, np.int64)
+        lib = sdp_io._lib()
+        q = lib.decode_bigfloats(buf.ctypes.data, len(buf), 0, n, nl, L, lim.ctypes.data, ex.ctypes.data, mpf.EZ)
+        enc = sdp_io._encode(lim, ex, nl, L)
+        save(f"bigfloat_records_nl{nl}_L{L}", raw=buf, n=n, nl=nl, L=L, limbs=lim, exps=ex, end=q,
+             enc=np.frombuffer(enc, np.uint8))
+
+
 def case_basecase():
     # sdpvibe/basecase.py:268-293 on single 32x32 tiles (equilibrated, fixed point)
     rng = random.Random(23)
