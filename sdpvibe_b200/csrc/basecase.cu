@@ -320,19 +320,40 @@ __device__ __forceinline__ void mac96(u32& c0, u32& c1, u32& c2, u32 x, u32 y) {
 
 __device__ __forceinline__ void column96(u32& c0, u32& c1, u32& c2, const u32* x, const u32* y, int k, int i0,
                                          int i1) {
-  u32 d0 = 0, d1 = 0, d2 = 0;
+  // four independent carry chains (the sum is exact whatever the grouping), loads of eight terms ahead
+  u32 d0 = 0, d1 = 0, d2 = 0, e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
   int i = i0;
-  for (; i + 3 <= i1; i += 4) {
+  for (; i + 7 <= i1; i += 8) {
+    u32 a[8], b[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      a[u] = x[i + u];
+      b[u] = y[k - i - u];
+    }
+    mac96(c0, c1, c2, a[0], b[0]);
+    mac96(d0, d1, d2, a[1], b[1]);
+    mac96(e0, e1, e2, a[2], b[2]);
+    mac96(f0, f1, f2, a[3], b[3]);
+    mac96(c0, c1, c2, a[4], b[4]);
+    mac96(d0, d1, d2, a[5], b[5]);
+    mac96(e0, e1, e2, a[6], b[6]);
+    mac96(f0, f1, f2, a[7], b[7]);
+  }
+  if (i + 3 <= i1) {
     const u32 a0 = x[i], a1 = x[i + 1], a2 = x[i + 2], a3 = x[i + 3];
     const u32 b0 = y[k - i], b1 = y[k - i - 1], b2 = y[k - i - 2], b3 = y[k - i - 3];
     mac96(c0, c1, c2, a0, b0);
     mac96(d0, d1, d2, a1, b1);
-    mac96(c0, c1, c2, a2, b2);
-    mac96(d0, d1, d2, a3, b3);
+    mac96(e0, e1, e2, a2, b2);
+    mac96(f0, f1, f2, a3, b3);
+    i += 4;
   }
   for (; i <= i1; i++) mac96(c0, c1, c2, x[i], y[k - i]);
+  add96(d0, d1, d2, f0, f1, f2);
+  add96(c0, c1, c2, e0, e1, e2);
   add96(c0, c1, c2, d0, d1, d2);
 }
+
 
 // Carry into this lane of a 32-lane digit chain: g = this lane's digit overflowed (carry out whatever
 // comes in), p = this lane's digit is all ones (passes a carry on).  cin: carry into lane 0; cout: carry
@@ -511,11 +532,14 @@ __device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arit
   __syncwarp();
 }
 
+// Entries sit in shared memory at an odd pitch of WP = WL | 1 words: the thread products read one operand
+// word per lane from different entries, and an odd pitch puts those words in distinct banks.
+__host__ __device__ constexpr int pitch(int WL) { return WL | 1; }
 __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
-  return (size_t)(528 + 32) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 5 * FW * 4 + 64;
+  return (size_t)(528 + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratch) + 5 * FW * 4 + 64;
 }
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
-  return (size_t)(528 + 32) * WL * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
+  return (size_t)(528 + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
 }
 
 __device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
@@ -524,8 +548,9 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
                                                                    int WL, int LF, unsigned* __restrict__ err) {
   extern __shared__ __align__(16) u32 sm[];
   u32* T = sm;                                                   // lower triangle, entry (i, j) at tri(i, j)
-  u32* colmag = T + 528 * WL;                                    // |l_ik| of the current column
-  WarpScratch* ws = reinterpret_cast<WarpScratch*>(colmag + 32 * WL);
+  const int WP = pitch(WL);
+  u32* colmag = T + 528 * WP;                                    // |l_ik| of the current column
+  WarpScratch* ws = reinterpret_cast<WarpScratch*>(colmag + 32 * WP);
   u32* nw = reinterpret_cast<u32*>(ws + kWarpsS);
   u32 *sd = nw, *sr = nw + FW, *st1 = nw + 2 * FW, *st2 = nw + 3 * FW, *sone = nw + 4 * FW;
   uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * FW);
@@ -535,13 +560,13 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
   u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
   for (int i = 0; i < BT; i++) {
     const u32* src = G + (size_t)i * BT * WL;
-    u32* dst = T + (size_t)tri(i, 0) * WL;
-    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[w];
+    u32* dst = T + (size_t)tri(i, 0) * WP;
+    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[(w / WL) * WP + w % WL] = src[w];
   }
   __syncthreads();
   // Pivot k (warp 0): r = d^-1/2 by the Newton schedule, l_kk = d r, r kept in sr and RINV.
   auto pivot = [&](int k) {
-    u32* akk = T + (size_t)tri(k, k) * WL;
+    u32* akk = T + (size_t)tri(k, k) * WP;
     for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
     for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
     __syncwarp();
@@ -571,14 +596,14 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
   // the same truncated products as without look-ahead (their exact sum is order-free).
   for (int k = 0; k < BT; k++) {
     for (int i = k + 1 + warp; i < BT; i += kWarpsS) {           // l_ik = a_ik * r_k
-      u32* aik = T + (size_t)tri(i, k) * WL;
-      wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WL, colsign + i, coltop + i);
+      u32* aik = T + (size_t)tri(i, k) * WP;
+      wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
     }
     __syncthreads();
     if (k == BT - 1) break;
     if (warp == 0) {
-      u32* dn = T + (size_t)tri(k + 1, k + 1) * WL;                // a_{k+1,k+1} -= l_{k+1,k}^2
-      const u32* lk = colmag + (size_t)(k + 1) * WL;
+      u32* dn = T + (size_t)tri(k + 1, k + 1) * WP;                // a_{k+1,k+1} -= l_{k+1,k}^2
+      const u32* lk = colmag + (size_t)(k + 1) * WP;
       wmul(lk, lk, 0, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
       warp_addsub(dn, dn, st1, true, WL);
       pivot(k + 1);
@@ -589,7 +614,7 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
         while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
         while (ii * (ii + 1) / 2 > p) ii--;
         const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
-        fx_rmw(T + (size_t)tri(i, j) * WL, colmag + (size_t)i * WL, coltop[i], colmag + (size_t)j * WL, coltop[j],
+        fx_rmw(T + (size_t)tri(i, j) * WP, colmag + (size_t)i * WP, coltop[i], colmag + (size_t)j * WP, coltop[j],
                colsign[i] != colsign[j], WL, LF);
       }
     }
@@ -597,8 +622,8 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
   }
   for (int i = 0; i < BT; i++) {
     u32* dst = G + (size_t)i * BT * WL;
-    const u32* src = T + (size_t)tri(i, 0) * WL;
-    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[w];
+    const u32* src = T + (size_t)tri(i, 0) * WP;
+    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[(w / WL) * WP + w % WL];
   }
 }
 
@@ -612,8 +637,9 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
                                                                     u32* __restrict__ X, int WL, int LF) {
   extern __shared__ __align__(16) u32 sm[];
   u32* Xm = sm;                                                  // slots tri(i, k), lower triangle
-  u32* Lcol = Xm + 528 * WL;                                     // |l_ij| of the current column j, by row i
-  WarpScratch* ws = reinterpret_cast<WarpScratch*>(Lcol + 32 * WL);
+  const int WP = pitch(WL);
+  u32* Lcol = Xm + 528 * WP;                                     // |l_ij| of the current column j, by row i
+  WarpScratch* ws = reinterpret_cast<WarpScratch*>(Lcol + 32 * WP);
   uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of finished x
   uint8_t* xt = xs + 528;
   uint8_t* ls = xt + 528;                                        // signs, tops of the column of L
@@ -622,11 +648,11 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
   const u32* LG = Lt + (size_t)blockIdx.x * BT * BT * WL;
   const u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
   u32* XG = X + (size_t)blockIdx.x * BT * BT * WL;
-  for (int e = tid; e < 528 * WL; e += kThreadsS) Xm[e] = 0;
+  for (int e = tid; e < 528 * WP; e += kThreadsS) Xm[e] = 0;
   __syncthreads();
   for (int i = warp; i < BT; i += kWarpsS) {                     // x_ii = r_i
     int top;
-    const int sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WL, WL, top);
+    const int sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WP, WL, top);
     if (lane == 0) {
       xs[tri(i, i)] = (uint8_t)sg;
       xt[tri(i, i)] = (uint8_t)top;
@@ -635,7 +661,7 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
   for (int j = 0; j < BT - 1; j++) {
     for (int i = j + 1 + warp; i < BT; i += kWarpsS) {
       int top;
-      const int sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WL, WL, top);
+      const int sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WP, WL, top);
       if (lane == 0) {
         ls[i] = (uint8_t)sg;
         lt[i] = (uint8_t)top;
@@ -646,13 +672,13 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
     for (int p = tid; p < np; p += kThreadsS) {                  // slot (i, k) += l_ij x_jk
       const int i = j + 1 + p / nk, k = p % nk;
       const int e = tri(j, k);
-      fx_rmw(Xm + (size_t)tri(i, k) * WL, Lcol + (size_t)i * WL, lt[i], Xm + (size_t)e * WL, xt[e], ls[i] == xs[e],
+      fx_rmw(Xm + (size_t)tri(i, k) * WP, Lcol + (size_t)i * WP, lt[i], Xm + (size_t)e * WP, xt[e], ls[i] == xs[e],
              WL, LF);
     }
     __syncthreads();
     for (int k = warp; k <= j; k += kWarpsS) {                   // x_{j+1,k} = -(sum) r_{j+1}
       const int ei = tri(j + 1, k);
-      wmul(Xm + (size_t)ei * WL, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WL,
+      wmul(Xm + (size_t)ei * WP, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WP,
            xs + ei, xt + ei);
       if (lane == 0) xs[ei] ^= 1;                                // the negation
       __syncwarp();
@@ -667,7 +693,7 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
       continue;
     }
     const int ei = tri(i, k);
-    u32 v0 = lane < WL ? Xm[(size_t)ei * WL + lane] : 0u, v1 = lane + 32 < WL ? Xm[(size_t)ei * WL + lane + 32] : 0u;
+    u32 v0 = lane < WL ? Xm[(size_t)ei * WP + lane] : 0u, v1 = lane + 32 < WL ? Xm[(size_t)ei * WP + lane + 32] : 0u;
     if (xs[ei]) warp_negate(v0, v1, WL);
     if (lane < WL) dst[lane] = v0;
     if (lane + 32 < WL) dst[lane + 32] = v1;
