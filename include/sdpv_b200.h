@@ -86,6 +86,18 @@ int sdpv_mpf_mul(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
 /* O = A + sgn*B entrywise.  Replaces mpf.add / mpf_add (sdpvibe/mpf.py:92-124, 326-331). */
 int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
                  int sgn, int32_t* O, int64_t* eO, void* stream);
+/* ---------------------------------------------------------------- launch-shape knobs (autotuner)
+ * Results never depend on them.  SDPV_TUNE_CRT_CTAS: CRT CTAs per SM (1..4, default 3);
+ * SDPV_TUNE_NARROW_MAX: residue-GEMM narrow items when one side has at most this many rows (0 = never,
+ * else a multiple of 16 up to 64; default 64); SDPV_TUNE_PACK_MAX: small blocks packed several to a tile
+ * when both sides have at most this many rows (0 = never, multiple of 16 up to 64; default 64).
+ * No reference counterpart (the reference's launch shapes are fixed). */
+#define SDPV_TUNE_CRT_CTAS 0
+#define SDPV_TUNE_NARROW_MAX 1
+#define SDPV_TUNE_PACK_MAX 2
+#define SDPV_TUNE_COUNT 3
+int sdpv_tune_set(int knob, int value);
+int sdpv_tune_get(int knob, int* value);
 /* ---------------------------------------------------------------- binary SDP records (El::BigFloat over GMP limbs)
  * Record: byte is_zero; unless zero, int32 size, int64 exp, nl 64-bit limbs; value = sign(size) M
  * 2^(64 (exp - |size|)).  Replaces decode_bigfloats / encode_bigfloats (sdpvibe/_bigfloat.c:16-111).

@@ -38,6 +38,8 @@ _SIGS = {
     "sdpv_mpf_from_f64": [_I, _L, _P, _P, _P, _P],
     "sdpv_schur_assemble": [_I, _L, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _P, _P],
     "sdpv_bigfloat_index": [_P, _L, _L, _L, _I, _P, _P],
+    "sdpv_tune_set": [_I, _I],
+    "sdpv_tune_get": [_I, _P],
     "sdpv_bigfloat_unpack": [_P, _P, _L, _I, _I, _P, _P, _P],
     "sdpv_bigfloat_pack": [_P, _P, _L, _I, _I, _P, _P, _P],
     "sdpv_top_max": [_P, _P, _I, _L, _L, _L, _I, _P, _P],
@@ -73,8 +75,31 @@ def lib():
                     f = getattr(h, name)
                     f.argtypes = argt
                     f.restype = ctypes.c_char_p if name == "sdpv_last_error" else ctypes.c_int
+                _apply_tuning(h)
                 _lib = h
     return _lib
+
+
+TUNING_TABLE = os.path.join(HERE, "tuning_b200.json")
+
+
+def _apply_tuning(h):
+    """the autotuner's launch-shape knobs (sdpvibe_b200/autotune.py), when its table was made on this GPU
+    model; SDPV_TUNING=0 keeps the defaults"""
+    if os.environ.get("SDPV_TUNING", "1") == "0" or not os.path.exists(TUNING_TABLE):
+        return
+    try:
+        import json
+        with open(TUNING_TABLE) as f:
+            table = json.load(f)
+        if not torch.cuda.is_available() or table.get("device") != torch.cuda.get_device_name():
+            return
+    except (OSError, ValueError, RuntimeError):
+        return
+    ids = {"crt_ctas": 0, "narrow_max": 1, "pack_max": 2}
+    for name, value in table.get("knobs", {}).items():
+        if name in ids:
+            h.sdpv_tune_set(ids[name], int(value))
 
 
 def stream():

@@ -13,7 +13,7 @@ _active = None
 
 # Entry points that configure or query rather than launch a kernel.
 NON_LAUNCH = {"sdpv_version", "sdpv_last_error", "sdpv_ctx_create", "sdpv_ctx_destroy", "sdpv_ctx_query",
-              "sdpv_ctx_moduli", "sdpv_get_error", "sdpv_bigfloat_index"}
+              "sdpv_ctx_moduli", "sdpv_get_error", "sdpv_bigfloat_index", "sdpv_tune_set", "sdpv_tune_get"}
 
 
 class Trace:

@@ -18,6 +18,7 @@ namespace sdpv {
 int set_cuda_error(cudaError_t e);         // records the text, returns SDPV_ECUDA
 void set_message(const char* msg);         // records a diagnostic for sdpv_last_error
 unsigned* device_error_word();             // this device's error word (no allocation)
+int tune(int knob);                        // launch-shape knob (SDPV_TUNE_*), see tuning.cu
 inline int launch_status() {
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? SDPV_OK : set_cuda_error(e);

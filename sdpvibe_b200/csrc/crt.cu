@@ -243,7 +243,7 @@ int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i6
   i64 ntiles = (B + 127) / 128;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  i64 gx = 3 * (i64)sms;
+  i64 gx = (i64)sdpv::tune(SDPV_TUNE_CRT_CTAS) * sms;
   if (gx > ntiles) gx = ntiles;
   crt_kernel<MODE><<<(unsigned)gx, kThreads, smem, st>>>(acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, d.n, d.E,
                                                           d.W, d.ktc, d.Epad, d.mods, d.minv, d.inv, d.md, d.ct, out,

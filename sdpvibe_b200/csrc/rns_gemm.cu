@@ -608,7 +608,8 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   // Small blocks (M, N <= 64, not syrk) are packed: pack blocks share one 128 x 128 tile (their stacked rows
   // against their stacked B rows; only the diagonal sub-blocks are kept), so fewer, fuller tiles run.
   int pack = 1;
-  if (mode == 0 && nb > 1 && M <= 64 && N <= 64) {
+  const int pack_max = sdpv::tune(SDPV_TUNE_PACK_MAX), narrow_max = sdpv::tune(SDPV_TUNE_NARROW_MAX);
+  if (mode == 0 && nb > 1 && M <= pack_max && N <= pack_max) {
     i64 p = 128 / M < 128 / N ? 128 / M : 128 / N;
     pack = (int)(p < nb ? p : nb);
   }
@@ -617,8 +618,8 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   // A is the long side, 2: B is (C stored transposed from the tile).
   int nmode = 0, nTB = 0;
   if (mode == 0 && pack <= 1) {
-    if (N <= 64 && M > 64) nmode = 1;
-    else if (M <= 64 && N > 64) nmode = 2;
+    if (N <= narrow_max && M > narrow_max) nmode = 1;
+    else if (M <= narrow_max && N > narrow_max) nmode = 2;
     if (nmode) nTB = (int)(((nmode == 1 ? N : M) + 15) / 16 * 16);
   }
   CUtensorMap mAh, mAl, mBh, mBl;

@@ -33,3 +33,20 @@ def test_library_exports_every_declared_symbol():
 def test_python_binding_covers_header():
     from sdpvibe_b200 import _lib
     assert set(declared()) <= set(_lib._SIGS)
+
+
+def test_tuning_knobs_validated():
+    """the launch-shape knobs accept their documented ranges only (host-side, no GPU)"""
+    import ctypes
+    from sdpvibe_b200 import _lib
+    h = _lib.lib()
+    v = ctypes.c_int(0)
+    for knob, good, bad in ((0, (1, 4), (0, 5)), (1, (0, 32, 64), (8, 80)), (2, (0, 64), (-16, 128))):
+        assert h.sdpv_tune_get(knob, ctypes.byref(v)) == 0
+        old = v.value
+        for g in good:
+            assert h.sdpv_tune_set(knob, g) == 0
+        for b in bad:
+            assert h.sdpv_tune_set(knob, b) == _lib.EINVAL
+        assert h.sdpv_tune_set(knob, old) == 0
+    assert h.sdpv_tune_set(3, 1) == _lib.EINVAL

@@ -644,3 +644,38 @@ def test_rns_gemm_fresh_overwrites(sb, nb, M, N, K):
         sl = slice(b * M, (b + 1) * M)
         ref = O.accumulate(T, Ah[:, sl], Al[:, sl], Bh[:, b * N:(b + 1) * N], Bl[:, b * N:(b + 1) * N], zero, 0)
         assert np.array_equal(got[:, sl], ref)
+
+
+def test_tuning_knobs_do_not_change_results(sb):
+    """every value of the launch-shape knobs gives the same bits: narrow items on or off, packing on or
+    off, CRT CTAs per SM"""
+    from sdpvibe_b200.autotune import set_knob, get_knob
+    from sdpvibe_b200.mpmat import ctx
+    L = 26
+    rng = np.random.default_rng(12)
+    T = O.tables(L)
+    R = ctx(L)
+    saved = {k: get_knob(k) for k in ("crt_ctas", "narrow_max", "pack_max")}
+    try:
+        for nb, M, N, K in ((4, 32, 300, 32), (6, 32, 40, 48)):
+            Ah, Al = _rand_residues(rng, T, T.n, nb * M, K)
+            Bh, Bl = _rand_residues(rng, T, T.n, nb * N, K)
+            outs = []
+            for nm, pm in ((64, 64), (0, 0), (32, 32)):
+                set_knob("narrow_max", nm)
+                set_knob("pack_max", pm)
+                acc = torch.zeros((T.n, nb * M, N), dtype=torch.int16, device="cuda")
+                R.accumulate(cu(Ah), cu(Al), cu(Bh), cu(Bl), acc, nb=nb, fresh=True)
+                outs.append(np_(acc))
+            assert all(np.array_equal(outs[0], o) for o in outs[1:])
+        m = T.m32.astype(np.int64)[:, None, None]
+        acc = cu((rng.integers(0, 1 << 30, size=(T.n, 70, 90)) % m).astype(np.int16))
+        got = []
+        for c in (1, 2, 3, 4):
+            set_knob("crt_ctas", c)
+            W, bl, _ = R.crt_block(acc, 90, 0, 90, 70)
+            got.append((np_(W), np_(bl)))
+        assert all(np.array_equal(got[0][0], g[0]) and np.array_equal(got[0][1], g[1]) for g in got[1:])
+    finally:
+        for k, v in saved.items():
+            set_knob(k, v)
