@@ -303,7 +303,7 @@ def run_b200(args, rank, world, local_rank):
         graph.replay()
     with ClockSampler(local_rank) as clk:
         ms = timed(graph.replay, args.steps)
-    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues_u8", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
     ms_eager = timed(step, args.steps, tr)
     for _ in range(2):
         step_e2e()
@@ -312,7 +312,7 @@ def run_b200(args, rank, world, local_rank):
     t_step = ms / args.steps * 1e-3
     value = world * algorithmic_ops(R) / t_step / 1e12
     gemm_ms = tr.kernel_ms("sdpv_rns_gemm")
-    res_ms = tr.kernel_ms("sdpv_residues")
+    res_ms = tr.kernel_ms("sdpv_residues_u8")
     crt_ms = tr.kernel_ms("sdpv_crt_norm")
     hbm, bf16, src = load_peaks()
     if rank != 0:
@@ -337,7 +337,7 @@ def run_b200(args, rank, world, local_rank):
                      "int8_cublaslt_measured_tops": int8_lib,
                      "launch_ms_mean": statistics.mean(gemm_ms), "launches": len(gemm_ms),
                      "ops_per_launch": ops_per_launch},
-        "roofline_decomposition": {"bound": "hbm", "kernel": "sdpv_residues", "achieved":
+        "roofline_decomposition": {"bound": "hbm", "kernel": "sdpv_residues_u8", "achieved":
                                    res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                                    "frac": res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9 / hbm,
                                    "launch_ms_mean": statistics.mean(res_ms), "bytes_per_launch": res_bytes},
@@ -435,7 +435,8 @@ def run_cholsolve(args, rank, world, local_rank):
         return s.elapsed_time(e)
     for _ in range(max(args.warmup, 3)):
         step()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_norm",
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_rns_gemm",
+             "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
              "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
     tr = _trace.Trace(timed=names)
@@ -607,7 +608,8 @@ def solver_measurement(steps, warmup, local_rank, world=1):
             s.timer.marks.clear()
             tr.launches.clear()
             tr.events.clear()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_norm",
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_rns_gemm",
+             "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
              "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
     tr = _trace.Trace(timed=names)              # graph replays are timed whole, one entry per graph key

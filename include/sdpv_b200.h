@@ -150,6 +150,11 @@ int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R,
  * Replaces RNS.residues / _residue_kernel (sdpvibe/rns.py:66-103, 196-214). */
 int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0,
                   int G, int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream);
+/* The same decomposition in the GEMM's internal digit format: the canonical residue r in [0, m) as
+ * Rhi = r >> 7 in [0, 256), Rlo = r & 127 (uint8), for sdpv_rns_gemm with mode bit 2.  No reference
+ * counterpart (an internal format: one centring correction less per residue). */
+int sdpv_residues_u8(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0,
+                     int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride, void* stream);
 
 /* ---------------------------------------------------------------- residue GEMM (b) and Gram (d)
  * For each of the G moduli g0..g0+G and each of nb blocks:
@@ -158,7 +163,8 @@ int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t l
  * acc (n, nb*M, ldc) int16 (row stride ldc >= N; a
  * multiple of 8 lets the epilogue move 16 bytes at a time).  mode bit 0 clear: all entries;
  * set (syrk): B = A (Bhi/Blo ignored, N = M) and only entries with i >= j are updated.  mode bit 1 set
- * (fresh): the updated entries of acc are taken as zero and overwritten, not read.
+ * (fresh): the updated entries of acc are taken as zero and overwritten, not read.  mode bit 2 set: the
+ * operands are unsigned digits (sdpv_residues_u8; KC <= 32768 keeps the int32 sums exact).
  * KC must be a multiple of 16 and <= 65536.  Replaces RNS.accumulate / _gemm_kernel
  * (sdpvibe/rns.py:106-137, 217-224), batched._bgemm_kernel (sdpvibe/batched.py:96-127) and
  * batched._syrk_lower_kernel (sdpvibe/batched.py:130-162). */

@@ -181,6 +181,10 @@ __device__ __forceinline__ void mma_commit(u64* bar) {
 __host__ __device__ constexpr u32 idesc_i8(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((u32)(N >> 3) << 17) | ((u32)(M >> 4) << 24);
 }
+// The same with unsigned 8-bit A and B (digit formats 0).
+__host__ __device__ constexpr u32 idesc_u8(int M, int N) {
+  return (2u << 4) | ((u32)(N >> 3) << 17) | ((u32)(M >> 4) << 24);
+}
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 bytes apart.
 __device__ __forceinline__ u64 sdesc_sw128(u32 smem_addr) {
   u64 d = 0;

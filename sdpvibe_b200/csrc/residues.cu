@@ -35,7 +35,27 @@ struct ResSmem {
   int abort;
 };
 
-template <int KT, int TILE, int THREADS>
+// Digits of the residue of v (congruent to the entry mod m): round(v / m) from the float estimate (off by
+// at most one), then either the centred residue r in [-(m >> 1), m >> 1] split r = 128 hi + lo, lo in
+// [-64, 64) (the API format, int8 digits) or, for the GEMM's internal operands (U8), the canonical residue
+// r in [0, m) split hi = r >> 7 in [0, 256), lo = r & 127 (unsigned digits, one correction fewer).
+template <bool U8>
+__device__ __forceinline__ void residue_digits(int v, int m, int hm, float minv, int& hb, int& lb) {
+  const float t = fmaf((float)v, minv, 12582912.0f);               // round(v/m) in the low mantissa
+  int r = v - (__float_as_int(t) - 0x4B400000) * m;                // |r| <= m/2 + m/300
+  if (U8) {
+    r += (r < 0) ? m : 0;
+    hb = r >> 7;
+    lb = r & 127;
+  } else {
+    r -= (r > hm) ? m : 0;                                         // exact centring
+    r += (r < -hm) ? m : 0;
+    hb = (r + 64) >> 7;
+    lb = r - (hb << 7);
+  }
+}
+
+template <int KT, int TILE, int THREADS, bool U8>
 __global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
     residues_kernel(const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
                     int group0, const uint8_t* __restrict__ tab, const int32_t* __restrict__ mods,
@@ -167,15 +187,8 @@ __global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
       for (int j = 0; j < 32; j += 4) {
         int hb[4], lb[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          int v = 128 * (int)hi[j + u] + (int)lo[j + u];                 // congruent to the entry mod m
-          float t = fmaf((float)v, minv, 12582912.0f);                     // round(v/m) in the low mantissa
-          int r = v - (__float_as_int(t) - 0x4B400000) * m;                // |r| <= m/2 + m/300
-          r -= (r > hm) ? m : 0;                                           // exact centring
-          r += (r < -hm) ? m : 0;
-          hb[u] = (r + 64) >> 7;                                           // r = 128 hi + lo, lo in [-64, 64)
-          lb[u] = r - (hb[u] << 7);
-        }
+        for (int u = 0; u < 4; u++)
+          residue_digits<U8>(128 * (int)hi[j + u] + (int)lo[j + u], m, hm, minv, hb[u], lb[u]);
         ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
         pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
       }
@@ -246,7 +259,7 @@ __device__ __forceinline__ bool named_sync_or(int id, int nthreads, bool pred) {
   return out != 0;
 }
 
-template <int KT, int RAW, int STG>
+template <int KT, int RAW, int STG, bool U8>
 __global__ void __launch_bounds__(WS_THREADS, 1)
     residues_ws_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
                        int use_tma, const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp,
@@ -402,15 +415,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         for (int j = 0; j < 32; j += 4) {
           int hb[4], lb[4];
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            int v = 128 * (int)hi[j + u] + (int)lo[j + u];
-            float t = fmaf((float)v, minv, 12582912.0f);
-            int r = v - (__float_as_int(t) - 0x4B400000) * m;
-            r -= (r > hm) ? m : 0;
-            r += (r < -hm) ? m : 0;
-            hb[u] = (r + 64) >> 7;
-            lb[u] = r - (hb[u] << 7);
-          }
+          for (int u = 0; u < 4; u++)
+            residue_digits<U8>(128 * (int)hi[j + u] + (int)lo[j + u], m, hm, minv, hb[u], lb[u]);
           ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
           pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
         }
@@ -471,7 +477,7 @@ int num_sms() {
   return v;
 }
 
-template <int KT, int TILE, int THREADS>
+template <int KT, int TILE, int THREADS, bool U8>
 int launch_residues(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
                     int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   const sdpv::CtxDev& d = c->d;
@@ -487,7 +493,7 @@ int launch_residues(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(residues_kernel<KT, TILE, THREADS>,
+    cudaError_t e = cudaFuncSetAttribute(residues_kernel<KT, TILE, THREADS, U8>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return sdpv::set_cuda_error(e);
     attr_set[dev & 63] = true;
@@ -497,7 +503,7 @@ int launch_residues(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k
   i64 gx = per_sm * (i64)num_sms();
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
-  residues_kernel<KT, TILE, THREADS><<<grid, THREADS, smem, st>>>(X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tab,
+  residues_kernel<KT, TILE, THREADS, U8><<<grid, THREADS, smem, st>>>(X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tab,
                                                                    d.mods, d.minv, d.n, Rhi, Rlo, ps,
                                                                    sdpv::device_error_word());
   return sdpv::launch_status();
@@ -516,7 +522,7 @@ bool res_store_map(CUtensorMap* map, void* base, i64 nent, i64 G, i64 ps) {
          CUDA_SUCCESS;
 }
 
-template <int KT, int RAW, int STG>
+template <int KT, int RAW, int STG, bool U8>
 int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
               int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   const sdpv::CtxDev& d = c->d;
@@ -526,7 +532,7 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG>,
+    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG, U8>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return sdpv::set_cuda_error(e);
     attr_set[dev & 63] = true;
@@ -545,13 +551,13 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
   i64 gx = num_sms();
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
-  residues_ws_kernel<KT, RAW, STG><<<grid, WS_THREADS, smem, st>>>(mh, ml, use_tma, X, d.L, rows, ld, k0, kc, kp, g0,
+  residues_ws_kernel<KT, RAW, STG, U8><<<grid, WS_THREADS, smem, st>>>(mh, ml, use_tma, X, d.L, rows, ld, k0, kc, kp, g0,
                                                                     G, grp0, d.tab, d.mods, d.minv, d.n, Rhi, Rlo,
                                                                     ps, sdpv::device_error_word());
   return sdpv::launch_status();
 }
 
-template <int KT>
+template <int KT, bool U8>
 int launch_kt(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
               int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   static int tile = [] {
@@ -561,16 +567,17 @@ int launch_kt(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
     if (v && atoi(v) == 64) return 64;
     return 0;
   }();
-  if (tile == 0 && KT == 1) return launch_ws<1, 3, 2>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-  if (tile == 0 && KT == 2) return launch_ws<2, 2, 1>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-  if (tile == 128) return launch_residues<KT, 128, 256>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-  return launch_residues<KT, 64, 128>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 0 && KT == 1) return launch_ws<1, 3, 2, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 0 && KT == 2) return launch_ws<2, 2, 1, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 128) return launch_residues<KT, 128, 256, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  return launch_residues<KT, 64, 128, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
 }
 
 }  // namespace
 
-extern "C" int sdpv_residues(const sdpv_ctx* c, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc,
-                             int g0, int G, int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream) {
+template <bool U8>
+int residues_entry(const sdpv_ctx* c, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0, int G,
+                   int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream) {
   if (!c || rows < 0 || kc < 0 || k0 < 0 || k0 + kc > ld || g0 < 0 || G < 1 || g0 + G > c->d.n) return SDPV_EINVAL;
   i64 kp = (kc + 15) / 16 * 16;
   i64 ps = plane_stride ? plane_stride : rows * kp;
@@ -578,9 +585,20 @@ extern "C" int sdpv_residues(const sdpv_ctx* c, const int32_t* X, int64_t rows, 
   if (rows == 0 || kp == 0) return SDPV_OK;
   cudaStream_t st = sdpv::as_stream(stream);
   switch (c->d.kt) {
-    case 1: return launch_kt<1>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-    case 2: return launch_kt<2>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-    case 3: return launch_kt<3>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    case 1: return launch_kt<1, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    case 2: return launch_kt<2, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+    case 3: return launch_kt<3, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
     default: return SDPV_EINVAL;                        // L > 94
   }
+}
+
+extern "C" int sdpv_residues(const sdpv_ctx* c, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc,
+                             int g0, int G, int8_t* Rhi, int8_t* Rlo, int64_t plane_stride, void* stream) {
+  return residues_entry<false>(c, X, rows, ld, k0, kc, g0, G, Rhi, Rlo, plane_stride, stream);
+}
+
+extern "C" int sdpv_residues_u8(const sdpv_ctx* c, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc,
+                                int g0, int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride, void* stream) {
+  return residues_entry<true>(c, X, rows, ld, k0, kc, g0, G, reinterpret_cast<int8_t*>(Rhi),
+                              reinterpret_cast<int8_t*>(Rlo), plane_stride, stream);
 }

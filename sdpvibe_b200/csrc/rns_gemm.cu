@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
-                    int nfull, int nmode, int nTB,
+                    int nfull, int nmode, int nTB, int u8ops,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       // narrow items: as the tail items, N = 2 TB over [Bhi; Blo], in two TMEM buffers (256 columns apart)
       // so that an item's MMAs run while the epilogue still reads the previous item
       const int TB = nTB;
-      const u32 idesc = idesc_i8(128, 2 * TB), idescT = idesc_i8(128, TB);
+      const u32 idesc = u8ops ? idesc_u8(128, 2 * TB) : idesc_i8(128, 2 * TB);
+      const u32 idescT = u8ops ? idesc_u8(128, TB) : idesc_i8(128, TB);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
         const u32 buf = li & 1;
@@ -255,7 +256,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (lane == 0) {
       // tail items: N = 2 TB over [Bhi; Blo] (hh | hl at column 0, (hl + lh) | ll at column TB)
       const int TB = tailTB ? tailTB : 128;
-      const u32 idesc = idesc_i8(128, 2 * TB), idesc128 = idesc_i8(128, TB);
+      const u32 idesc = u8ops ? idesc_u8(128, 2 * TB) : idesc_i8(128, 2 * TB);
+      const u32 idesc128 = u8ops ? idesc_u8(128, TB) : idesc_i8(128, TB);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
         bool diag = false;
@@ -589,9 +591,11 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
                              const int8_t* Blo, int64_t a_stride, int64_t b_stride, int16_t* acc, int64_t ldc, int g0,
                              int G, int64_t nb, int64_t M, int64_t N, int64_t KC, int mode, void* stream) {
   if (!c || g0 < 0 || G < 1 || g0 + G > c->d.n || nb < 1 || M < 0 || N < 0 || KC < 0 || KC > 65536 ||
-      (KC & 15) || (mode & ~3) || nb > 65535 || G > 65535)
+      (KC & 15) || (mode & ~7) || nb > 65535 || G > 65535)
     return SDPV_EINVAL;
   const bool fresh = (mode & 2) != 0;                  // accumulator known to be zero: overwrite
+  const int u8ops = (mode & 4) ? 1 : 0;                // unsigned digits: int32 sums exact for K <= 32768
+  if (u8ops && KC > 32768) return SDPV_EINVAL;
   mode &= 1;
   if (mode == 1) {
     Bhi = Ahi;
@@ -669,7 +673,7 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       if (nitems == 0) continue;
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
       rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, nmode, nTB, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
+          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
           KC, mode, ntn, ptiles, nitems, fresh, pack, sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;

@@ -197,21 +197,22 @@ def main():
         X = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.N, a.K), dtype=np.int64)
                              .astype(np.int32)).to(dev)
         if a.kernel == "residues":
-            ts = _events(lambda: R.residues(X, 0, a.K, spread=not a.packed), a.reps, a.warmup)
+            ts = _events(lambda: R.residues(X, 0, a.K, spread=not a.packed, unsigned=not a.packed), a.reps, a.warmup)
             bytes_ = a.N * a.K * (4 * a.L + 2 * R.n)
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), gbs=bytes_ / (min(ts) * 1e-3) / 1e9)
         else:
-            Ah, Al = R.residues(X, 0, a.K, spread=not a.packed)
+            Ah, Al = R.residues(X, 0, a.K, spread=not a.packed, unsigned=not a.packed)
             if a.kernel == "syrk":
                 acc = torch.zeros((R.n, a.N, a.N), dtype=torch.int16, device=dev)
-                ts = _events(lambda: R.accumulate(Ah, Al, None, None, acc, syrk=True), a.reps, a.warmup)
+                ts = _events(lambda: R.accumulate(Ah, Al, None, None, acc, syrk=True, unsigned=not a.packed), a.reps,
+                             a.warmup)
                 ops = R.n * 8 * (a.N * (a.N + 1) // 2) * a.K
             else:
                 Y = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.M, a.K), dtype=np.int64)
                                      .astype(np.int32)).to(dev)
-                Bh, Bl = R.residues(Y, 0, a.K, spread=not a.packed)
+                Bh, Bl = R.residues(Y, 0, a.K, spread=not a.packed, unsigned=not a.packed)
                 acc = torch.zeros((R.n, a.M, a.N), dtype=torch.int16, device=dev)
-                ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc), a.reps, a.warmup)
+                ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc, unsigned=not a.packed), a.reps, a.warmup)
                 ops = R.n * 8 * a.M * a.N * a.K
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12)
     elif a.kernel == "bgemm":
@@ -220,11 +221,11 @@ def main():
                              .astype(np.int32)).to(dev)
         Y = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.nb * a.N, a.K), dtype=np.int64)
                              .astype(np.int32)).to(dev)
-        Ah, Al = R.residues(X, 0, a.K, spread=True)
-        Bh, Bl = R.residues(Y, 0, a.K, spread=True)
+        Ah, Al = R.residues(X, 0, a.K, spread=True, unsigned=True)
+        Bh, Bl = R.residues(Y, 0, a.K, spread=True, unsigned=True)
         acc = torch.zeros((R.n, a.nb * a.M, a.N), dtype=torch.int16, device=dev)
-        ts = _events(lambda: R.accumulate(Ah, Al, Bh, Bl, acc, nb=a.nb, fresh=True), a.reps, a.warmup)
-        tr = _events(lambda: R.residues(X, 0, a.K, spread=True), a.reps, a.warmup)
+        ts = _events(lambda: R.accumulate(Ah, Al, Bh, Bl, acc, nb=a.nb, fresh=True, unsigned=True), a.reps, a.warmup)
+        tr = _events(lambda: R.residues(X, 0, a.K, spread=True, unsigned=True), a.reps, a.warmup)
         ops = R.n * 8 * a.nb * a.M * a.N * a.K
         out.update(nb=a.nb, ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12,
                    items=((a.M + 127) // 128) * ((a.N + 127) // 128) * a.nb * R.n, ms_residues_A=min(tr))

@@ -10,7 +10,7 @@ import torch
 from .rns import RNS, dev
 from .limbops import shift_round, add_same, bitlen_words
 
-KC_MAX = 65536            # inner-dimension chunk of one residue GEMM launch (int32 accumulation bound)
+KC_MAX = 32768            # inner-dimension chunk of one residue GEMM launch (int32 bound of unsigned digits)
 RES_BUDGET = 4 << 30      # residue bytes per launch before the moduli are split into groups
 
 
@@ -193,13 +193,13 @@ def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False):
         kk = min(KC_MAX, K - k0)
         for g0 in range(0, R.n, GR):
             G = min(GR, R.n - g0)
-            Ah, Al = R.residues(Av, k0, kk, g0, G, spread=True)
+            Ah, Al = R.residues(Av, k0, kk, g0, G, spread=True, unsigned=True)
             first = fresh and k0 == 0
             if syrk:
-                R.accumulate(Ah, Al, None, None, acc, g0, nb=nb, syrk=True, fresh=first)
+                R.accumulate(Ah, Al, None, None, acc, g0, nb=nb, syrk=True, fresh=first, unsigned=True)
             else:
-                Bh, Bl = R.residues(Bv, k0, kk, g0, G, spread=True)
-                R.accumulate(Ah, Al, Bh, Bl, acc, g0, nb=nb, fresh=first)
+                Bh, Bl = R.residues(Bv, k0, kk, g0, G, spread=True, unsigned=True)
+                R.accumulate(Ah, Al, Bh, Bl, acc, g0, nb=nb, fresh=first, unsigned=True)
             del Ah, Al
 
 
@@ -229,8 +229,8 @@ def _same_product(R, X, acc):
     K = X.shape[2]
     for k0 in range(0, K, KC_MAX):
         kk = min(KC_MAX, K - k0)
-        Ah, Al = R.residues(X, k0, kk, spread=True)
-        R.accumulate(Ah, Al, Ah, Al, acc, fresh=(k0 == 0))
+        Ah, Al = R.residues(X, k0, kk, spread=True, unsigned=True)
+        R.accumulate(Ah, Al, Ah, Al, acc, fresh=(k0 == 0), unsigned=True)
 
 
 def _crt_round(acc, e_in, out_exp, L, colblock=None):

@@ -55,31 +55,34 @@ class RNS:
                 pass
 
     # ---- step 1: residues (sdpvibe/rns.py:196-214)
-    def residues(self, X, k0, kc, g0=0, G=None, spread=False):
+    def residues(self, X, k0, kc, g0=0, G=None, spread=False, unsigned=False):
         """X: (L, rows, K) int32 limb planes -> (Rhi, Rlo) (G, rows, kp) int8, kp = kc rounded up to 16.
         spread=True places the modulus planes an odd multiple of 2 KB apart (a strided view) so the
-        2G output streams spread over the HBM channels; accumulate() accepts either layout."""
+        2G output streams spread over the HBM channels; accumulate() accepts either layout.
+        unsigned=True gives the GEMM's internal digits instead of the API's: the canonical residue
+        r in [0, m) as hi = r >> 7, lo = r & 127 (uint8 planes); pass unsigned=True to accumulate too."""
         L, rows, K = X.shape
         assert L == self.L
         G = G or self.n
         kp = -(-kc // self.KPAD) * self.KPAD
         X = X.contiguous()
+        dt = torch.uint8 if unsigned else torch.int8
         if spread:
             ps = plane_stride(rows * kp)
-            buf_h = torch.empty((G * ps,), dtype=torch.int8, device=X.device)
+            buf_h = torch.empty((G * ps,), dtype=dt, device=X.device)
             buf_l = torch.empty_like(buf_h)
             Rhi = buf_h.as_strided((G, rows, kp), (ps, kp, 1))
             Rlo = buf_l.as_strided((G, rows, kp), (ps, kp, 1))
         else:
             ps = 0
-            Rhi = torch.empty((G, rows, kp), dtype=torch.int8, device=X.device)
+            Rhi = torch.empty((G, rows, kp), dtype=dt, device=X.device)
             Rlo = torch.empty_like(Rhi)
-        _lib.call("sdpv_residues", self._h, _lib.ptr(X), rows, K, k0, kc, g0, G, _lib.ptr_strided(Rhi),
-                  _lib.ptr_strided(Rlo), ps, _lib.stream())
+        _lib.call("sdpv_residues_u8" if unsigned else "sdpv_residues", self._h, _lib.ptr(X), rows, K, k0, kc, g0, G,
+                  _lib.ptr_strided(Rhi), _lib.ptr_strided(Rlo), ps, _lib.stream())
         return Rhi, Rlo
 
     # ---- step 2: accumulate residues of A @ Bt^T (sdpvibe/rns.py:217-224)
-    def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False, fresh=False):
+    def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False, fresh=False, unsigned=False):
         """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows.
         acc may have padded rows (acc.shape[2] >= N): its row stride is passed to the kernel.  fresh: the
         updated entries are overwritten (acc's content there is taken as zero and not read)."""
@@ -94,7 +97,7 @@ class RNS:
             assert t.stride(2) == 1 and t.stride(1) == KC, "residue planes must have packed rows"
         _lib.call("sdpv_rns_gemm", self._h, _lib.ptr_strided(Ahi), _lib.ptr_strided(Alo), _lib.ptr_strided(Bhi),
                   _lib.ptr_strided(Blo), Ahi.stride(0), Bhi.stride(0), _lib.ptr(acc), acc.stride(1), g0, G, nb, M, N,
-                  KC, (1 if syrk else 0) | (2 if fresh else 0), _lib.stream())
+                  KC, (1 if syrk else 0) | (2 if fresh else 0) | (4 if unsigned else 0), _lib.stream())
 
     # ---- step 3: CRT of a block of entries (sdpvibe/rns.py:227-245)
     def crt_block(self, acc, N, j0, w, rows):

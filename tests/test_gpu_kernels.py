@@ -679,3 +679,29 @@ def test_tuning_knobs_do_not_change_results(sb):
     finally:
         for k, v in saved.items():
             set_knob(k, v)
+
+
+
+@pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (24, 37, 700), (26, 5, 4096)])
+def test_unsigned_digit_residues_and_gemm(sb, L, rows, K):
+    """the GEMM's internal digit format: canonical residues r in [0, m) as hi = r >> 7, lo = r & 127 equal the
+    oracle's residues; their products (mode bit 2) equal the oracle's, also as syrk"""
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(L + rows)
+    T = O.tables(L)
+    R = ctx(L)
+    X = rand_limbs(rng, L, rows * K).reshape(L, rows, K)
+    rh, rl = O.residues(T, X, 0, K)                                  # centred (API) digits
+    m = T.m32.astype(np.int64)[:, None, None]
+    rc = ((128 * rh.astype(np.int64) + rl) % m)[:, :, :K]
+    Uh, Ul = R.residues(cu(X), 0, K, spread=True, unsigned=True)
+    assert np.array_equal(np_(Uh)[:, :, :K], (rc >> 7).astype(np.uint8))
+    assert np.array_equal(np_(Ul)[:, :, :K], (rc & 127).astype(np.uint8))
+    M = min(rows, 60)
+    acc0 = (rng.integers(0, 1 << 30, size=(T.n, M, M)) % m).astype(np.int16)
+    for syrk in (False, True):
+        acc = cu(acc0).clone()
+        A_h, A_l = Uh[:, :M].contiguous(), Ul[:, :M].contiguous()
+        R.accumulate(A_h, A_l, A_h, A_l, acc, syrk=syrk, unsigned=True)
+        ref = O.accumulate(T, np_(A_h), np_(A_l), np_(A_h), np_(A_l), acc0, 0, lower=syrk)
+        assert np.array_equal(np_(acc), ref), syrk
