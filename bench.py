@@ -475,6 +475,12 @@ def run_cholsolve(args, rank, world, local_rank):
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cholsolve_cpu_baseline(ns, os.cpu_count() or 1)
+    if args.precision_iters > 0:                 # the same systems solved at L = 50
+        X26 = mpf.chol_solve_many([(A, B) for _, _, A, B in buckets])
+        b50 = cholsolve_buckets(cases, 50)
+        X50 = mpf.chol_solve_many([(A, B) for _, _, A, B in b50])
+        errs = [_rel_mpf_error(a, b) for a, b in zip(X26, X50)]
+        line["error_vs_2x_precision"] = {"L": 50, "max_rel_per_bucket": errs, "max_rel": max(errs)}
     print(json.dumps(line), flush=True)
 
 
@@ -578,8 +584,47 @@ def run_solver(args, rank, world, local_rank):
     degree d ~ U[20,40], K = d+1), N = 1000, L = 26 (the 768-bit precision rule).  A step is one
     iteration; `--warmup` first iterations are excluded; metric s/iteration (lower is better)."""
     line = solver_measurement(args.steps, args.warmup, local_rank, world)
+    if args.precision_iters > 0:
+        line["error_vs_2x_precision"] = solver_precision_check(args.precision_iters)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _rel_mpf_error(A26, A50):
+    """max |A26 - A50| / max |A50| over the entries (A26 widened exactly to A50's limbs, the difference
+    formed in MPF on the device)"""
+    import mpmath as mp
+    from sdpvibe_b200.adjoint import widen
+    from sdpvibe_b200.mpf import add, max_abs
+    with mp.workprec(32 * A50.L + 64):
+        d = max_abs(add(widen(A26, A50.L), A50, -1))
+        ref = max_abs(A50)
+        return float(d / ref) if ref else float(d)
+
+
+def solver_precision_check(iters):
+    """the same SDP (the 26-limb data widened exactly) run at L = 50, twice the working precision: per
+    iteration the relative differences of the primal and dual objectives and the step lengths, and of y
+    after the last iteration.  The step lengths come from float64 eigenvalues of matrices that differ in
+    their last bits, so the iterates agree to about the float64 step-length accuracy, not to 2^-830."""
+    import mpmath as mp
+    from sdpvibe_b200.solver import Solver
+    from sdpvibe_b200.synthetic import ising_like_sdp
+    from sdpvibe_b200.adjoint import widen_sdp
+    sdp, _ = ising_like_sdp(26)
+    runs = {}
+    for L in (26, 50):
+        s = Solver(widen_sdp(sdp, L) if L != 26 else sdp, L)
+        log = []
+        s.run(max_iter=iters, log=log)
+        runs[L] = (log, s.y)
+    with mp.workprec(32 * 50 + 64):
+        def rel(a, b):
+            return float(abs(a - b) / max(abs(b), mp.mpf(10) ** -300))
+        per_it = [{k: rel(a[k], b[k]) for k in ("pobj", "dobj", "P_step", "D_step")}
+                  for a, b in zip(runs[26][0], runs[50][0])]
+    return {"L": 50, "iterations": len(per_it), "max_rel": {k: max(r[k] for r in per_it) for k in per_it[0]},
+            "per_iteration": per_it, "y_rel_last": _rel_mpf_error(runs[26][1], runs[50][1])}
 
 
 def solver_measurement(steps, warmup, local_rank, world=1):
@@ -654,6 +699,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--iters", type=int, default=20, help="sensitivity: solver iterations before the sensitivities")
     ap.add_argument("--fd-dirs", type=int, default=8, help="sensitivity: directions checked by finite differences")
+    ap.add_argument("--precision-iters", type=int, default=6,
+                    help="solver / cholsolve: iterations (solver) compared with a run at twice the precision; 0 skips")
     ap.add_argument("--no-solver", action="store_true", help="gram: skip the SDP s/iteration measurement")
     ap.add_argument("--workload", choices=("gram", "cholsolve", "solver", "sensitivity"), default="gram",
                     help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "
