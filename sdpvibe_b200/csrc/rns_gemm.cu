@@ -20,7 +20,10 @@
 //     accumulators are in registers the epilogue releases TMEM (mbarrier), so the next item's MMAs run
 //     while it reduces and stores; the producer streams the next item's slices through the same ring.
 // int32 accumulation is exact for K <= 65536 (|hh|, |hl + lh| <= K 2^14).
-// Syrk mode (Gram): B = A, only lower-triangle tiles are scheduled and only entries i >= j written.
+// Syrk mode (Gram): B = A, only lower-triangle tiles are scheduled and only entries i >= j written.  When
+// the last row block has at most 32 rows (N = 274: 256 + 18), the diagonal items also multiply their row
+// block by those tail rows (slot 2 of the ring, TMEM columns 384..479), so the row blocks are not read a
+// second time for the tail; one small launch adds the tail rows against themselves.
 #include <mutex>
 
 #include "common.cuh"
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
-                    int nfull, int nmode, int nTB, int u8ops,
+                    int nfull, int ftail, int tfirst, int nmode, int nTB, int u8ops,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (tailTB || nmode) {                    // syrk tail / narrow: big-side row block t against TB rows
           b = (int)(bg % nb);
           g = gofs + (int)(bg / nb);
-          m0 = (int)t * 128;
+          m0 = (int)(t + tfirst) * 128;
           n0 = tailTB ? nfull : 0;
         } else if (pack > 1) {                    // packed: tile t holds blocks t*pack .. (rows stacked)
           b = 0;
@@ -192,10 +195,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_load_4d(S.stage[s][2] + TB * 128, &mTl, &S.full[s], kx, n0, b, g);
             continue;
           }
-          mbar_expect_tx(&S.full[s], (diag ? 2 : 4) * kSlice);
+          mbar_expect_tx(&S.full[s], (diag ? 2 * kSlice + 2 * ftail * 128 : 4 * kSlice));
           tma_load_4d(S.stage[s][0], &mAh, &S.full[s], kx, m0, b, g);
           tma_load_4d(S.stage[s][1], &mAl, &S.full[s], kx, m0, b, g);
-          if (diag) continue;                     // [Ahi; Alo] in slots 0, 1 serve as [Bhi; Blo]
+          if (diag) {                             // [Ahi; Alo] in slots 0, 1 serve as [Bhi; Blo]
+            if (ftail) {                          // fused syrk tail: [Thi; Tlo] of the last rows in slot 2
+              tma_load_4d(S.stage[s][2], &mTh, &S.full[s], kx, nfull, b, g);
+              tma_load_4d(S.stage[s][2] + ftail * 128, &mTl, &S.full[s], kx, nfull, b, g);
+            }
+            continue;
+          }
           tma_load_4d(S.stage[s][2], &mBh, &S.full[s], kx, n0, b, g);
           tma_load_4d(S.stage[s][3], &mBl, &S.full[s], kx, n0, b, g);
         }
@@ -258,6 +267,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int TB = tailTB ? tailTB : 128;
       const u32 idesc = u8ops ? idesc_u8(128, 2 * TB) : idesc_i8(128, 2 * TB);
       const u32 idesc128 = u8ops ? idesc_u8(128, TB) : idesc_i8(128, TB);
+      const int FT = ftail ? ftail : 16;          // fused tail of the diagonal tiles: TMEM columns 384 ..
+      const u32 idescF = u8ops ? idesc_u8(128, 2 * FT) : idesc_i8(128, 2 * FT);
+      const u32 idescF1 = u8ops ? idesc_u8(128, FT) : idesc_i8(128, FT);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
         bool diag = false;
@@ -284,6 +296,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           const u32 bh = diag ? ah : smem_u32(S.stage[s][2]);
           // descriptors of K step ks: start address + 32 ks bytes = field + 2 ks (no carry out of the field)
           const u64 dah = sdesc_sw128(ah), dal = sdesc_sw128(al), dbh = sdesc_sw128(bh);
+          const bool dt = diag && ftail;
+          const u32 th = smem_u32(S.stage[s][2]);
+          const u64 dth = sdesc_sw128(th);
           auto step = [&](int ks) {
             const u64 bd = dbh + 2 * ks;
             if ((kb | ks) == 0) {
@@ -293,6 +308,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             } else {
               mma_i8(tmem + 0, dah + 2 * ks, bd, idesc, 1u);
               mma_i8(tmem + TB, dal + 2 * ks, bd, idesc, 1u);
+            }
+            if (dt) {                             // A [Thi; Tlo]^T, N = 2 FT, at columns 384 ..
+              const u64 td = dth + 2 * ks;
+              if ((kb | ks) == 0) {
+                mma_i8(tmem + 384, dah, td, idescF, 0u);
+                mma_i8(tmem + 384 + 2 * FT, dal, sdesc_sw128(th + FT * 128), idescF1, 0u);
+                mma_i8(tmem + 384 + FT, dal, td, idescF1, 1u);
+              } else {
+                mma_i8(tmem + 384, dah + 2 * ks, td, idescF, 1u);
+                mma_i8(tmem + 384 + FT, dal + 2 * ks, td, idescF, 1u);
+              }
             }
           };
           const i64 krem = KC - kb * 128;                                 // K steps past KC are zero
@@ -373,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int gg = g0 + gofs + g;
       const int m = S.tmod[g], c14 = S.tc14[g];
       const float minv = S.tminv[g];
-      const i64 i = t * 128 + q * 32 + lane;                        // A row (output column)
+      const i64 i = (t + tfirst) * 128 + q * 32 + lane;             // A row (output column)
       const int tail = (int)(N - nfull);
       int16_t* colp = acc + ((i64)gg * nb * M + (i64)b * M + nfull) * ldc + i;
       int old[16];
@@ -473,6 +499,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int rrow = q * 32 + lane;
       const i64 i = m0 + rrow;                                      // output row within the block
       int16_t* rowp = acc + (rowbase + rrow) * ldc;
+      // fused syrk tail of a diagonal tile: entry (A row i, tail row j) = Q[nfull + j][i], stored transposed
+      // (a warp's lanes are consecutive i: coalesced); this thread takes tail rows 16 ch .. 16 ch + 15
+      const bool dt = ftail && tm == tn;
+      const int tail = (int)(N - nfull);
+      int16_t* colp = acc + ((i64)gg * nb * M + (i64)b * M + nfull) * ldc + i;
+      int told[16];
+#pragma unroll
+      for (int u = 0; u < 16; u++) told[u] = (dt && !fresh && 16 * ch + u < tail) ? (int)colp[(i64)(16 * ch + u) * ldc] : 0;
       u32 olds[2][16];                                              // old residues of this row, in pairs
 #pragma unroll
       for (int c = 0; c < 2; c++)
@@ -529,6 +563,26 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool fail = epi_sync_or(!ok_me);             // uniform over the epilogue warps
       if (fail) break;
       tc_fence_after();
+      if (dt) {                                          // read before epi_compute releases TMEM
+        u32 hh[16], hx[16], ll[16];
+        const u32 base = tmem + ((u32)(q * 32) << 16) + 384 + 16 * ch;
+        tmem_ld16(base, hh);
+        tmem_ld16(base + ftail, hx);
+        tmem_ld16(base + 2 * ftail, ll);
+        tmem_ld_wait();
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int j = 16 * ch + u;
+          int a = (int)hh[u], x = (int)hx[u];
+          int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+          int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+          int v = ra * c14 + rx * 128 + (int)ll[u] + told[u];
+          int r = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+          r += (r < 0) ? m : 0;
+          r -= (r >= m) ? m : 0;
+          if (j < tail) colp[(i64)j * ldc] = (int16_t)r;
+        }
+      }
       u32 outp[2][16];
       epi_compute(tmem, q, ch, lane, m, c14, minv, olds, outp, &S.tmem_empty);
       if (vec) {
@@ -648,9 +702,10 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   });
   if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
-  // syrk whose last row block has at most 32 rows: full lower tiles over the first nfull rows, then one
-  // item per A row block against those rows (N = 64 products, stored transposed) -- not 128 x 128 tiles
-  // that are mostly padding
+  // syrk whose last row block has at most 32 rows: full lower tiles over the first nfull rows, the tail rows
+  // against each full row block inside that row block's diagonal item (its operand slices are in shared
+  // memory already; N = 64 products at TMEM columns 384.., stored transposed), and the tail rows against
+  // themselves in one more small launch -- not 128 x 128 tiles that are mostly padding
   const int nfull = (int)(N / 128) * 128, tailTB = (mode == 1 && N > 128 && N - nfull > 0 && N - nfull <= 32) ? 32 : 0;
   if (tailTB) ntm = nfull / 128;
   i64 tiles = mode == 0 ? (i64)ntm * ntn : (i64)ntm * (ntm + 1) / 2;
@@ -668,12 +723,15 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
     const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
     for (int part = 0; part < (tailTB ? 2 : 1); part++) {
       const int tb = part ? tailTB : 0;
-      const i64 ptiles = part ? nfull / 128 + 1 : tiles;
+      // the diagonal items of the full tiles also take the tail rows against their row block (fused tail);
+      // the tail launch is left with the last row block against the tail rows (the corner)
+      const int ftail = (tailTB && !part) ? tailTB : 0, tfirst = part ? nfull / 128 : 0;
+      const i64 ptiles = part ? 1 : tiles;
       const i64 nitems = ptiles * (pack > 1 ? 1 : nb) * Gl;
       if (nitems == 0) continue;
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
       rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
+          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
           KC, mode, ntn, ptiles, nitems, fresh, pack, sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;

@@ -216,6 +216,38 @@ def test_rns_gemm_random(sb, L, nb, M, N, K, syrk):
         assert np.array_equal(got[:, sl], ref)
 
 
+@pytest.mark.parametrize("nb,M,K,fresh,unsigned", [(1, 129, 16, False, False), (1, 274, 1008, True, True),
+                                                   (2, 150, 48, True, False), (3, 288, 80, False, True),
+                                                   (1, 400, 32, False, False), (2, 257, 400, True, True)])
+def test_rns_gemm_syrk_fused_tail(sb, nb, M, K, fresh, unsigned):
+    """syrk whose last row block has 1..32 rows: the tail rows against each full row block come out of the
+    diagonal items (fused), the tail against itself out of the corner launch; fresh (no old residues read)
+    and unsigned digits (mode bits 2 and 4) included"""
+    from sdpvibe_b200.mpmat import ctx
+    L = 26
+    rng = np.random.default_rng(M + K + nb)
+    T = O.tables(L)
+    R = ctx(L)
+    m = T.m32.astype(np.int64)[:, None, None]
+    if unsigned:
+        r = rng.integers(0, 1 << 30, size=(T.n, nb * M, K)) % m
+        Ah, Al = (r >> 7).astype(np.uint8), (r & 127).astype(np.uint8)
+    else:
+        Ah, Al = _rand_residues(rng, T, T.n, nb * M, K)
+    acc0 = (rng.integers(0, 1 << 30, size=(T.n, nb * M, M)) % m).astype(np.int16)
+    acc = cu(acc0).clone()
+    R.accumulate(cu(Ah), cu(Al), cu(Ah), cu(Al), acc, 0, nb=nb, syrk=True, fresh=fresh, unsigned=unsigned)
+    got = np_(acc)
+    low = np.tril(np.ones((M, M), dtype=bool))
+    for b in range(nb):
+        sl = slice(b * M, (b + 1) * M)
+        base = np.zeros_like(acc0[:, sl]) if fresh else acc0[:, sl]
+        ref = O.accumulate(T, Ah[:, sl].astype(np.int64), Al[:, sl].astype(np.int64), Ah[:, sl].astype(np.int64),
+                           Al[:, sl].astype(np.int64), base, 0, lower=True)
+        assert np.array_equal(got[:, sl][:, low], ref[:, low])
+        assert np.array_equal(got[:, sl][:, ~low], acc0[:, sl][:, ~low])     # upper triangle untouched
+
+
 # ------------------------------------------------------------------ CRT (c)
 @pytest.mark.parametrize("name", golden_names("crt_block_"))
 def test_crt_block_golden(sb, name):
