@@ -45,6 +45,8 @@ struct CtxDev {
   int32_t* inv;      // (n) (M/m)^-1 mod m
   int32_t* md;       // (Epad) signed base-256 digits of M, zero padded
   uint8_t* tab;      // decomposition tables as swizzled SMEM images: [group][lo|hi][kt][128 rows][128 B]
+  uint8_t* tabu;     // the same layout with unsigned digits of the canonical 256^j mod m (hi = t >> 7,
+                     // lo = t & 127) and column 4L = (-2^(32L)) mod m against the sign byte
   uint8_t* ct;       // CRT digit table as swizzled SMEM images: [chunk][ktc][128 rows][128 B]
   int ktc;           // 128-byte K tiles of the CRT product (ceil(n/128))
 };

@@ -129,6 +129,13 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
   std::vector<float> vminv(n);
   int ngroups = d.npad / 128;
   std::vector<uint8_t> tab((size_t)ngroups * 2 * d.kt * 128 * 128, 0);
+  std::vector<uint8_t> tabu(tab.size(), 0);
+  auto put_u = [&](int grp, int row, int j, long t) {   // canonical t in [0, m) as unsigned digits
+    int kt = j / 128, col = j % 128;
+    u32 off = sw128_off(row, col / 16) + (col % 16);
+    tabu[(((size_t)grp * 2 + 0) * d.kt + kt) * 128 * 128 + off] = (uint8_t)(t & 127);
+    tabu[(((size_t)grp * 2 + 1) * d.kt + kt) * 128 * 128 + off] = (uint8_t)(t >> 7);
+  };
   for (int g = 0; g < n; g++) {
     long m = mods[g];
     vm[g] = (int32_t)m;
@@ -138,6 +145,7 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
     int grp = g / 128, row = g % 128;
     for (int j = 0; j < NB; j++) {
       long t = powmod(256, j, m);
+      put_u(grp, row, j, t);
       if (t > m / 2) t -= m;  // centred
       tsum += t;
       long lo = ((t + 64) % 128 + 128) % 128 - 64;
@@ -151,6 +159,7 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
     }
     long c1 = ((128 * tsum) % m + m) % m;
     long c2 = powmod(2, 32L * L, m);
+    put_u(grp, row, NB, (m - c2) % m);        // unsigned table: the sign byte subtracts 2^(32L)
     vc1[g] = (int32_t)c1;
     vc1m2[g] = (int32_t)(c1 - c2);
     // Column NB multiplies a constant byte 1 (adds C1), column NB+1 the sign byte (subtracts C2):
@@ -195,6 +204,7 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
   if (!st) st = upload(&d.inv, vinv);
   if (!st) st = upload(&d.md, vmd);
   if (!st) st = upload(&d.tab, tab);
+  if (!st) st = upload(&d.tabu, tabu);
   if (!st) st = upload(&d.ct, ct);
   c->mods_host = new int32_t[n];
   memcpy(c->mods_host, vm.data(), sizeof(int32_t) * n);
@@ -209,7 +219,7 @@ extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
 extern "C" int sdpv_ctx_destroy(sdpv_ctx* c) {
   if (!c) return SDPV_OK;
   sdpv::CtxDev& d = c->d;
-  void* ptrs[] = {d.mods, d.minv, d.c14, d.c1, d.c1m2, d.inv, d.md, d.tab, d.ct};
+  void* ptrs[] = {d.mods, d.minv, d.c14, d.c1, d.c1m2, d.inv, d.md, d.tab, d.tabu, d.ct};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete[] c->mods_host;

@@ -11,6 +11,12 @@
 // epilogue each thread reduces one modulus for 32 consecutive entries and stores 32 contiguous
 // residue bytes per plane.  The next tile's limbs are loaded into registers while the current tile
 // is reduced, and several CTAs share each SM so their phases overlap.
+//
+// The warp-specialised kernel (L <= 63) uses unsigned operands instead: the limb bytes u_j as they are
+// and a sign byte against the canonical digits of 256^j mod m (hi = t >> 7, lo = t & 127) and of
+// (-2^(32L)) mod m, as u8 x u8 products.  v = 128 D_hi + D_lo is then congruent to x, non-negative and
+// below 2^31, so the canonical residue comes from an exact Barrett quotient floor(v ceil(2^46/m) / 2^46)
+// with no float estimate and no correction step.
 #include <cstdlib>
 #include <cstring>
 
@@ -337,8 +343,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
 #pragma unroll
         for (int t = 0; t < 4; t++) {
           int l = 4 * c + t;
-          if (l < L) w[t] = raw[l * WS_TILE + ent] ^ 0x80808080u;
-          else if (l == L) w[t] = 1u | ((raw[(L - 1) * WS_TILE + ent] >> 31) << 8);
+          if (l < L) w[t] = raw[l * WS_TILE + ent];                    // the limb's bytes, unsigned
+          else if (l == L) w[t] = raw[(L - 1) * WS_TILE + ent] >> 31;  // sign byte (column 4L)
           else w[t] = 0u;
         }
         *reinterpret_cast<uint4*>(&S.xb[slot][c >> 3][sw128_off(ent, c & 7)]) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   } else if (warp == 4) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const u32 idesc = idesc_i8(128, WS_TILE);
+      const u32 idesc = idesc_u8(128, WS_TILE);
       if (!mbar_wait(&S.bar_tab, 0, err)) S.abort = 1;
       int issued = 0;
       for (int it = 0; it < niter && !S.abort; it++) {
@@ -381,13 +387,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     const int row = quarter * 32 + lane;
     const int g = grp * 128 + row;
     const bool gvalid = (g >= g0) && (g < g0 + G) && (g < n);
-    int m = 1;
-    float minv = 1.f;
-    if (gvalid) {
-      m = mods[g];
-      minv = minvs[g];
-    }
+    int m = 32639;                                       // rows past the moduli: any 15-bit modulus
+    if (gvalid) m = mods[g];
     const int hm = m >> 1;
+    const u32 bm = (u32)(((1ull << 46) + (u64)m - 1) / (u64)m);   // ceil(2^46 / m) < 2^32 (m > 2^14)
     int8_t* outh = Rhi + (i64)(g - g0) * pstride;
     int8_t* outl = Rlo + (i64)(g - g0) * pstride;
     const bool elected = (tid == WS_LOADERS + 32);       // first reducer thread issues the bulk stores
@@ -413,12 +416,32 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         u32 ph[8], pl[8];
 #pragma unroll
         for (int j = 0; j < 32; j += 4) {
-          int hb[4], lb[4];
+          u32 r[4];
 #pragma unroll
-          for (int u = 0; u < 4; u++)
-            residue_digits<U8>(128 * (int)hi[j + u] + (int)lo[j + u], m, hm, minv, hb[u], lb[u]);
-          ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
-          pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
+          for (int u = 0; u < 4; u++) {
+            // v = 128 D_hi + D_lo: a sum of unsigned digit products, 0 <= v < 2^31, v = entry (mod m);
+            // floor(v / m) = floor(v ceil(2^46 / m) / 2^46) exactly for v < 2^31, m < 2^15
+            const u32 v = 128u * hi[j + u] + lo[j + u];
+            const u32 q = __umulhi(v, bm) >> 14;
+            r[u] = v - q * (u32)m;                                   // canonical residue in [0, m)
+          }
+          if (U8) {
+            // pairs of 15-bit residues in 16-bit halves; hi = r >> 7 is byte 0 / 2 of (pair >> 7), lo byte 0 / 2
+            // of the pair masked to 7 bits
+            const u32 p01 = r[0] + (r[1] << 16), p23 = r[2] + (r[3] << 16);
+            ph[j >> 2] = __byte_perm(p01 >> 7, p23 >> 7, 0x6420);
+            pl[j >> 2] = __byte_perm(p01, p23, 0x6420) & 0x7F7F7F7Fu;
+          } else {
+            int hb[4], lb[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {                            // centred, split 128 hi + lo, lo in [-64, 64)
+              const int c = (int)r[u] - (((int)r[u] > hm) ? m : 0);
+              hb[u] = (c + 64) >> 7;
+              lb[u] = c - (hb[u] << 7);
+            }
+            ph[j >> 2] = __byte_perm(__byte_perm(hb[0], hb[1], 0x0040), __byte_perm(hb[2], hb[3], 0x0040), 0x5410);
+            pl[j >> 2] = __byte_perm(__byte_perm(lb[0], lb[1], 0x0040), __byte_perm(lb[2], lb[3], 0x0040), 0x5410);
+          }
         }
         if (use_tma) {
           // row = modulus within the group, 16-byte chunks col/16 and col/16 + 1 (128-byte swizzle)
@@ -552,7 +575,7 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
   residues_ws_kernel<KT, RAW, STG, U8><<<grid, WS_THREADS, smem, st>>>(mh, ml, use_tma, X, d.L, rows, ld, k0, kc, kp, g0,
-                                                                    G, grp0, d.tab, d.mods, d.minv, d.n, Rhi, Rlo,
+                                                                    G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo,
                                                                     ps, sdpv::device_error_word());
   return sdpv::launch_status();
 }
