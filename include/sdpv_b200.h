@@ -90,12 +90,14 @@ int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
  * Results never depend on them.  SDPV_TUNE_CRT_CTAS: CRT CTAs per SM (1..4, default 3);
  * SDPV_TUNE_NARROW_MAX: residue-GEMM narrow items when one side has at most this many rows (0 = never,
  * else a multiple of 16 up to 64; default 64); SDPV_TUNE_PACK_MAX: small blocks packed several to a tile
- * when both sides have at most this many rows (0 = never, multiple of 16 up to 64; default 64).
+ * when both sides have at most this many rows (0 = never, multiple of 16 up to 64; default 64);
+ * SDPV_TUNE_RES_WARPS: reducer warps of the decomposition kernel (8 or 16; default 8).
  * No reference counterpart (the reference's launch shapes are fixed). */
 #define SDPV_TUNE_CRT_CTAS 0
 #define SDPV_TUNE_NARROW_MAX 1
 #define SDPV_TUNE_PACK_MAX 2
-#define SDPV_TUNE_COUNT 3
+#define SDPV_TUNE_RES_WARPS 3
+#define SDPV_TUNE_COUNT 4
 int sdpv_tune_set(int knob, int value);
 int sdpv_tune_get(int knob, int* value);
 /* ---------------------------------------------------------------- binary SDP records (El::BigFloat over GMP limbs)

@@ -12,6 +12,8 @@ Knobs and their shapes:
               (90 x 32 x 1000, K 32; 30 x 64 x 1000, K 64; 131 x 96 x 8, K 64)
   pack_max    block size limit for packing small blocks into one GEMM tile: the Cholesky recursion of
               the c2 buckets (106 x 32 x 32, K 32; 131 x 64 x 32, K 64; 98 x 16 x 16, K 16)
+  res_warps   reducer warps of the decomposition kernel: the Gram chunk's residues (274 x 7000 entries,
+              L + 1 = 27 limbs, unsigned digits) and the solver's (1000 x 1000, L = 26, API digits)
 
 The prime set and the digit split of the residues are the reference's (they define the API's residue and
 CRT formats), so they are not tuned.
@@ -27,7 +29,8 @@ from . import _lib
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning_b200.json")
-KNOBS = {"crt_ctas": (0, [1, 2, 3, 4]), "narrow_max": (1, [0, 32, 48, 64]), "pack_max": (2, [0, 32, 64])}
+KNOBS = {"crt_ctas": (0, [1, 2, 3, 4]), "narrow_max": (1, [0, 32, 48, 64]), "pack_max": (2, [0, 32, 64]),
+         "res_warps": (3, [8, 16])}
 
 
 def set_knob(name, value):
@@ -84,6 +87,13 @@ def _gemm_case(R, nb, M, N, K, rng):
     return lambda: R.accumulate(Ah, Al, Bh, Bl, acc, nb=nb, fresh=True)
 
 
+def _res_case(L, rows, K, unsigned):
+    from .mpmat import ctx
+    R = ctx(L)
+    X = torch.randint(-(1 << 31), (1 << 31) - 1, (L, rows, K), dtype=torch.int32, device="cuda")
+    return lambda: R.residues(X, 0, K, spread=True, unsigned=unsigned)
+
+
 def tune(reps=5, L=26):
     from .mpmat import ctx
     R = ctx(L)
@@ -99,6 +109,7 @@ def tune(reps=5, L=26):
                        _gemm_case(R, 131, 96, 8, 64, rng)],
         "pack_max": [_gemm_case(R, 106, 32, 32, 32, rng), _gemm_case(R, 131, 64, 32, 64, rng),
                      _gemm_case(R, 98, 16, 16, 16, rng)],
+        "res_warps": [_res_case(27, 274, 7000, True), _res_case(26, 1000, 1000, False)],
     }
     knobs, timings = {}, {}
     for name, (_, values) in KNOBS.items():

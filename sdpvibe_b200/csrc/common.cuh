@@ -129,6 +129,11 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, u32 src_by
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                : "memory");
 }
+// 16-byte copy (both addresses 16-byte aligned); the bytes past src_bytes are written as zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, u32 src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {

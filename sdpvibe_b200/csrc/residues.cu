@@ -233,8 +233,10 @@ __global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
 //              digit split and 32-byte stores.
 // mbarriers: xb_full (128 loader arrivals), xb_empty (MMA commit), tm_full (MMA commit),
 // tm_empty (256 reducer arrivals).  Every wait is bounded; a timeout aborts all roles.
-constexpr int WS_TILE = 128, WS_LOADERS = 128, WS_REDUCERS = 256;
-constexpr int WS_THREADS = WS_LOADERS + 32 + WS_REDUCERS;
+constexpr int WS_TILE = 128, WS_LOADERS = 128;
+// RW reducer warps (8 or 16): RW / 4 per TMEM lane quarter, 128 / (RW / 4) columns each
+template <int RW>
+constexpr int ws_threads() { return WS_LOADERS + 32 + 32 * RW; }
 
 template <int KT, int RAW, int STG>
 struct WsSmem {
@@ -265,10 +267,10 @@ __device__ __forceinline__ bool named_sync_or(int id, int nthreads, bool pred) {
   return out != 0;
 }
 
-template <int KT, int RAW, int STG, bool U8>
-__global__ void __launch_bounds__(WS_THREADS, 1)
+template <int KT, int RAW, int STG, bool U8, int RW>
+__global__ void __launch_bounds__(ws_threads<RW>(), 1)
     residues_ws_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-                       int use_tma, const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp,
+                       int use_tma, int vec, const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp,
                        int g0, int G,
                        int group0, const uint8_t* __restrict__ tab, const int32_t* __restrict__ mods,
                        const float* __restrict__ minvs, int n, int8_t* __restrict__ Rhi, int8_t* __restrict__ Rlo, i64 pstride,
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       mbar_init(&S.xb_full[b], WS_LOADERS);
       mbar_init(&S.xb_empty[b], 1);
       mbar_init(&S.tm_full[b], 1);
-      mbar_init(&S.tm_empty[b], WS_REDUCERS);
+      mbar_init(&S.tm_empty[b], 32 * RW);
     }
     S.abort = 0;
     mbar_fence_init();
@@ -309,12 +311,25 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     auto issue = [&](int it) {
       if (it < niter) {
         i64 tile = blockIdx.x + (i64)it * gridDim.x;
-        i64 e = tile * WS_TILE + ent;
-        i64 i = e / kp, k = e - (e / kp) * kp;
-        bool ok = (e < nent) && (k < kc);
-        const int32_t* base = X + (ok ? i * ld + k0 + k : 0);
-        u32* dst = &S.raw[it % RAW][0][ent];
-        for (int l = 0; l < L; l++) cp_async4(dst + l * WS_TILE, base + (ok ? (i64)l * plane : 0), ok ? 4u : 0u);
+        if (vec) {
+          // 16-byte copies: thread = (4-entry group ent & 31, limbs ent / 32 + 4 s); a group never straddles
+          // an entry row (kp is a multiple of 16) and its words past kc are zero filled
+          const int gi = ent & 31;
+          const i64 e = tile * WS_TILE + 4 * gi;
+          const i64 i = e / kp, k = e - i * kp;
+          const bool ok = (e < nent) && (k < kc);
+          const u32 nb = ok ? (u32)(4 * (kc - k < 4 ? kc - k : 4)) : 0u;
+          const int32_t* base = X + (ok ? i * ld + k0 + k : 0);
+          for (int l = ent >> 5; l < L; l += 4)
+            cp_async16(&S.raw[it % RAW][l][4 * gi], base + (ok ? (i64)l * plane : 0), nb);
+        } else {
+          i64 e = tile * WS_TILE + ent;
+          i64 i = e / kp, k = e - (e / kp) * kp;
+          bool ok = (e < nent) && (k < kc);
+          const int32_t* base = X + (ok ? i * ld + k0 + k : 0);
+          u32* dst = &S.raw[it % RAW][0][ent];
+          for (int l = 0; l < L; l++) cp_async4(dst + l * WS_TILE, base + (ok ? (i64)l * plane : 0), ok ? 4u : 0u);
+        }
       }
       cp_async_commit();
     };
@@ -337,18 +352,17 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         break;
       }
       const u32* raw = &S.raw[it % RAW][0][0];
+      u32 w[4 * kMaxChunks];                         // all words first, then the stores (no load-store chain)
 #pragma unroll
-      for (int c = 0; c < kMaxChunks; c++) {
-        u32 w[4];
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-          int l = 4 * c + t;
-          if (l < L) w[t] = raw[l * WS_TILE + ent];                    // the limb's bytes, unsigned
-          else if (l == L) w[t] = raw[(L - 1) * WS_TILE + ent] >> 31;  // sign byte (column 4L)
-          else w[t] = 0u;
-        }
-        *reinterpret_cast<uint4*>(&S.xb[slot][c >> 3][sw128_off(ent, c & 7)]) = make_uint4(w[0], w[1], w[2], w[3]);
+      for (int l = 0; l < 4 * kMaxChunks; l++) {
+        if (l < L) w[l] = raw[l * WS_TILE + ent];                       // the limb's bytes, unsigned
+        else if (l == L) w[l] = raw[(L - 1) * WS_TILE + ent] >> 31;     // sign byte (column 4L)
+        else w[l] = 0u;
       }
+#pragma unroll
+      for (int c = 0; c < kMaxChunks; c++)
+        *reinterpret_cast<uint4*>(&S.xb[slot][c >> 3][sw128_off(ent, c & 7)]) =
+            make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
       fence_proxy_async_smem();
       mbar_arrive(&S.xb_full[slot]);
     }
@@ -383,7 +397,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     }
   } else {
     // ------------------------------------------------ reducers
-    const int quarter = warp & 3, half = (warp - 5) >> 2;
+    constexpr int WS_REDUCERS = 32 * RW, CHUNKS = 16 / RW;        // 32-column chunks per warp and tile
+    const int quarter = warp & 3, part = (warp - 5) >> 2;
     const int row = quarter * 32 + lane;
     const int g = grp * 128 + row;
     const bool gvalid = (g >= g0) && (g < g0 + G) && (g < n);
@@ -406,8 +421,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       tc_fence_after();
       const i64 tile = blockIdx.x + (i64)it * gridDim.x;
 #pragma unroll 1
-      for (int c = 0; c < 2; c++) {
-        const int col = half * 64 + c * 32;
+      for (int c = 0; c < CHUNKS; c++) {
+        const int col = part * (32 * CHUNKS) + c * 32;
         u32 lo[32], hi[32];
         const u32 taddr = tmem + ((u32)(quarter * 32) << 16) + (u32)b * 256 + col;
         tmem_ld32(taddr, lo);
@@ -545,7 +560,7 @@ bool res_store_map(CUtensorMap* map, void* base, i64 nent, i64 G, i64 ps) {
          CUDA_SUCCESS;
 }
 
-template <int KT, int RAW, int STG, bool U8>
+template <int KT, int RAW, int STG, bool U8, int RW>
 int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
               int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   const sdpv::CtxDev& d = c->d;
@@ -555,7 +570,7 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG, U8>,
+    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG, U8, RW>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return sdpv::set_cuda_error(e);
     attr_set[dev & 63] = true;
@@ -569,14 +584,16 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
     memset(&mh, 0, sizeof(mh));
     memset(&ml, 0, sizeof(ml));
   }
+  // 16-byte limb copies when every 4-entry group of a row starts 16-byte aligned
+  const int vec = (ld % 4 == 0) && (k0 % 4 == 0) && ((((uintptr_t)X) & 15) == 0);
   int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
   i64 ntiles = (nent + WS_TILE - 1) / WS_TILE;
   i64 gx = num_sms();
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
-  residues_ws_kernel<KT, RAW, STG, U8><<<grid, WS_THREADS, smem, st>>>(mh, ml, use_tma, X, d.L, rows, ld, k0, kc, kp, g0,
-                                                                    G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo,
-                                                                    ps, sdpv::device_error_word());
+  residues_ws_kernel<KT, RAW, STG, U8, RW><<<grid, ws_threads<RW>(), smem, st>>>(
+      mh, ml, use_tma, vec, X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo, ps,
+      sdpv::device_error_word());
   return sdpv::launch_status();
 }
 
@@ -590,8 +607,13 @@ int launch_kt(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
     if (v && atoi(v) == 64) return 64;
     return 0;
   }();
-  if (tile == 0 && KT == 1) return launch_ws<1, 3, 2, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
-  if (tile == 0 && KT == 2) return launch_ws<2, 2, 1, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  const bool rw16 = sdpv::tune(SDPV_TUNE_RES_WARPS) == 16;
+  if (tile == 0 && KT == 1)
+    return rw16 ? launch_ws<1, 3, 2, U8, 16>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st)
+                : launch_ws<1, 3, 2, U8, 8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  if (tile == 0 && KT == 2)
+    return rw16 ? launch_ws<2, 2, 1, U8, 16>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st)
+                : launch_ws<2, 2, 1, U8, 8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
   if (tile == 128) return launch_residues<KT, 128, 256, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
   return launch_residues<KT, 64, 128, U8>(c, X, rows, ld, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
 }

@@ -6,10 +6,11 @@
 #include "common.cuh"
 
 namespace {
-// defaults: CRT CTAs per SM, narrow-item limit of the short side, block-packing limit
-std::atomic<int> g_knob[SDPV_TUNE_COUNT] = {{3}, {64}, {64}};
-constexpr int kLo[SDPV_TUNE_COUNT] = {1, 0, 0};
-constexpr int kHi[SDPV_TUNE_COUNT] = {4, 64, 64};
+// defaults: CRT CTAs per SM, narrow-item limit of the short side, block-packing limit, decomposition
+// reducer warps
+std::atomic<int> g_knob[SDPV_TUNE_COUNT] = {{3}, {64}, {64}, {8}};
+constexpr int kLo[SDPV_TUNE_COUNT] = {1, 0, 0, 8};
+constexpr int kHi[SDPV_TUNE_COUNT] = {4, 64, 64, 16};
 }  // namespace
 
 namespace sdpv {
@@ -19,6 +20,7 @@ int tune(int knob) { return g_knob[knob].load(std::memory_order_relaxed); }
 extern "C" int sdpv_tune_set(int knob, int value) {
   if (knob < 0 || knob >= SDPV_TUNE_COUNT || value < kLo[knob] || value > kHi[knob]) return SDPV_EINVAL;
   if ((knob == SDPV_TUNE_NARROW_MAX || knob == SDPV_TUNE_PACK_MAX) && value % 16) return SDPV_EINVAL;
+  if (knob == SDPV_TUNE_RES_WARPS && value % 8) return SDPV_EINVAL;
   g_knob[knob].store(value, std::memory_order_relaxed);
   return SDPV_OK;
 }

@@ -41,7 +41,8 @@ def test_tuning_knobs_validated():
     from sdpvibe_b200 import _lib
     h = _lib.lib()
     v = ctypes.c_int(0)
-    for knob, good, bad in ((0, (1, 4), (0, 5)), (1, (0, 32, 64), (8, 80)), (2, (0, 64), (-16, 128))):
+    for knob, good, bad in ((0, (1, 4), (0, 5)), (1, (0, 32, 64), (8, 80)), (2, (0, 64), (-16, 128)),
+                            (3, (8, 16), (0, 12, 24))):
         assert h.sdpv_tune_get(knob, ctypes.byref(v)) == 0
         old = v.value
         for g in good:

@@ -713,6 +713,36 @@ def test_tuning_knobs_do_not_change_results(sb):
             set_knob(k, v)
 
 
+@pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (50, 9, 130), (26, 3, 4097)])
+def test_decomposition_reducer_warps(sb, L, rows, K):
+    """8 and 16 reducer warps of the decomposition kernel give the oracle's residues (API digits) and its
+    canonical residues (unsigned digits)"""
+    from sdpvibe_b200.autotune import set_knob, get_knob
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(L + rows + K)
+    T = O.tables(L)
+    R = ctx(L)
+    X = rand_limbs(rng, L, rows * K).reshape(L, rows, K)
+    X[:, 0, :5] = 0
+    X[-1, 0, 5] = -(1 << 31)
+    X[:, 0, 6] = -1
+    rh, rl = O.residues(T, X, 1, K - 1)
+    m = T.m32.astype(np.int64)[:, None, None]
+    rc = (128 * rh.astype(np.int64) + rl) % m
+    saved = get_knob("res_warps")
+    try:
+        for w in (8, 16):
+            set_knob("res_warps", w)
+            hi, lo = R.residues(cu(X), 1, K - 1)
+            assert np.array_equal(np_(hi), rh) and np.array_equal(np_(lo), rl), w
+            uh, ul = R.residues(cu(X), 1, K - 1, spread=True, unsigned=True)
+            kk = rc.shape[2]
+            assert np.array_equal(np_(uh)[:, :, :kk], (rc >> 7).astype(np.uint8)), w
+            assert np.array_equal(np_(ul)[:, :, :kk], (rc & 127).astype(np.uint8)), w
+    finally:
+        set_knob("res_warps", saved)
+
+
 
 @pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (24, 37, 700), (26, 5, 4096)])
 def test_unsigned_digit_residues_and_gemm(sb, L, rows, K):
