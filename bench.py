@@ -303,7 +303,8 @@ def run_b200(args, rank, world, local_rank):
         graph.replay()
     with ClockSampler(local_rank) as clk:
         ms = timed(graph.replay, args.steps)
-    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues_u8", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_crt_norm", "sdpv_align",
+                             "sdpv_align_rows", "sdpv_top_max"})
     ms_eager = timed(step, args.steps, tr)
     for _ in range(2):
         step_e2e()
@@ -312,7 +313,8 @@ def run_b200(args, rank, world, local_rank):
     t_step = ms / args.steps * 1e-3
     value = world * algorithmic_ops(R) / t_step / 1e12
     gemm_ms = tr.kernel_ms("sdpv_rns_gemm")
-    res_ms = tr.kernel_ms("sdpv_residues_u8")
+    res_kernel = "sdpv_residues_rows" if tr.kernel_ms("sdpv_residues_rows") else "sdpv_residues_u8"
+    res_ms = tr.kernel_ms(res_kernel)
     crt_ms = tr.kernel_ms("sdpv_crt_norm")
     hbm, bf16, src = load_peaks()
     if rank != 0:
@@ -321,7 +323,8 @@ def run_b200(args, rank, world, local_rank):
     peak = 2 * bf16
     ops_per_launch = algorithmic_ops(R) / NCHUNK
     achieved = ops_per_launch / (statistics.mean(gemm_ms) * 1e-3) / 1e12
-    # decomposition: limb bytes read (L+1 limbs after alignment) + residue bytes written, per launch
+    # decomposition: limb bytes read (L+1 limbs after alignment) + residue bytes written, per launch (the
+    # operand rows it reads are 128 bytes per entry, 4 (L+1) of them limb bytes)
     res_bytes = (R / NCHUNK) * NCOLS * (4 * (L + 1) + 2 * N_MOD)
     line = {
         "metric": METRIC, "value": value, "unit": "TOPS", "n_gpus": world, "steps": args.steps,
@@ -337,12 +340,12 @@ def run_b200(args, rank, world, local_rank):
                      "int8_cublaslt_measured_tops": int8_lib,
                      "launch_ms_mean": statistics.mean(gemm_ms), "launches": len(gemm_ms),
                      "ops_per_launch": ops_per_launch},
-        "roofline_decomposition": {"bound": "hbm", "kernel": "sdpv_residues_u8", "achieved":
+        "roofline_decomposition": {"bound": "hbm", "kernel": res_kernel, "achieved":
                                    res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                                    "frac": res_bytes / (statistics.mean(res_ms) * 1e-3) / 1e9 / hbm,
                                    "launch_ms_mean": statistics.mean(res_ms), "bytes_per_launch": res_bytes},
         "crt_ms": sum(crt_ms) / args.steps,
-        "kernel_ms_per_step": {k: sum(tr.kernel_ms(k)) / args.steps for k in sorted(tr.timed)},
+        "kernel_ms_per_step": {k: sum(tr.kernel_ms(k)) / args.steps for k in sorted(tr.timed) if tr.kernel_ms(k)},
         "e2e": {"value": world * algorithmic_ops(R) / (ms_e2e / args.steps * 1e-3) / 1e12, "unit": "TOPS",
                 "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "ms_per_step_eager": ms_eager / args.steps,
@@ -435,10 +438,10 @@ def run_cholsolve(args, rank, world, local_rank):
         return s.elapsed_time(e)
     for _ in range(max(args.warmup, 3)):
         step()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_rns_gemm",
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
              "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_rows")
     tr = _trace.Trace(timed=names)
     with ClockSampler(local_rank) as clk:
         ms = timed(step, args.steps, tr)
@@ -653,10 +656,10 @@ def solver_measurement(steps, warmup, local_rank, world=1):
             s.timer.marks.clear()
             tr.launches.clear()
             tr.events.clear()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_rns_gemm",
+    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
              "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_rows")
     tr = _trace.Trace(timed=names)              # graph replays are timed whole, one entry per graph key
     with ClockSampler(local_rank) as clk, tr:
         torch.cuda.synchronize()

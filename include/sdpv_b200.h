@@ -143,6 +143,13 @@ int sdpv_top_max(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t 
  * shift_round of mpf._align_rows (sdpvibe/mpf.py:390-398) and GramAcc.add (sdpvibe/mpf.py:572-576). */
 int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, const int64_t* target,
                int per_col, int transpose, int Lout, int32_t* out, void* stream);
+/* The transposed alignment written as operand rows for sdpv_residues_rows: entry (b, r, c) of m becomes row
+ * (b C + c) Rp + r of out (nb, C, Rp, rb) uint8, rb = 128 bytes for Lout <= 31, 256 for Lout <= 63: the Lout
+ * aligned limbs little endian, then a sign byte (1 when the result is negative) at byte 4 Lout, then zeros;
+ * rows R .. Rp - 1 of each column are zero rows.  Rp >= R, a multiple of 128.  Same rounding and overflow
+ * rule as sdpv_align.  No reference counterpart (an internal layout of GramAcc.add's aligned chunk). */
+int sdpv_align_rows(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
+                    const int64_t* target, int per_col, int Lout, int64_t Rp, uint8_t* out, void* stream);
 
 /* ---------------------------------------------------------------- residue decomposition (a)
  * Residues of X[:, :, k0:k0+kc] for moduli g0..g0+G of ctx: X (L, rows, ld) int32 limb planes;
@@ -157,6 +164,12 @@ int sdpv_residues(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t l
  * counterpart (an internal format: one centring correction less per residue). */
 int sdpv_residues_u8(const sdpv_ctx* ctx, const int32_t* X, int64_t rows, int64_t ld, int64_t k0, int64_t kc, int g0,
                      int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride, void* stream);
+/* sdpv_residues_u8 of operand rows (sdpv_align_rows, ctx's L limbs): entry (i, k) of the result (i < nI,
+ * k < kc) is row i Rp + k0 + k of rows.  k0 and Rp multiples of 128, k0 + kc <= Rp, rows k0 + kc .. k0 + kp - 1
+ * zero (so when kc is not a multiple of 16, k0 + kc must be the column's row count); g0 a multiple of 128;
+ * ctx's L <= 63.  Rhi, Rlo (G, nI, kp) as sdpv_residues_u8. */
+int sdpv_residues_rows(const sdpv_ctx* ctx, const uint8_t* rows, int64_t nI, int64_t Rp, int64_t k0, int64_t kc,
+                       int g0, int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride, void* stream);
 
 /* ---------------------------------------------------------------- residue GEMM (b) and Gram (d)
  * For each of the G moduli g0..g0+G and each of nb blocks:

@@ -94,6 +94,14 @@ def _res_case(L, rows, K, unsigned):
     return lambda: R.residues(X, 0, K, spread=True, unsigned=unsigned)
 
 
+def _rows_case(L, nI, K):
+    from .mpmat import ctx
+    R = ctx(L)
+    Rp = -(-K // 128) * 128
+    Xr = torch.randint(0, 256, (nI, Rp, 128 if L <= 31 else 256), dtype=torch.uint8, device="cuda")
+    return lambda: R.residues_rows(Xr, nI, Rp, 0, K)
+
+
 def tune(reps=5, L=26):
     from .mpmat import ctx
     R = ctx(L)
@@ -109,7 +117,7 @@ def tune(reps=5, L=26):
                        _gemm_case(R, 131, 96, 8, 64, rng)],
         "pack_max": [_gemm_case(R, 106, 32, 32, 32, rng), _gemm_case(R, 131, 64, 32, 64, rng),
                      _gemm_case(R, 98, 16, 16, 16, rng)],
-        "res_warps": [_res_case(27, 274, 7000, True), _res_case(26, 1000, 1000, False)],
+        "res_warps": [_res_case(27, 274, 7000, True), _res_case(26, 1000, 1000, False), _rows_case(27, 274, 7000)],
     }
     knobs, timings = {}, {}
     for name, (_, values) in KNOBS.items():

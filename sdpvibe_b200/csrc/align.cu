@@ -204,6 +204,136 @@ __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __rest
   }
 }
 
+// shift_entry / shift_entry32 with the Lout output words in registers (o[k], k < Lout < RW; loops unrolled to
+// RW so that every index is static); returns the sign bit of the result.
+template <int RW, class Word>
+__device__ __forceinline__ u32 shift_entry_regs(Word word, int L, i64 s, int Lout, u32 (&o)[RW], unsigned* err) {
+  u32 prev = 0;
+  if (s >= 0) {
+    const u32 ext = ((int32_t)word(L - 1) < 0) ? 0xffffffffu : 0u;
+    const int si = (int)(s > 32 * (i64)(L + 1) ? 32 * (i64)(L + 1) : s);
+    const int q = si >> 5, r = si & 31;
+    auto w = [&](int i) -> u32 { return i < L ? (u32)word(i) : ext; };
+    u32 carry = si > 0 ? (w((si - 1) >> 5) >> ((si - 1) & 31)) & 1u : 0u;
+    u32 lo = w(q);
+#pragma unroll
+    for (int k = 0; k < RW; k++) {                  // words past Lout are computed and dropped
+      const u32 hi = w(q + k + 1);
+      const u32 f = __funnelshift_r(lo, hi, r);
+      const u32 v = f + carry;
+      carry = v < f ? 1u : 0u;
+      lo = hi;
+      if (k < Lout) {
+        o[k] = v;
+        prev = v;
+      } else if (k == Lout && v != ((prev >> 31) ? 0xffffffffu : 0u)) {
+        atomicOr(err, SDPV_ERRBIT_OVERFLOW);
+      }
+    }
+    return prev >> 31;
+  }
+  i64 q = s >> 5;
+  int r = (int)(s - 32 * q);
+  u64 ext = ((int32_t)word(L - 1) < 0) ? 0xffffffffull : 0ull;
+  auto w = [&](i64 i) -> u64 { return i < 0 ? 0ull : (i >= L ? ext : (u64)word((int)i)); };
+  i64 sb = s - 1, qb = sb >> 5;
+  int rb = (int)(sb - 32 * qb);
+  u64 carry = (sb >= 0) ? ((w(qb) >> rb) & 1ull) : 0ull;
+  u64 lo = w(q);
+#pragma unroll
+  for (int k = 0; k < RW; k++) {
+    u64 hi = w(q + k + 1);
+    u64 v = ((((hi << 32) | lo) >> r) & 0xffffffffull) + carry;
+    lo = hi;
+    carry = v >> 32;
+    v &= 0xffffffffull;
+    if (k < Lout) {
+      o[k] = (u32)v;
+      prev = (u32)v;
+    } else if (k == Lout && (u32)v != ((prev >> 31) ? 0xffffffffu : 0u)) {
+      atomicOr(err, SDPV_ERRBIT_OVERFLOW);
+    }
+  }
+  return prev >> 31;
+}
+
+// Byte offset of the per-warp output staging of align_rows_kernel in its dynamic shared memory.
+__host__ __device__ inline size_t align_rows_stage_offset(int L) {
+  return ((size_t)L * TR * (TC + 1) * 4 + 8 + TR * TC * 8 + 15) / 16 * 16;
+}
+
+// Transposed alignment into operand rows of 4 RW bytes per entry, entry (b, c, r) at row (b C + c) Rp + r:
+// the Lout limbs little endian, then the sign byte (1 for a negative entry) at byte 4 Lout, then zeros; rows
+// R .. Rp - 1 of every column are zero rows.  Staging as in align_t_kernel; each thread writes its rows with
+// 16-byte stores.
+template <int RW>
+__global__ void __launch_bounds__(kThreads) align_rows_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e,
+                                                              int L, i64 nb, i64 R, i64 C, i64 Rp,
+                                                              const i64* __restrict__ target, int per_col, int Lout,
+                                                              uint8_t* __restrict__ out, unsigned* err) {
+  extern __shared__ u32 sm[];                       // [L][TR][TC + 1] limbs, then [TR][TC] exponents
+  i64* se = reinterpret_cast<i64*>(sm + (size_t)L * TR * (TC + 1) + ((L * TR * (TC + 1)) & 1));
+  const i64 n = nb * R * C;
+  const i64 b = blockIdx.z;
+  const i64 r0 = (i64)blockIdx.x * TR, c0 = (i64)blockIdx.y * TC;
+  const int tid = threadIdx.x;
+  for (int pos = tid; pos < TR * TC; pos += kThreads) {
+    const int rr = pos / TC, cc = pos % TC;
+    const i64 r = r0 + rr, c = c0 + cc;
+    const bool in = r < R && c < C;
+    const int32_t* src = m + (in ? (b * R + r) * C + c : 0);
+    u32* dst = &sm[rr * (TC + 1) + cc];
+    const u32 nb4 = in ? 4u : 0u;
+    for (int l = 0; l < L; l++, src += n, dst += TR * (TC + 1)) cp_async4(dst, src, nb4);
+  }
+  cp_async_commit();
+  for (int t = tid; t < TR * TC; t += kThreads) {
+    int rr = t / TC, cc = t % TC;
+    i64 r = r0 + rr, c = c0 + cc;
+    se[t] = (r < R && c < C) ? e[(b * R + r) * C + c] : SDPV_EZ;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // each warp stages its 32 rows (two columns x 16 rows, 16-byte chunks swizzled by row) and copies them out
+  // 512 contiguous bytes per instruction
+  const int lane = tid & 31;
+  u32* stg = reinterpret_cast<u32*>(reinterpret_cast<uint8_t*>(sm) + align_rows_stage_offset(L)) + (tid >> 5) * 32 * RW;
+  for (int t0 = 0; t0 < TR * TC; t0 += kThreads) {
+    const int t = t0 + tid;
+    const int rr = t % TR, cc = t / TR;
+    const i64 r = r0 + rr, c = c0 + cc;
+    u32 o[RW];
+#pragma unroll
+    for (int k = 0; k < RW; k++) o[k] = 0u;
+    u32 sgn = 0;
+    if (r < R && c < C) {
+      i64 ev = se[rr * TC + cc];
+      i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
+      const u32* base = sm + rr * (TC + 1) + cc;
+      sgn = shift_entry_regs<RW>([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, o, err);
+    }
+    // word k: the limb (k < Lout), the sign byte (k == Lout), zero above (a select per static k)
+    auto wd = [&](int k) { return o[k] | (k == Lout ? sgn : 0u); };
+#pragma unroll
+    for (int q = 0; q < RW / 4; q++)
+      *reinterpret_cast<uint4*>(stg + lane * RW + 4 * (q ^ (lane & 7))) = make_uint4(wd(4 * q), wd(4 * q + 1),
+                                                                                     wd(4 * q + 2), wd(4 * q + 3));
+    __syncwarp();
+    const i64 cA = c0 + (t0 + (tid & ~31)) / TR;          // column of lanes 0-15 (lanes 16-31: the next one)
+#pragma unroll
+    for (int j = 0; j < RW / 4; j++) {
+      const int off = j * 512 + lane * 16;
+      const int sr = off / (4 * RW), q = (off % (4 * RW)) / 16;   // staged row, 16-byte chunk
+      const i64 cs = cA + (sr >= 16 ? 1 : 0);
+      if (cs < C) {
+        const uint4 v = *reinterpret_cast<const uint4*>(stg + sr * RW + 4 * (q ^ (sr & 7)));
+        *reinterpret_cast<uint4*>(out + ((b * C + cs) * Rp + r0 + (sr & 15)) * (i64)(4 * RW) + 16 * q) = v;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 inline unsigned blocks(i64 n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -231,6 +361,35 @@ extern "C" int sdpv_top_max(const int32_t* m, const int64_t* e, int L, int64_t n
     dim3 grid((unsigned)((C + 31) / 32), (unsigned)ry, (unsigned)nb);
     top_max_cols_kernel<<<grid, kThreads, 0, st>>>(m, e, L, nb, R, C, out);
   }
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_align_rows(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
+                               const int64_t* target, int per_col, int Lout, int64_t Rp, uint8_t* out, void* stream) {
+  if (L < 1 || L > 64 || Lout < 1 || Lout > 63 || nb < 0 || R < 0 || C < 0 || nb > 65535 || Rp < R || (Rp & 127))
+    return SDPV_EINVAL;
+  if (nb * Rp * C == 0) return SDPV_OK;
+  cudaStream_t st = sdpv::as_stream(stream);
+  unsigned* err = sdpv::device_error_word();
+  const int wide = Lout > 31;                          // 256-byte rows
+  const size_t stage = (size_t)(kThreads / 32) * 32 * (wide ? 256 : 128);
+  size_t smem = align_rows_stage_offset(L) + stage;
+  const size_t smax = align_rows_stage_offset(64) + (size_t)(kThreads / 32) * 32 * 256;
+  dim3 grid((unsigned)((Rp + TR - 1) / TR), (unsigned)((C + TC - 1) / TC), (unsigned)nb);
+  if (grid.y > 65535 || (Rp + TR - 1) / TR > 0x7fffffff) return SDPV_EINVAL;
+  static bool attr[2][64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[wide][dev & 63]) {
+    cudaError_t ce = cudaFuncSetAttribute(wide ? align_rows_kernel<64> : align_rows_kernel<32>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    if (ce != cudaSuccess) return sdpv::set_cuda_error(ce);
+    attr[wide][dev & 63] = true;
+  }
+  if (wide)
+    align_rows_kernel<64><<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, Rp, target, per_col, Lout, out, err);
+  else
+    align_rows_kernel<32><<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, Rp, target, per_col, Lout, out, err);
   return sdpv::launch_status();
 }
 

@@ -245,7 +245,7 @@ struct WsSmem {
   uint8_t xb[2][KT][WS_TILE * 128];
   uint8_t out[STG][2][kTileBytes];      // residue tiles (128 moduli x 128 entries, hi | lo), 128-byte swizzle
   u32 raw[RAW][32 * KT - 1][WS_TILE];
-  u64 bar_tab, xb_full[2], xb_empty[2], tm_full[2], tm_empty[2];
+  u64 bar_tab, xb_full[2], xb_empty[2], tm_full[2], tm_empty[2], raw_full[RAW];
   u32 tmem_slot;
   volatile int abort;
 };
@@ -267,9 +267,20 @@ __device__ __forceinline__ bool named_sync_or(int id, int nthreads, bool pred) {
   return out != 0;
 }
 
-template <int KT, int RAW, int STG, bool U8, int RW>
+// MODE 0: limb planes by per-thread cp.async, tiles of 128 consecutive entries (i kp + k enumeration), 2-D
+//   residue stores (or per-thread stores).
+// MODE 1: operand rows (4 L limb bytes, a sign byte, zeros; 128 KT bytes per entry) from sdpv_align_rows,
+//   entry (i, k) at row i Rp + k0 + k: thread 0 of the loaders streams each tile's rows straight into the
+//   K-major operand buffer with TMA (map_in); no transform.
+// MODE 2: limb planes by TMA: thread 0 loads each tile's L x 128 words with one 3-D copy (map_in over
+//   (kc, rows, L) from X + k0; words past kc zero filled) into the raw ring; the loaders transform as in
+//   MODE 0.
+// MODEs 1 and 2 use tiles (i, 128-entry block of k) (tpi blocks per i) and 3-D residue stores over
+// (kp, rows, G), clipped at kp.
+template <int KT, int RAW, int STG, bool U8, int RW, int MODE>
 __global__ void __launch_bounds__(ws_threads<RW>(), 1)
     residues_ws_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                       const __grid_constant__ CUtensorMap map_in, i64 Rp, i64 tpi,
                        int use_tma, int vec, const int32_t* __restrict__ X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp,
                        int g0, int G,
                        int group0, const uint8_t* __restrict__ tab, const int32_t* __restrict__ mods,
@@ -282,18 +293,20 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int grp = group0 + blockIdx.y;
   const i64 nent = rows * kp;
-  const i64 ntiles = (nent + WS_TILE - 1) / WS_TILE;
+  constexpr bool TILED = MODE != 0;
+  const i64 ntiles = TILED ? rows * tpi : (nent + WS_TILE - 1) / WS_TILE;
   const i64 plane = rows * ld;
   const int niter = blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
 
   if (tid == 0) {
     mbar_init(&S.bar_tab, 1);
     for (int b = 0; b < 2; b++) {
-      mbar_init(&S.xb_full[b], WS_LOADERS);
+      mbar_init(&S.xb_full[b], MODE == 1 ? 1 : WS_LOADERS);
       mbar_init(&S.xb_empty[b], 1);
       mbar_init(&S.tm_full[b], 1);
       mbar_init(&S.tm_empty[b], 32 * RW);
     }
+    for (int r = 0; r < RAW; r++) mbar_init(&S.raw_full[r], 1);
     S.abort = 0;
     mbar_fence_init();
   }
@@ -305,10 +318,41 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
   tc_fence_after();
   const u32 tmem = S.tmem_slot;
 
-  if (warp < 4) {
+  if (MODE == 1 && warp < 4) {
+    // ------------------------------------------------ operand rows by TMA (one thread)
+    if (tid == 0) {
+      mbar_expect_tx(&S.bar_tab, 2 * KT * kTileBytes);
+      const uint8_t* src = tab + (size_t)grp * 2 * KT * kTileBytes;
+      bulk_load(&S.tab_lo[0][0], src, KT * kTileBytes, &S.bar_tab);
+      bulk_load(&S.tab_hi[0][0], src + (size_t)KT * kTileBytes, KT * kTileBytes, &S.bar_tab);
+      for (int it = 0; it < niter; it++) {
+        const int slot = it & 1;
+        if (it >= 2 && !mbar_wait(&S.xb_empty[slot], ((it >> 1) - 1) & 1, err)) {
+          S.abort = 1;
+          break;
+        }
+        if (S.abort) break;
+        const i64 tile = blockIdx.x + (i64)it * gridDim.x;
+        const i64 i = tile / tpi, kb = tile - i * tpi;
+        mbar_expect_tx(&S.xb_full[slot], KT * kTileBytes);
+#pragma unroll
+        for (int kt = 0; kt < KT; kt++)
+          tma_load_2d(&S.xb[slot][kt][0], &map_in, &S.xb_full[slot], 128 * kt, (int)(i * Rp + k0 + kb * 128));
+      }
+    }
+  } else if (warp < 4) {
     // ------------------------------------------------ loaders
     const int ent = tid;
     auto issue = [&](int it) {
+      if (MODE == 2) {                           // one 3-D copy of the tile's L x 128 limb words
+        if (tid == 0 && it < niter) {
+          const i64 tile = blockIdx.x + (i64)it * gridDim.x;
+          const i64 i = tile / tpi, kb = tile - i * tpi;
+          mbar_expect_tx(&S.raw_full[it % RAW], (u32)L * WS_TILE * 4);
+          tma_load_3d(&S.raw[it % RAW][0][0], &map_in, &S.raw_full[it % RAW], (int)(kb * WS_TILE), (int)i, 0);
+        }
+        return;
+      }
       if (it < niter) {
         i64 tile = blockIdx.x + (i64)it * gridDim.x;
         if (vec) {
@@ -340,12 +384,15 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
       bulk_load(&S.tab_hi[0][0], src + (size_t)KT * kTileBytes, KT * kTileBytes, &S.bar_tab);
     }
     for (int it = 0; it < RAW - 1; it++) issue(it);
-    for (int it = 0; it < niter; it++) {
+    int it = 0;
+    for (; it < niter; it++) {
       named_sync(1, WS_LOADERS);                 // everyone is done reading the raw stage refilled next
       issue(it + RAW - 1);
-      cp_async_wait<RAW - 1>();
+      bool fail = false;
+      if (MODE == 2) fail = !mbar_wait(&S.raw_full[it % RAW], (it / RAW) & 1, err);
+      else cp_async_wait<RAW - 1>();
       const int slot = it & 1;
-      bool fail = it >= 2 && !mbar_wait(&S.xb_empty[slot], ((it >> 1) - 1) & 1, err);
+      fail = fail || (it >= 2 && !mbar_wait(&S.xb_empty[slot], ((it >> 1) - 1) & 1, err));
       // tile it's words (from all loaders) have landed; the abort decision is uniform across loaders
       if (named_sync_or(1, WS_LOADERS, fail || S.abort)) {
         S.abort = 1;
@@ -367,6 +414,8 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
       mbar_arrive(&S.xb_full[slot]);
     }
     cp_async_wait<0>();
+    if (MODE == 2 && tid == 0)                   // after an abort: let the copies in flight land (bounded)
+      for (int j = it; j < niter && j < it + RAW; j++) mbar_wait(&S.raw_full[j % RAW], (j / RAW) & 1, err);
   } else if (warp == 4) {
     // ------------------------------------------------ MMA issuer
     if (lane == 0) {
@@ -492,8 +541,14 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
         if (elected) {
           // moduli rows beyond g0 + G and entries beyond nent are clipped by the tensor bounds
           const int y = grp * 128 - g0;
-          tma_store_2d(&map_hi, &S.out[sb][0][0], (int)(tile * WS_TILE), y);
-          tma_store_2d(&map_lo, &S.out[sb][1][0], (int)(tile * WS_TILE), y);
+          if (TILED) {                                     // (k block, entry row i, moduli), clipped at kp
+            const i64 i = tile / tpi, kb = tile - i * tpi;
+            tma_store_3d(&map_hi, &S.out[sb][0][0], (int)(kb * WS_TILE), (int)i, y);
+            tma_store_3d(&map_lo, &S.out[sb][1][0], (int)(kb * WS_TILE), (int)i, y);
+          } else {
+            tma_store_2d(&map_hi, &S.out[sb][0][0], (int)(tile * WS_TILE), y);
+            tma_store_2d(&map_lo, &S.out[sb][1][0], (int)(tile * WS_TILE), y);
+          }
           bulk_commit();
         }
       }
@@ -560,40 +615,121 @@ bool res_store_map(CUtensorMap* map, void* base, i64 nent, i64 G, i64 ps) {
          CUDA_SUCCESS;
 }
 
+// 3-D uint8 map over residue planes (kp entries, nI rows, G moduli), plane stride ps: 128 x 1 x 128 boxes.
+bool res_store_map3(CUtensorMap* map, void* base, i64 kp, i64 nI, i64 G, i64 ps) {
+  sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)nI, (cuuint64_t)G};
+  cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)ps};
+  cuuint32_t box[3] = {128, 1, 128};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+template <int KT, int RAW, int STG, bool U8, int RW, int MODE>
+bool ws_attr(size_t smem) {
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    if (cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG, U8, RW, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return false;
+    attr_set[dev & 63] = true;
+  }
+  return true;
+}
+
 template <int KT, int RAW, int STG, bool U8, int RW>
 int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, int g0, int G,
               int8_t* Rhi, int8_t* Rlo, i64 ps, cudaStream_t st) {
   const sdpv::CtxDev& d = c->d;
   size_t smem = sizeof(WsSmem<KT, RAW, STG>) + 1024;
   if (smem > 227 * 1024) return SDPV_EINVAL;
-  static bool attr_set[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(residues_ws_kernel<KT, RAW, STG, U8, RW>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return sdpv::set_cuda_error(e);
-    attr_set[dev & 63] = true;
-  }
   const i64 nent = rows * kp;
+  int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
+  i64 gx = num_sms();
+  const bool out_ok = (g0 % 128 == 0) && ((((uintptr_t)Rhi) | ((uintptr_t)Rlo)) & 15) == 0;
+  // TMA both ways (MODE 2) when the limb rows start 16-byte aligned and the residue planes allow bulk stores
+  if (out_ok && ld % 4 == 0 && k0 % 4 == 0 && ((((uintptr_t)X) & 15) == 0) && d.L <= 256 && rows < (1ll << 31) &&
+      kc < (1ll << 31)) {
+    sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
+    CUtensorMap mi, mh, ml;
+    cuuint64_t dims[3] = {(cuuint64_t)kc, (cuuint64_t)rows, (cuuint64_t)d.L};
+    cuuint64_t strides[2] = {(cuuint64_t)(ld * 4), (cuuint64_t)(rows * ld * 4)};
+    cuuint32_t box[3] = {128, 1, (cuuint32_t)d.L};
+    cuuint32_t estr[3] = {1, 1, 1};
+    if (fn && fn(&mi, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<int32_t*>(X + k0), dims, strides, box, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+        res_store_map3(&mh, Rhi, kp, rows, G, ps) && res_store_map3(&ml, Rlo, kp, rows, G, ps)) {
+      if (!ws_attr<KT, RAW, STG, U8, RW, 2>(smem)) return sdpv::set_cuda_error(cudaGetLastError());
+      const i64 tpi = (kp + WS_TILE - 1) / WS_TILE, ntiles = rows * tpi;
+      if (gx > ntiles) gx = ntiles;
+      dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
+      residues_ws_kernel<KT, RAW, STG, U8, RW, 2><<<grid, ws_threads<RW>(), smem, st>>>(
+          mh, ml, mi, 0, tpi, 1, 1, X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo,
+          ps, sdpv::device_error_word());
+      return sdpv::launch_status();
+    }
+  }
+  if (!ws_attr<KT, RAW, STG, U8, RW, 0>(smem)) return sdpv::set_cuda_error(cudaGetLastError());
   // bulk tensor stores need 16-byte aligned planes and a box that starts at modulus row >= 0
   CUtensorMap mh, ml;
-  int use_tma = (g0 % 128 == 0) && ((((uintptr_t)Rhi) | ((uintptr_t)Rlo)) & 15) == 0 && nent < (1ll << 31) &&
-                res_store_map(&mh, Rhi, nent, G, ps) && res_store_map(&ml, Rlo, nent, G, ps);
+  int use_tma = out_ok && nent < (1ll << 31) && res_store_map(&mh, Rhi, nent, G, ps) &&
+                res_store_map(&ml, Rlo, nent, G, ps);
   if (!use_tma) {
     memset(&mh, 0, sizeof(mh));
     memset(&ml, 0, sizeof(ml));
   }
   // 16-byte limb copies when every 4-entry group of a row starts 16-byte aligned
   const int vec = (ld % 4 == 0) && (k0 % 4 == 0) && ((((uintptr_t)X) & 15) == 0);
-  int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
   i64 ntiles = (nent + WS_TILE - 1) / WS_TILE;
+  if (gx > ntiles) gx = ntiles;
+  dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
+  CUtensorMap unused;
+  memset(&unused, 0, sizeof(unused));
+  residues_ws_kernel<KT, RAW, STG, U8, RW, 0><<<grid, ws_threads<RW>(), smem, st>>>(
+      mh, ml, unused, 0, 1, use_tma, vec, X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo, ps,
+      sdpv::device_error_word());
+  return sdpv::launch_status();
+}
+
+// Operand-row input (unsigned digits out): tiles (i, 128-entry block of k), TMA in and out.
+template <int KT, int RW>
+int launch_ws_rows(const sdpv_ctx* c, const uint8_t* rows_in, i64 nI, i64 Rp, i64 k0, i64 kc, i64 kp, int g0, int G,
+                   uint8_t* Rhi, uint8_t* Rlo, i64 ps, cudaStream_t st) {
+  constexpr int RAW = 1, STG = KT == 1 ? 2 : 1;
+  const sdpv::CtxDev& d = c->d;
+  size_t smem = sizeof(WsSmem<KT, RAW, STG>) + 1024;
+  if (smem > 227 * 1024) return SDPV_EINVAL;
+  if (!ws_attr<KT, RAW, STG, true, RW, 1>(smem)) return sdpv::set_cuda_error(cudaGetLastError());
+  sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
+  if (!fn) return SDPV_EINVAL;
+  const i64 rb = 128 * KT;                                 // bytes per operand row
+  CUtensorMap mi, mh, ml;
+  {
+    cuuint64_t dims[2] = {(cuuint64_t)rb, (cuuint64_t)(nI * Rp)};
+    cuuint64_t strides[1] = {(cuuint64_t)rb};
+    cuuint32_t box[2] = {128, 128};
+    cuuint32_t estr[2] = {1, 1};
+    if (fn(&mi, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(rows_in), dims, strides, box, estr,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return SDPV_EINVAL;
+  }
+  if (!res_store_map3(&mh, Rhi, kp, nI, G, ps) || !res_store_map3(&ml, Rlo, kp, nI, G, ps)) return SDPV_EINVAL;
+  const i64 tpi = (kp + WS_TILE - 1) / WS_TILE;
+  const i64 ntiles = nI * tpi;
+  int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
   i64 gx = num_sms();
   if (gx > ntiles) gx = ntiles;
   dim3 grid((unsigned)gx, (unsigned)(grp1 - grp0 + 1));
-  residues_ws_kernel<KT, RAW, STG, U8, RW><<<grid, ws_threads<RW>(), smem, st>>>(
-      mh, ml, use_tma, vec, X, d.L, rows, ld, k0, kc, kp, g0, G, grp0, d.tabu, d.mods, d.minv, d.n, Rhi, Rlo, ps,
-      sdpv::device_error_word());
+  residues_ws_kernel<KT, RAW, STG, true, RW, 1><<<grid, ws_threads<RW>(), smem, st>>>(
+      mh, ml, mi, Rp, tpi, 1, 0, nullptr, d.L, nI, 0, k0, kc, kp, g0, G, grp0, d.tabu, d.mods, d.minv, d.n,
+      reinterpret_cast<int8_t*>(Rhi), reinterpret_cast<int8_t*>(Rlo), ps, sdpv::device_error_word());
   return sdpv::launch_status();
 }
 
@@ -646,4 +782,25 @@ extern "C" int sdpv_residues_u8(const sdpv_ctx* c, const int32_t* X, int64_t row
                                 int g0, int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride, void* stream) {
   return residues_entry<true>(c, X, rows, ld, k0, kc, g0, G, reinterpret_cast<int8_t*>(Rhi),
                               reinterpret_cast<int8_t*>(Rlo), plane_stride, stream);
+}
+
+extern "C" int sdpv_residues_rows(const sdpv_ctx* c, const uint8_t* rows, int64_t nI, int64_t Rp, int64_t k0,
+                                  int64_t kc, int g0, int G, uint8_t* Rhi, uint8_t* Rlo, int64_t plane_stride,
+                                  void* stream) {
+  if (!c || !rows || nI < 0 || kc < 0 || k0 < 0 || (k0 & 127) || Rp < 0 || (Rp & 127) || k0 + kc > Rp || g0 < 0 ||
+      (g0 & 127) || G < 1 || g0 + G > c->d.n || (c->d.kt != 1 && c->d.kt != 2))
+    return SDPV_EINVAL;
+  const i64 kp = (kc + 15) / 16 * 16;
+  const i64 ps = plane_stride ? plane_stride : nI * kp;
+  if (ps < nI * kp || (ps & 15) || ((((uintptr_t)rows) | ((uintptr_t)Rhi) | ((uintptr_t)Rlo)) & 15) ||
+      nI * Rp >= (1ll << 31) || nI >= (1ll << 31))
+    return SDPV_EINVAL;
+  if (nI == 0 || kc == 0) return SDPV_OK;
+  cudaStream_t st = sdpv::as_stream(stream);
+  const bool rw16 = sdpv::tune(SDPV_TUNE_RES_WARPS) == 16;
+  if (c->d.kt == 1)
+    return rw16 ? launch_ws_rows<1, 16>(c, rows, nI, Rp, k0, kc, kp, g0, G, Rhi, Rlo, ps, st)
+                : launch_ws_rows<1, 8>(c, rows, nI, Rp, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
+  return rw16 ? launch_ws_rows<2, 16>(c, rows, nI, Rp, k0, kc, kp, g0, G, Rhi, Rlo, ps, st)
+              : launch_ws_rows<2, 8>(c, rows, nI, Rp, k0, kc, kp, g0, G, Rhi, Rlo, ps, st);
 }

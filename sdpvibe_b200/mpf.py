@@ -345,6 +345,19 @@ def aligned(A, target, per_col, transpose, Lout=None):
     return out
 
 
+def aligned_rows(A, target, per_col, Lout, Rp):
+    """aligned(A, target, per_col, transpose=True, Lout) as operand rows for RNS.residues_rows: (nb, C, Rp,
+    rb) uint8, row (b, c, r) = the Lout limbs' bytes, a sign byte, zeros (rb = 128 bytes for Lout <= 31, 256
+    for Lout <= 63); rows R .. Rp - 1 zero (one kernel)."""
+    nb, R, C = _dims3(A)
+    rb = 128 if Lout <= 31 else 256
+    m, e = A.m.contiguous(), A.e.contiguous()
+    out = torch.empty((nb, C, Rp, rb), dtype=torch.uint8, device=m.device)
+    _lib.call("sdpv_align_rows", _lib.ptr(m), _lib.ptr(e), A.L, nb, R, C, _lib.ptr(target.contiguous()), int(per_col),
+              Lout, Rp, _lib.ptr(out), _lib.stream())
+    return out
+
+
 def _row_exponents(tmax, L):
     """mpf.py:394-395: common exponent max(top) - NB per row, 0 for all-zero rows."""
     E = tmax - NBITS(L)
@@ -406,6 +419,7 @@ class GramAcc:
     so ``add`` never waits for the GPU and a whole accumulation can be captured in a CUDA graph; the
     arithmetic, and so every bit of the result, is that of the host-branch formulation."""
     HEAD = 28
+    OPERAND_ROWS = False       # True: align to operand rows and decompose them (sdpv_align_rows / _residues_rows)
 
     def __init__(self, N, L, E_ref=None):
         self.N, self.L = N, L
@@ -434,13 +448,23 @@ class GramAcc:
         known = self.E > EZ // 2
         self.E = torch.where(live & ~known, tp, self.E)
         rows = P.shape[0]
-        # columns aligned to E_j - NB in L+1 limbs and transposed to (N, rows), one kernel
-        X = aligned(P, (self.E - NBITS(L))[None, :], per_col=True, transpose=True, Lout=L + 1).view(L + 1, N, rows)
         if self.acc is None:
             # rows padded to a multiple of 8 entries (16 bytes) for the vectorised GEMM epilogue
             self.acc = torch.zeros((R.n, N, -(-N // 8) * 8), dtype=torch.int16, device=dev)
-        if rows:
+        if not rows:
+            return
+        target = (self.E - NBITS(L))[None, :]
+        if self.OPERAND_ROWS and L + 1 <= 63:
+            # columns aligned to E_j - NB in L+1 limbs as operand rows (column j's rows padded to a multiple of
+            # 128), decomposed straight from them
+            from .mpmat import residue_product_rows
+            Rp = -(-rows // 128) * 128
+            Xr = aligned_rows(P, target, per_col=True, Lout=L + 1, Rp=Rp)
+            residue_product_rows(R, Xr, N, Rp, rows, self.acc)
+        else:
+            # columns aligned in L+1 limbs and transposed to (N, rows) limb planes, one kernel
             from .mpmat import residue_product
+            X = aligned(P, target, per_col=True, transpose=True, Lout=L + 1).view(L + 1, N, rows)
             residue_product(R, X, None, self.acc, syrk=True)
 
     def _crt(self, pred=None):

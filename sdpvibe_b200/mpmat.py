@@ -203,6 +203,20 @@ def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False):
             del Ah, Al
 
 
+def residue_product_rows(R, Xr, nI, Rp, K, acc, fresh=False):
+    """residue_product(R, X, None, acc, syrk=True) of operand rows (mpf.aligned_rows: nI columns of Rp rows,
+    K of them used): acc += residues of X X^T, lower triangle."""
+    per_mod = nI * min(K, KC_MAX) * 2
+    GR = R.n if R.n * per_mod <= RES_BUDGET else max(128, (RES_BUDGET // per_mod) // 128 * 128)
+    for k0 in range(0, K, KC_MAX):                  # KC_MAX is a multiple of 128
+        kk = min(KC_MAX, K - k0)
+        for g0 in range(0, R.n, GR):
+            G = min(GR, R.n - g0)
+            Ah, Al = R.residues_rows(Xr, nI, Rp, k0, kk, g0, G)
+            R.accumulate(Ah, Al, None, None, acc, g0, syrk=True, fresh=fresh and k0 == 0, unsigned=True)
+            del Ah, Al
+
+
 def gemm_nt(A, Bt, out_exp="col", kc=4096, colblock=None, bt_rowexp=None):
     """C = A @ Bt^T, exact, then rounded (sdpvibe/mpmat.py:169-202).  A: (M, K) single exponent; Bt:
     (N, K) single exponent, or per-row exponents bt_rowexp (N,).  out_exp: 'col', 'mat', or an int /

@@ -81,6 +81,20 @@ class RNS:
                   _lib.ptr_strided(Rhi), _lib.ptr_strided(Rlo), ps, _lib.stream())
         return Rhi, Rlo
 
+    def residues_rows(self, Xr, nI, Rp, k0, kc, g0=0, G=None):
+        """residues(..., spread=True, unsigned=True) of operand rows (mpf.aligned_rows): entry (i, k) is row
+        i * Rp + k0 + k of Xr; k0 a multiple of 128, g0 of 128; rows k0 + kc .. k0 + kp - 1 must be zero rows."""
+        G = G or self.n
+        kp = -(-kc // self.KPAD) * self.KPAD
+        ps = plane_stride(nI * kp)
+        buf_h = torch.empty((G * ps,), dtype=torch.uint8, device=Xr.device)
+        buf_l = torch.empty_like(buf_h)
+        Rhi = buf_h.as_strided((G, nI, kp), (ps, kp, 1))
+        Rlo = buf_l.as_strided((G, nI, kp), (ps, kp, 1))
+        _lib.call("sdpv_residues_rows", self._h, _lib.ptr(Xr), nI, Rp, k0, kc, g0, G, _lib.ptr_strided(Rhi),
+                  _lib.ptr_strided(Rlo), ps, _lib.stream())
+        return Rhi, Rlo
+
     # ---- step 2: accumulate residues of A @ Bt^T (sdpvibe/rns.py:217-224)
     def accumulate(self, Ahi, Alo, Bhi, Blo, acc, g0=0, nb=1, syrk=False, fresh=False, unsigned=False):
         """acc[g0:g0+G] += residues of A @ B^T; with nb > 1 the operands hold nb blocks stacked along rows.

@@ -248,6 +248,42 @@ def test_rns_gemm_syrk_fused_tail(sb, nb, M, K, fresh, unsigned):
         assert np.array_equal(got[:, sl][:, ~low], acc0[:, sl][:, ~low])     # upper triangle untouched
 
 
+@pytest.mark.parametrize("L,R,C", [(26, 300, 37), (26, 130, 5), (50, 200, 9), (26, 33000, 3), (26, 7, 1)])
+def test_operand_rows_alignment_and_residues(sb, L, R, C):
+    """GramAcc's operand rows: the bytes of the planar aligned limbs, the sign byte, zero padding rows; their
+    residues equal the planar path's (unsigned digits), for both 128-entry K ranges of a 33000-row chunk"""
+    from sdpvibe_b200.mpf import MPF, aligned, aligned_rows, top_max, NBITS, EZ
+    from sdpvibe_b200.mpmat import ctx
+    rng = np.random.default_rng(L + R + C)
+    m = rand_limbs(rng, L, R * C).reshape(L, R, C)
+    e = rng.integers(-8, 9, size=(R, C))
+    m[:, 0, :] = 0
+    e[0, :] = EZ                                                 # a zero row
+    m[:, 1 % R, 0] = 0
+    m[0, 1 % R, 0] = 5                                           # a short mantissa
+    P = MPF(cu(m), cu(e))
+    tp = top_max(P, over_rows=True)[0]
+    target = (torch.where(tp > EZ // 2, tp, torch.zeros_like(tp)) - NBITS(L))[None, :]
+    Lo = L + 1
+    X = aligned(P, target, per_col=True, transpose=True, Lout=Lo).view(Lo, C, R)
+    Rp = -(-R // 128) * 128
+    Xr = aligned_rows(P, target, per_col=True, Lout=Lo, Rp=Rp)
+    rb = Xr.shape[-1]
+    assert rb == (128 if Lo <= 31 else 256)
+    xr = np_(Xr).reshape(C, Rp, rb)
+    xp = np_(X)                                                  # (Lo, C, R) int32
+    limb_bytes = np.ascontiguousarray(np.moveaxis(xp, 0, -1)).view(np.uint8).reshape(C, R, 4 * Lo)
+    assert np.array_equal(xr[:, :R, :4 * Lo], limb_bytes)
+    assert np.array_equal(xr[:, :R, 4 * Lo], (xp[Lo - 1] < 0).astype(np.uint8))
+    assert not xr[:, :R, 4 * Lo + 1:].any() and not xr[:, R:].any()
+    Rc = ctx(Lo)
+    for k0 in range(0, R, 32768):
+        kc = min(32768, R - k0)
+        gh, gl = Rc.residues_rows(Xr, C, Rp, k0, kc)
+        wh, wl = Rc.residues(X, k0, kc, spread=True, unsigned=True)
+        assert np.array_equal(np_(gh), np_(wh)) and np.array_equal(np_(gl), np_(wl)), k0
+
+
 # ------------------------------------------------------------------ CRT (c)
 @pytest.mark.parametrize("name", golden_names("crt_block_"))
 def test_crt_block_golden(sb, name):
@@ -713,7 +749,7 @@ def test_tuning_knobs_do_not_change_results(sb):
             set_knob(k, v)
 
 
-@pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (50, 9, 130), (26, 3, 4097)])
+@pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (50, 9, 132), (26, 3, 4097), (50, 17, 4000)])
 def test_decomposition_reducer_warps(sb, L, rows, K):
     """8 and 16 reducer warps of the decomposition kernel give the oracle's residues (API digits) and its
     canonical residues (unsigned digits)"""
@@ -727,8 +763,15 @@ def test_decomposition_reducer_warps(sb, L, rows, K):
     X[-1, 0, 5] = -(1 << 31)
     X[:, 0, 6] = -1
     rh, rl = O.residues(T, X, 1, K - 1)
+    rh0, rl0 = O.residues(T, X, 0, K)
     m = T.m32.astype(np.int64)[:, None, None]
     rc = (128 * rh.astype(np.int64) + rl) % m
+    # the same entries as operand rows (limb bytes, sign byte, zero rows up to a multiple of 128)
+    Rp = -(-(K - 1) // 128) * 128
+    Xr = np.zeros((rows, Rp, 128 if L <= 31 else 256), np.uint8)
+    xs = X[:, :, 1:]
+    Xr[:, :K - 1, :4 * L] = np.ascontiguousarray(np.moveaxis(xs, 0, -1)).view(np.uint8).reshape(rows, K - 1, 4 * L)
+    Xr[:, :K - 1, 4 * L] = (xs[L - 1] < 0)
     saved = get_knob("res_warps")
     try:
         for w in (8, 16):
@@ -739,6 +782,11 @@ def test_decomposition_reducer_warps(sb, L, rows, K):
             kk = rc.shape[2]
             assert np.array_equal(np_(uh)[:, :, :kk], (rc >> 7).astype(np.uint8)), w
             assert np.array_equal(np_(ul)[:, :, :kk], (rc & 127).astype(np.uint8)), w
+            vh, vl = R.residues_rows(cu(Xr), rows, Rp, 0, K - 1)
+            assert np.array_equal(np_(vh), np_(uh)) and np.array_equal(np_(vl), np_(ul)), w
+            # k0 = 0 and 16-byte aligned rows: the limb planes come in by TMA
+            hi0, lo0 = R.residues(cu(X), 0, K)
+            assert np.array_equal(np_(hi0), rh0) and np.array_equal(np_(lo0), rl0), w
     finally:
         set_knob("res_warps", saved)
 
