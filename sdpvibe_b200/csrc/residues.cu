@@ -229,14 +229,16 @@ __global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
 //   warps 0-3  loaders: 4-byte cp.async of the next tiles' limb planes into a raw ring (kRawStages),
 //              then the transform into a double-buffered K-major entry tile (xb[2]);
 //   warp 4     MMA issuer (one lane): D_lo / D_hi of a 128-entry tile into one of two TMEM buffers;
-//   warps 5-12 reducers: TMEM lane quarter = warp % 4, 64 entries each; exact centred reduction,
-//              digit split and 32-byte stores.
+//   warps 5-12 reducers: TMEM lane quarter = warp % 4, 64 entries each; exact residue, digit split, staging
+//              of the residue tile (or direct stores where bulk stores cannot be used);
+//   warp 13    store warp (one lane): the bulk tensor stores of each staged tile, releasing its staging buffer
+//              once read (stg_full: reducer arrivals, stg_empty: the store lane).
 // mbarriers: xb_full (128 loader arrivals), xb_empty (MMA commit), tm_full (MMA commit),
 // tm_empty (256 reducer arrivals).  Every wait is bounded; a timeout aborts all roles.
 constexpr int WS_TILE = 128, WS_LOADERS = 128;
 // RW reducer warps (8 or 16): RW / 4 per TMEM lane quarter, 128 / (RW / 4) columns each
 template <int RW>
-constexpr int ws_threads() { return WS_LOADERS + 32 + 32 * RW; }
+constexpr int ws_threads() { return WS_LOADERS + 32 + 32 * RW + 32; }      // + the store warp
 
 template <int KT, int RAW, int STG>
 struct WsSmem {
@@ -246,6 +248,7 @@ struct WsSmem {
   uint8_t out[STG][2][kTileBytes];      // residue tiles (128 moduli x 128 entries, hi | lo), 128-byte swizzle
   u32 raw[RAW][32 * KT - 1][WS_TILE];
   u64 bar_tab, xb_full[2], xb_empty[2], tm_full[2], tm_empty[2], raw_full[RAW];
+  u64 stg_full[STG], stg_empty[STG];     // staged residue tile complete / read by its bulk store
   u32 tmem_slot;
   volatile int abort;
 };
@@ -307,6 +310,10 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
       mbar_init(&S.tm_empty[b], 32 * RW);
     }
     for (int r = 0; r < RAW; r++) mbar_init(&S.raw_full[r], 1);
+    for (int r = 0; r < STG; r++) {
+      mbar_init(&S.stg_full[r], 32 * RW);
+      mbar_init(&S.stg_empty[r], 1);
+    }
     S.abort = 0;
     mbar_fence_init();
   }
@@ -444,9 +451,36 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
       // on an abort, let the last committed products finish before TMEM is released (bounded)
       if (S.abort && issued > 0) mbar_wait(&S.tm_full[(issued - 1) & 1], ((issued - 1) >> 1) & 1, err);
     }
+  } else if (warp == 5 + RW) {
+    // ------------------------------------------------ bulk stores of the staged residue tiles (one lane), off the
+    // reducers' path: staging sb is released once its store has read it
+    if (lane == 0 && use_tma) {
+      for (int it = 0; it < niter; it++) {
+        const int sb = it % STG;
+        if (!mbar_wait(&S.stg_full[sb], (it / STG) & 1, err)) {
+          S.abort = 1;
+          break;
+        }
+        const i64 tile = blockIdx.x + (i64)it * gridDim.x;
+        // moduli rows beyond g0 + G and entries beyond nent (kp in the tiled modes) are clipped by the bounds
+        const int y = grp * 128 - g0;
+        if (TILED) {                                     // (k block, entry row i, moduli)
+          const i64 i = tile / tpi, kb = tile - i * tpi;
+          tma_store_3d(&map_hi, &S.out[sb][0][0], (int)(kb * WS_TILE), (int)i, y);
+          tma_store_3d(&map_lo, &S.out[sb][1][0], (int)(kb * WS_TILE), (int)i, y);
+        } else {
+          tma_store_2d(&map_hi, &S.out[sb][0][0], (int)(tile * WS_TILE), y);
+          tma_store_2d(&map_lo, &S.out[sb][1][0], (int)(tile * WS_TILE), y);
+        }
+        bulk_commit();
+        bulk_wait_read<STG - 1>();                       // the store of tile it - (STG - 1) has read its staging
+        if (it >= STG - 1) mbar_arrive(&S.stg_empty[(it - (STG - 1)) % STG]);
+      }
+      bulk_wait<0>();
+    }
   } else {
     // ------------------------------------------------ reducers
-    constexpr int WS_REDUCERS = 32 * RW, CHUNKS = 16 / RW;        // 32-column chunks per warp and tile
+    constexpr int CHUNKS = 16 / RW;                              // 32-column chunks per warp and tile
     const int quarter = warp & 3, part = (warp - 5) >> 2;
     const int row = quarter * 32 + lane;
     const int g = grp * 128 + row;
@@ -457,13 +491,13 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
     const u32 bm = (u32)(((1ull << 46) + (u64)m - 1) / (u64)m);   // ceil(2^46 / m) < 2^32 (m > 2^14)
     int8_t* outh = Rhi + (i64)(g - g0) * pstride;
     int8_t* outl = Rlo + (i64)(g - g0) * pstride;
-    const bool elected = (tid == WS_LOADERS + 32);       // first reducer thread issues the bulk stores
     for (int it = 0; it < niter; it++) {
       const int b = it & 1, sb = it % STG;
       bool fail = !mbar_wait(&S.tm_full[b], (it >> 1) & 1, err);
-      if (use_tma && elected) bulk_wait_read<STG - 1>();  // staging buffer sb no longer read by its store
-      // uniform across all reducers (they share named barriers and warp-collective TMEM loads)
-      if (named_sync_or(2, WS_REDUCERS, fail || S.abort)) {
+      // staging sb free: the store of tile it - STG has read it
+      if (use_tma && it >= STG) fail = fail || !mbar_wait(&S.stg_empty[sb], ((it / STG) - 1) & 1, err);
+      // uniform across the warp (warp-collective TMEM loads)
+      if (__any_sync(0xffffffffu, fail || S.abort)) {
         S.abort = 1;
         break;
       }
@@ -537,23 +571,9 @@ __global__ void __launch_bounds__(ws_threads<RW>(), 1)
       mbar_arrive(&S.tm_empty[b]);
       if (use_tma) {
         fence_proxy_async_smem();                          // staging writes visible to the bulk copy engine
-        named_sync(2, WS_REDUCERS);
-        if (elected) {
-          // moduli rows beyond g0 + G and entries beyond nent are clipped by the tensor bounds
-          const int y = grp * 128 - g0;
-          if (TILED) {                                     // (k block, entry row i, moduli), clipped at kp
-            const i64 i = tile / tpi, kb = tile - i * tpi;
-            tma_store_3d(&map_hi, &S.out[sb][0][0], (int)(kb * WS_TILE), (int)i, y);
-            tma_store_3d(&map_lo, &S.out[sb][1][0], (int)(kb * WS_TILE), (int)i, y);
-          } else {
-            tma_store_2d(&map_hi, &S.out[sb][0][0], (int)(tile * WS_TILE), y);
-            tma_store_2d(&map_lo, &S.out[sb][1][0], (int)(tile * WS_TILE), y);
-          }
-          bulk_commit();
-        }
+        mbar_arrive(&S.stg_full[sb]);
       }
     }
-    if (use_tma && elected) bulk_wait<0>();
   }
   __syncthreads();
   if (warp == 4) tmem_dealloc(tmem, 512);
