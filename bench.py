@@ -304,7 +304,7 @@ def run_b200(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clk:
         ms = timed(graph.replay, args.steps)
     tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_crt_norm", "sdpv_align",
-                             "sdpv_align_rows", "sdpv_top_max"})
+                             "sdpv_align_t", "sdpv_align_rows", "sdpv_top_max"})
     ms_eager = timed(step, args.steps, tr)
     for _ in range(2):
         step_e2e()
@@ -441,7 +441,7 @@ def run_cholsolve(args, rank, world, local_rank):
     names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
              "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_rows")
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_t", "sdpv_align_rows")
     tr = _trace.Trace(timed=names)
     with ClockSampler(local_rank) as clk:
         ms = timed(step, args.steps, tr)
@@ -659,7 +659,7 @@ def solver_measurement(steps, warmup, local_rank, world=1):
     names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
              "sdpv_crt_norm",
              "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_rows")
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_t", "sdpv_align_rows")
     tr = _trace.Trace(timed=names)              # graph replays are timed whole, one entry per graph key
     with ClockSampler(local_rank) as clk, tr:
         torch.cuda.synchronize()

@@ -143,6 +143,11 @@ int sdpv_top_max(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t 
  * shift_round of mpf._align_rows (sdpvibe/mpf.py:390-398) and GramAcc.add (sdpvibe/mpf.py:572-576). */
 int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, const int64_t* target,
                int per_col, int transpose, int Lout, int32_t* out, void* stream);
+/* sdpv_align with transpose = 1 into (Lout, nb, C, Rld) limb planes, Rld >= R (rows R .. Rld - 1 of each
+ * column are left untouched): a row length that is a multiple of 4 lets the decomposition read the planes
+ * with bulk tensor copies.  No reference counterpart. */
+int sdpv_align_t(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C, const int64_t* target,
+                 int per_col, int Lout, int64_t Rld, int32_t* out, void* stream);
 /* The transposed alignment written as operand rows for sdpv_residues_rows: entry (b, r, c) of m becomes row
  * (b C + c) Rp + r of out (nb, C, Rp, rb) uint8, rb = 128 bytes for Lout <= 31, 256 for Lout <= 63: the Lout
  * aligned limbs little endian, then a sign byte (1 when the result is negative) at byte 4 Lout, then zeros;

@@ -48,6 +48,7 @@ _SIGS = {
     "sdpv_residues_u8": [_P, _P, _L, _L, _L, _L, _I, _I, _P, _P, _L, _P],
     "sdpv_residues_rows": [_P, _P, _L, _L, _L, _L, _I, _I, _P, _P, _L, _P],
     "sdpv_align_rows": [_P, _P, _I, _L, _L, _L, _P, _I, _I, _L, _P, _P],
+    "sdpv_align_t": [_P, _P, _I, _L, _L, _L, _P, _I, _I, _L, _P, _P],
     "sdpv_rns_gemm": [_P, _P, _P, _P, _P, _L, _L, _P, _L, _I, _I, _L, _L, _L, _L, _I, _P],
     "sdpv_crt_block": [_P, _P, _L, _L, _L, _L, _L, _P, _P, _P],
     "sdpv_crt_norm": [_P, _P, _L, _L, _L, _L, _L, _L, _P, _P, _I, _P, _P, _P],

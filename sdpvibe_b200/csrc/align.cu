@@ -167,11 +167,11 @@ __global__ void align_kernel(const int32_t* __restrict__ m, const i64* __restric
 constexpr int TR = 16, TC = 32;
 __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e,
                                                            int L, i64 nb, i64 R, i64 C, const i64* __restrict__ target,
-                                                           int per_col, int Lout, int32_t* __restrict__ out,
+                                                           int per_col, int Lout, i64 Rld, int32_t* __restrict__ out,
                                                            unsigned* err) {
   extern __shared__ u32 sm[];                       // [L][TR][TC + 1] limbs, then [TR][TC] exponents
   i64* se = reinterpret_cast<i64*>(sm + (size_t)L * TR * (TC + 1) + ((L * TR * (TC + 1)) & 1));
-  const i64 n = nb * R * C;
+  const i64 n = nb * R * C, no = nb * C * Rld;      // input / output plane sizes
   const i64 b = blockIdx.z;
   const i64 r0 = (i64)blockIdx.x * TR, c0 = (i64)blockIdx.y * TC;
   const int tid = threadIdx.x;
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __rest
     i64 ev = se[rr * TC + cc];
     i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
     const u32* base = sm + rr * (TC + 1) + cc;
-    shift_entry32([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * R + r, n, err);
+    shift_entry32([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * Rld + r, no, err);
   }
 }
 
@@ -393,16 +393,29 @@ extern "C" int sdpv_align_rows(const int32_t* m, const int64_t* e, int L, int64_
   return sdpv::launch_status();
 }
 
+extern "C" int sdpv_align_t(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
+                            const int64_t* target, int per_col, int Lout, int64_t Rld, int32_t* out, void* stream);
+
 extern "C" int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
                           const int64_t* target, int per_col, int transpose, int Lout, int32_t* out, void* stream) {
+  if (transpose) return sdpv_align_t(m, e, L, nb, R, C, target, per_col, Lout, R, out, stream);
   if (L < 1 || L > 64 || Lout < 1 || nb < 0 || R < 0 || C < 0 || nb > 65535) return SDPV_EINVAL;
   i64 n = nb * R * C;
   if (n == 0) return SDPV_OK;
   cudaStream_t st = sdpv::as_stream(stream);
   unsigned* err = sdpv::device_error_word();
-  if (!transpose) {
-    align_kernel<<<blocks(n), kThreads, 0, st>>>(m, e, L, nb, R, C, target, per_col, Lout, out, err);
-  } else {
+  align_kernel<<<blocks(n), kThreads, 0, st>>>(m, e, L, nb, R, C, target, per_col, Lout, out, err);
+  return sdpv::launch_status();
+}
+
+extern "C" int sdpv_align_t(const int32_t* m, const int64_t* e, int L, int64_t nb, int64_t R, int64_t C,
+                            const int64_t* target, int per_col, int Lout, int64_t Rld, int32_t* out, void* stream) {
+  if (L < 1 || L > 64 || Lout < 1 || nb < 0 || R < 0 || C < 0 || nb > 65535 || Rld < R) return SDPV_EINVAL;
+  i64 n = nb * R * C;
+  if (n == 0) return SDPV_OK;
+  cudaStream_t st = sdpv::as_stream(stream);
+  unsigned* err = sdpv::device_error_word();
+  {
     size_t smem = (size_t)L * TR * (TC + 1) * 4 + 8 + TR * TC * 8;
     static bool attr[64] = {};
     int dev = 0;
@@ -415,7 +428,7 @@ extern "C" int sdpv_align(const int32_t* m, const int64_t* e, int L, int64_t nb,
     }
     dim3 grid((unsigned)((R + TR - 1) / TR), (unsigned)((C + TC - 1) / TC), (unsigned)nb);
     if (grid.y > 65535 || (R + TR - 1) / TR > 0x7fffffff) return SDPV_EINVAL;
-    align_t_kernel<<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, target, per_col, Lout, out, err);
+    align_t_kernel<<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, target, per_col, Lout, Rld, out, err);
   }
   return sdpv::launch_status();
 }

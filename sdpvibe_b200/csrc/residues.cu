@@ -672,9 +672,11 @@ int launch_ws(const sdpv_ctx* c, const int32_t* X, i64 rows, i64 ld, i64 k0, i64
   int grp0 = g0 / 128, grp1 = (g0 + G - 1) / 128;
   i64 gx = num_sms();
   const bool out_ok = (g0 % 128 == 0) && ((((uintptr_t)Rhi) | ((uintptr_t)Rlo)) & 15) == 0;
-  // TMA both ways (MODE 2) when the limb rows start 16-byte aligned and the residue planes allow bulk stores
+  // TMA both ways (MODE 2) when the limb rows start 16-byte aligned, the residue planes allow bulk stores and
+  // tiling per entry row leaves at most 1/8 of the tiles' entries idle (short rows keep the packed tiles)
+  const i64 row_pad = (kp + WS_TILE - 1) / WS_TILE * WS_TILE - kp;
   if (out_ok && ld % 4 == 0 && k0 % 4 == 0 && ((((uintptr_t)X) & 15) == 0) && d.L <= 256 && rows < (1ll << 31) &&
-      kc < (1ll << 31)) {
+      kc < (1ll << 31) && 8 * row_pad <= kp) {
     sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
     CUtensorMap mi, mh, ml;
     cuuint64_t dims[3] = {(cuuint64_t)kc, (cuuint64_t)rows, (cuuint64_t)d.L};

@@ -333,12 +333,18 @@ def top_max(A, over_rows):
     return out
 
 
-def aligned(A, target, per_col, transpose, Lout=None):
+def aligned(A, target, per_col, transpose, Lout=None, ld=None):
     """Mantissas of A rounded to the exponents target (nb, R) per row or (nb, C) per column, as Lout
-    limbs, optionally transposed to (Lout, nb, C, R); zero entries give 0 (one kernel)."""
+    limbs, optionally transposed to (Lout, nb, C, R) -- or (Lout, nb, C, ld), ld >= R, with rows R .. ld - 1
+    unset; zero entries give 0 (one kernel)."""
     nb, R, C = _dims3(A)
     Lout = Lout or A.L
     m, e = A.m.contiguous(), A.e.contiguous()
+    if transpose and ld is not None:
+        out = torch.empty((Lout, nb, C, ld), dtype=torch.int32, device=m.device)
+        _lib.call("sdpv_align_t", _lib.ptr(m), _lib.ptr(e), A.L, nb, R, C, _lib.ptr(target.contiguous()), int(per_col),
+                  Lout, ld, _lib.ptr(out), _lib.stream())
+        return out
     out = torch.empty((Lout, nb, C, R) if transpose else (Lout, nb, R, C), dtype=torch.int32, device=m.device)
     _lib.call("sdpv_align", _lib.ptr(m), _lib.ptr(e), A.L, nb, R, C, _lib.ptr(target.contiguous()), int(per_col),
               int(transpose), Lout, _lib.ptr(out), _lib.stream())
@@ -462,10 +468,12 @@ class GramAcc:
             Xr = aligned_rows(P, target, per_col=True, Lout=L + 1, Rp=Rp)
             residue_product_rows(R, Xr, N, Rp, rows, self.acc)
         else:
-            # columns aligned in L+1 limbs and transposed to (N, rows) limb planes, one kernel
+            # columns aligned in L+1 limbs and transposed to (N, rows) limb planes (row length padded to a
+            # multiple of 4: 16-byte aligned rows for the decomposition's bulk copies), one kernel
             from .mpmat import residue_product
-            X = aligned(P, target, per_col=True, transpose=True, Lout=L + 1).view(L + 1, N, rows)
-            residue_product(R, X, None, self.acc, syrk=True)
+            ld = -(-rows // 4) * 4
+            X = aligned(P, target, per_col=True, transpose=True, Lout=L + 1, ld=ld).view(L + 1, N, ld)
+            residue_product(R, X, None, self.acc, syrk=True, kvalid=rows)
 
     def _crt(self, pred=None):
         L, N, R = self.L, self.N, self.R

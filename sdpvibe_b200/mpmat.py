@@ -182,10 +182,11 @@ def ctx(L):
     return _ctx[key]
 
 
-def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False):
-    """acc += residues of the exact products of nb stacked blocks: Av (L, nb*M, K), Bv (L, nb*N, K).
-    fresh: acc holds no data yet (the first K chunk overwrites instead of adding)."""
-    K = Av.shape[2]
+def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False, kvalid=None):
+    """acc += residues of the exact products of nb stacked blocks: Av (L, nb*M, K), Bv (L, nb*N, K); with
+    kvalid only the first kvalid of the K entries of each row are used.  fresh: acc holds no data yet (the
+    first K chunk overwrites instead of adding)."""
+    K = Av.shape[2] if kvalid is None else kvalid
     rows = Av.shape[1] + (0 if syrk else Bv.shape[1])
     per_mod = rows * min(K, KC_MAX) * 2
     GR = R.n if R.n * per_mod <= RES_BUDGET else max(R.G, (RES_BUDGET // per_mod) // R.G * R.G)

@@ -749,7 +749,7 @@ def test_tuning_knobs_do_not_change_results(sb):
             set_knob(k, v)
 
 
-@pytest.mark.parametrize("L,rows,K", [(27, 274, 300), (50, 9, 132), (26, 3, 4097), (50, 17, 4000)])
+@pytest.mark.parametrize("L,rows,K", [(27, 274, 1000), (50, 9, 132), (26, 3, 4097), (50, 17, 4000), (27, 5, 2048)])
 def test_decomposition_reducer_warps(sb, L, rows, K):
     """8 and 16 reducer warps of the decomposition kernel give the oracle's residues (API digits) and its
     canonical residues (unsigned digits)"""
