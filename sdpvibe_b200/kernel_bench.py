@@ -152,7 +152,8 @@ def _cholsolve(a, rng):
     tc = _events(chol_only, a.reps, a.warmup)
     names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_rns_gemm", "sdpv_crt_block",
              "sdpv_crt_norm", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align")
+             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_t",
+             "sdpv_align_rows", "sdpv_residues_rows")
     with _trace.Trace(timed=names) as tr:
         step()
         torch.cuda.synchronize()
