@@ -35,9 +35,10 @@ sys.path.insert(0, ROOT)
 METRIC = "768-bit SDP s/iter & residue-GEMM INT8 TOPS, fused vs plain, 1 B200, bit-exact"
 NBLOCKS, MLO, MHI, NCOLS, L, NCHUNK = 400, 20, 120, 274, 26, 4
 N_MOD = 128                       # moduli of the accumulator context (L + 1 = 27 limbs)
-# DRAM bytes (read + write) of one syrk launch per chunk row, from the ncu capture of
-# `kernel_bench --kernel syrk --N 274 --K 7000 --L 27` (524.8 MB read + 14.0 MB written / 7000 rows).
-SYRK_DRAM_BYTES_PER_ROW = (524.783104e6 + 13.99424e6) / 7000
+# DRAM bytes (read + write) of one syrk call (the full-tile launch with the fused tail, and the corner
+# launch) per chunk row, from the ncu capture of `kernel_bench --kernel syrk --N 274 --K 7000 --L 27`
+# ((522.41 + 32.86) MB read + (12.97 + 0.01) MB written / 7000 rows).
+SYRK_DRAM_BYTES_PER_ROW = (522.40768e6 + 32.863232e6 + 12.969984e6 + 0.006656e6) / 7000
 
 
 def workload_shape(seed=0):
@@ -335,7 +336,7 @@ def run_b200(args, rank, world, local_rank):
         "roofline": {"bound": "tensor", "kernel": "sdpv_rns_gemm (syrk, tcgen05 kind::i8)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": SYRK_DRAM_BYTES_PER_ROW * (R / NCHUNK),
-                     "traffic_note": "ncu dram read+write of one launch at N=274, K=7000 rows, scaled per row",
+                     "traffic_note": "ncu dram read+write of one call (full tiles + corner) at N=274, K=7000 rows, scaled per row",
                      "peak_source": f"2 x bf16_tflops of {src} (MEASURED_PEAKS.json): B200 dense int8 = 2 x dense bf16",
                      "int8_cublaslt_measured_tops": int8_lib,
                      "launch_ms_mean": statistics.mean(gemm_ms), "launches": len(gemm_ms),
