@@ -33,6 +33,7 @@ namespace {
 constexpr int kStages = 3;
 constexpr u32 kSlice = 128 * 128;            // one operand slice: 128 rows x 128 bytes
 constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue warps
+constexpr int kCornerKB = 8;                // syrk corner: K blocks of [Thi; Tlo] (8 KB) per ring stage
 
 constexpr int kMaxG = 128;                  // moduli per launch (more are split over launches)
 constexpr int kStg = 130;                   // staging row pitch (int16): 65 words, conflict-free by row
@@ -179,6 +180,25 @@ __global__ void __launch_bounds__(kThreads, 1)
           n0 = tn * 128;
         }
         const bool diag = mode == 1 && !tailTB && !nmode && pack <= 1 && m0 == n0;   // syrk diagonal: B = A
+        if (tailTB) {
+          // syrk corner (the tail rows against themselves): A = B = [Thi; Tlo], so one K block is the 2 TB
+          // rows of [Thi; Tlo] (8 KB) and a ring stage holds kCornerKB of them
+          for (int k8 = 0; k8 < nk; k8 += kCornerKB, kbg++) {
+            const u32 s = kbg % kStages;
+            if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
+              *(volatile int*)&S.abort = 1;
+              break;
+            }
+            const int nkb = nk - k8 < kCornerKB ? nk - k8 : kCornerKB;
+            mbar_expect_tx(&S.full[s], (u32)nkb * 2 * tailTB * 128);
+            for (int j = 0; j < nkb; j++) {
+              uint8_t* blk = &S.stage[s][0][0] + j * 2 * tailTB * 128;
+              tma_load_4d(blk, &mTh, &S.full[s], (k8 + j) * 128, nfull, b, g);
+              tma_load_4d(blk + tailTB * 128, &mTl, &S.full[s], (k8 + j) * 128, nfull, b, g);
+            }
+          }
+          continue;
+        }
         for (int kb = 0; kb < nk; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
@@ -285,7 +305,43 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         bool ok = true;
-        for (int kb = 0; kb < nk; kb++, kbg++) {
+        for (int k8 = 0; tailTB && k8 < nk; k8 += kCornerKB, kbg++) {
+          // syrk corner: K block j of the stage at byte 8 KB j: A hi = Thi, A lo = Tlo (the M = 128 operand reads
+          // on past the 32 loaded rows, into TMEM lanes whose entries the epilogue never stores; the reads stay
+          // inside the shared-memory allocation), B = [Thi; Tlo]
+          const u32 s = kbg % kStages;
+          if (!mbar_wait(&S.full[s], (kbg / kStages) & 1, err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int nkb = nk - k8 < kCornerKB ? nk - k8 : kCornerKB;
+          for (int j = 0; j < nkb; j++) {
+            const int kb = k8 + j;
+            const u32 blk = smem_u32(&S.stage[s][0][0]) + j * 2 * TB * 128;
+            const u64 dah = sdesc_sw128(blk), dal = sdesc_sw128(blk + TB * 128);
+            auto cstep = [&](int ks) {
+              const u64 bd = dah + 2 * ks;
+              if ((kb | ks) == 0) {
+                mma_i8(tmem + 0, dah, bd, idesc, 0u);                                            // hh | hl
+                mma_i8(tmem + 2 * TB, dal, dal, idesc128, 0u);                                   // ll
+                mma_i8(tmem + TB, dal, bd, idesc128, 1u);                                        // hl += lh
+              } else {
+                mma_i8(tmem + 0, dah + 2 * ks, bd, idesc, 1u);
+                mma_i8(tmem + TB, dal + 2 * ks, bd, idesc, 1u);
+              }
+            };
+            const i64 krem = KC - (i64)kb * 128;                          // K steps past KC are zero
+            if (krem >= 128) {
+#pragma unroll
+              for (int ks = 0; ks < 4; ks++) cstep(ks);
+            } else {
+              for (int ks = 0; ks < (int)((krem + 31) / 32); ks++) cstep(ks);
+            }
+          }
+          mma_commit(&S.empty[s]);
+        }
+        for (int kb = 0; !tailTB && kb < nk; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (!mbar_wait(&S.full[s], (kbg / kStages) & 1, err)) {
             ok = false;
