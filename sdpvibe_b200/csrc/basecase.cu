@@ -1,4 +1,4 @@
-// Cholesky base case on CUDA cores (north-star item (e)): 32 x 32 tiles in wide fixed point.
+// Cholesky base case on CUDA cores: 32 x 32 tiles in wide fixed point.
 //
 // A tile entry is WL 32-bit words (two's complement) with F = 32*LF fraction bits; tiles are entry-major
 // (tiles, 32, 32, WL), the layout of sdpvibe/basecase.py.  The arithmetic is the reference's, so results

@@ -1,4 +1,4 @@
-// CRT reconstruction fused with rounding (north-star item (c)).
+// CRT reconstruction fused with rounding.
 //
 // For an entry with residues a_i (n moduli m_i, M = prod m_i, |value| < M/4):
 //   y_i = a_i (M/m_i)^-1 mod m_i  (centred),  k = round(sum y_i / m_i),

@@ -1,4 +1,4 @@
-// Residue decomposition (north-star item (a)): limb planes -> int8 hi/lo residues modulo 15-bit primes.
+// Residue decomposition: limb planes -> int8 hi/lo residues modulo 15-bit primes.
 //
 // For an entry x with bytes u_j (j < 4L, little endian, two's complement) and a modulus m:
 //   x mod m = (sum_j (u_j - 128) T_j + C1 - neg*C2) mod m,  T_j = centred 256^j mod m = 128 Thi_j + Tlo_j

@@ -1,4 +1,4 @@
-// Residue GEMM on INT8 tensor cores (north-star items (b) and (d)).
+// Residue GEMM on INT8 tensor cores (the exact products and the Gram accumulation).
 //
 // Per modulus m (and block b):  acc <- (acc + A B^T) mod m  with A = 128 Ahi + Alo, B = 128 Bhi + Blo,
 // i.e. 2^14 Ahi Bhi^T + 2^7 (Ahi Blo^T + Alo Bhi^T) + Alo Blo^T  (sdpvibe/rns.py:106-137,
