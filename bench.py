@@ -164,6 +164,18 @@ def cpu_baseline(R, threads):
             "mp_mac_per_s": mp_macs(R) / t_step}
 
 
+def max_over_ranks(ms, world, device):
+    """The slowest rank's time: every rank calls this with its own device time (one MAX all-reduce, taken by
+    all ranks in the same order); with one rank the time itself."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path, on rank 0 only."""
     if rank != 0:
@@ -285,12 +297,7 @@ def run_b200(args, rank, world, local_rank):
                 fn()
         e.record()
         barrier()
-        ms = s.elapsed_time(e)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(s.elapsed_time(e), world, dev)
 
     for _ in range(max(args.warmup, 3)):
         step()
