@@ -225,16 +225,18 @@ __global__ void __launch_bounds__(THREADS, 512 / (2 * TILE))
 }
 
 // ---------------------------------------------------------------- warp-specialised persistent variant
-// One CTA per SM, 13 warps:
-//   warps 0-3  loaders: 4-byte cp.async of the next tiles' limb planes into a raw ring (kRawStages),
-//              then the transform into a double-buffered K-major entry tile (xb[2]);
+// One CTA per SM, 6 + RW warps (RW = 8 reducer warps, or 16):
+//   warps 0-3  loaders: the next tiles' limb planes into a raw ring (RAW stages) -- one 3-D TMA copy per
+//              tile (MODE 2) or per-thread 16- / 4-byte cp.async (MODE 0) -- then the transform into a
+//              double-buffered K-major entry tile (xb[2]); in MODE 1 one thread streams operand rows by TMA;
 //   warp 4     MMA issuer (one lane): D_lo / D_hi of a 128-entry tile into one of two TMEM buffers;
-//   warps 5-12 reducers: TMEM lane quarter = warp % 4, 64 entries each; exact residue, digit split, staging
-//              of the residue tile (or direct stores where bulk stores cannot be used);
-//   warp 13    store warp (one lane): the bulk tensor stores of each staged tile, releasing its staging buffer
-//              once read (stg_full: reducer arrivals, stg_empty: the store lane).
-// mbarriers: xb_full (128 loader arrivals), xb_empty (MMA commit), tm_full (MMA commit),
-// tm_empty (256 reducer arrivals).  Every wait is bounded; a timeout aborts all roles.
+//   warps 5..  reducers: TMEM lane quarter = warp % 4, 128 / (RW / 4) entries each; exact residue, digit
+//              split, staging of the residue tile (or direct stores where bulk stores cannot be used);
+//   last warp  store warp (one lane): the bulk tensor stores of each staged tile, releasing its staging
+//              buffer once read (stg_full: reducer arrivals, stg_empty: the store lane).
+// mbarriers: xb_full (loader arrivals, or the TMA bytes in MODE 1), xb_empty (MMA commit), tm_full (MMA
+// commit), tm_empty (reducer arrivals), raw_full (TMA bytes, MODE 2).  Every wait is bounded; a timeout
+// aborts all roles.
 constexpr int WS_TILE = 128, WS_LOADERS = 128;
 // RW reducer warps (8 or 16): RW / 4 per TMEM lane quarter, 128 / (RW / 4) columns each
 template <int RW>
