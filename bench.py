@@ -49,8 +49,8 @@ def workload_shape(seed=0):
     return m, rows
 
 
-def gen_chunk(rng, rows, cols, L):
-    """Normalised MPF (rows, cols): |mantissa| has exactly 32L-2 bits, random sign, e ~ U[-8, 8]."""
+def gen_chunk(rng, rows, cols, L, elo=-8, ehi=8):
+    """Normalised MPF (rows, cols): |mantissa| has exactly 32L-2 bits, random sign, e ~ U[elo, ehi]."""
     n = rows * cols
     mag = rng.integers(0, 1 << 32, size=(L, n), dtype=np.uint64).astype(np.uint32)
     mag[L - 1] = (mag[L - 1] & np.uint32((1 << 29) - 1)) | np.uint32(1 << 29)
@@ -62,7 +62,7 @@ def gen_chunk(rng, rows, cols, L):
         v = m[k].astype(np.uint64) + carry
         m[k] = v.astype(np.uint32)
         carry = carry & (v > 0xffffffff)
-    e = rng.integers(-8, 9, size=n).astype(np.int64)
+    e = rng.integers(elo, ehi + 1, size=n).astype(np.int64)
     return m.view(np.int32).reshape(L, rows, cols), e.reshape(rows, cols)
 
 
@@ -365,9 +365,141 @@ def run_b200(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline(R, os.cpu_count() or 1)
     if world == 1 and not args.no_solver:
         # the metric's other half: SDPB iterations of the 768-bit Ising-structured SDP on the same GPU
-        sv = solver_measurement(5, 1, local_rank)
+        sv = solver_measurement(local_rank)
         line["sdp_solver"] = {k: sv[k] for k in ("metric", "value", "unit", "steps", "warmup", "per_iteration_s",
+                                                  "metric_over", "steady_state_s_per_iter",
                                                   "config", "kernel_s_per_iter", "gpu_launches", "clocks")}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ multiprecision GEMM workload (mp-GEMM 256^3)
+G_N, G_L, G_MODS, G_E = 256, 24, 112, 216        # 768 bits: 112 moduli, 216 CRT bytes (tables of L = 24)
+
+
+def gemm_ops(n=G_N):
+    return G_MODS * 4 * 2 * n ** 3
+
+
+def gemm_cpu_baseline(threads):
+    """cpu_baseline/mpf_baseline.c's gemm line at 768 bits, n = 256 (GMP mpf, all threads): the reference's
+    CPU comparison for this configuration, one full GEMM (about a second of CPU work)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "mpf_baseline")
+    if not os.path.exists(exe):
+        from oracle import ref_build
+        ref_build.build_cpu_baseline()
+    if not os.path.exists(exe):
+        return None
+    out = subprocess.run([exe, "768", str(G_N), str(G_N), str(threads)], capture_output=True, text=True,
+                         timeout=600).stdout
+    for line in out.splitlines():
+        if line.strip().startswith("gemm"):
+            t = float(line.split()[1])
+            return {"value": gemm_ops() / t / 1e12, "unit": "TOPS", "cores": threads, "kind": "reference",
+                    "sample": f"cpu_baseline/mpf_baseline.c gemm {G_N}^3 at 768 bits (GMP mpf, {threads} threads), "
+                              "the whole workload", "s_per_step": t, "mp_mac_per_s": G_N ** 3 / t}
+    return None
+
+
+def run_gemm(args, rank, world, local_rank):
+    """C = A B with A, B 256 x 256 MPF at 768 bits (L = 24; NB-bit mantissas, random sign, exponents
+    U[-4, 4], numpy seed 0): sdpvibe_b200.mpf.gemm (sdpvibe/mpf.py:401-452).  Metric: residue-GEMM INT8
+    TOPS counted the reference's way (112 moduli x 4 digit products x 2 M N K) per GEMM.  The inputs (2 x 6.3
+    MB) fit in L2, so L2 is flushed (a 256 MB write) before every timed step, outside its CUDA events."""
+    import torch
+    from sdpvibe_b200 import mpf, _trace
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(0)
+    am, ae = gen_chunk(rng, G_N, G_N, G_L, -4, 4)
+    bm, be = gen_chunk(rng, G_N, G_N, G_L, -4, 4)
+    A = mpf.MPF(torch.from_numpy(am).to(dev), torch.from_numpy(ae).to(dev))
+    B = mpf.MPF(torch.from_numpy(bm).to(dev), torch.from_numpy(be).to(dev))
+    pinned = [torch.from_numpy(x).pin_memory() for x in (am, ae, bm, be)]
+    h2d = sum(t.numel() * t.element_size() for t in pinned)
+    out_m = torch.empty((G_L, G_N, G_N), dtype=torch.int32).pin_memory()
+    out_e = torch.empty((G_N, G_N), dtype=torch.int64).pin_memory()
+    d2h = out_m.numel() * 4 + out_e.numel() * 8
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        return mpf.gemm(A, B)
+
+    def step_e2e():
+        dm = [t.to(dev, non_blocking=True) for t in pinned]
+        C = mpf.gemm(mpf.MPF(dm[0], dm[1]), mpf.MPF(dm[2], dm[3]))
+        out_m.copy_(C.m, non_blocking=True)
+        out_e.copy_(C.e, non_blocking=True)
+
+    def timed(fn, k, trace=None):
+        total = 0.0
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            if trace is not None:
+                with trace:
+                    fn()
+            else:
+                fn()
+            e.record()
+            torch.cuda.synchronize()
+            total += s.elapsed_time(e)
+        return max_over_ranks(total, world, dev)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+        step_e2e()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(step, args.steps)
+    tr = _trace.Trace(timed={"sdpv_rns_gemm", "sdpv_residues_u8", "sdpv_crt_norm", "sdpv_align", "sdpv_top_max"})
+    ms_traced = timed(step, args.steps, tr)
+    ms_e2e = timed(step_e2e, args.steps)
+    if rank != 0:
+        return
+    hbm, bf16, src = load_peaks()
+    t_step = ms / args.steps * 1e-3
+    gemm_ms = statistics.mean(tr.kernel_ms("sdpv_rns_gemm"))
+    res_ms = statistics.mean(tr.kernel_ms("sdpv_residues_u8"))
+    crt_ms = statistics.mean(tr.kernel_ms("sdpv_crt_norm"))
+    ent = G_N * G_N
+    res_bytes = ent * (4 * G_L + 2 * G_MODS)                 # one operand: limb bytes in, residues out
+    crt_bytes = ent * (2 * G_MODS + 4 * G_L + 8)             # residues in, MPF limbs + exponents out
+    crt_ops = 2 * G_E * G_MODS * ent                         # the CRT digit product on the tensor cores
+    peak = 2 * bf16
+    line = {
+        "metric": METRIC, "value": world * gemm_ops() / t_step / 1e12, "unit": "TOPS", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8 (exact int8 x int8 -> int32 residue products)",
+        "data": "synthetic",
+        "config": {"workload": "mp-GEMM: C = A B, A and B 256 x 256 MPF at 768 bits (L=24, NB-bit mantissas, random "
+                               "sign, exponents U[-4,4], numpy seed 0), sdpvibe_b200.mpf.gemm, output bit-exact",
+                   "l2": "flushed (256 MB write) before every timed step, outside its events",
+                   "ops_per_step": gemm_ops(), "mp_mac_per_step": G_N ** 3},
+        "mp_mac_per_s": world * G_N ** 3 / t_step,
+        "roofline": {"bound": "tensor", "kernel": "sdpv_rns_gemm (tcgen05 kind::i8)",
+                     "achieved": gemm_ops() / (gemm_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": gemm_ops() / (gemm_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                     "peak_source": f"2 x bf16_tflops of {src} (MEASURED_PEAKS.json): B200 dense int8 = 2 x dense bf16",
+                     "launch_ms_mean": gemm_ms, "ops_per_launch": gemm_ops()},
+        "roofline_decomposition": {"bound": "hbm", "kernel": "sdpv_residues_u8", "unit": "GB/s", "peak": hbm,
+                                   "achieved": res_bytes / (res_ms * 1e-3) / 1e9,
+                                   "frac": res_bytes / (res_ms * 1e-3) / 1e9 / hbm, "launch_ms_mean": res_ms,
+                                   "bytes_per_launch": res_bytes},
+        "roofline_crt": {"bound": "hbm", "kernel": "sdpv_crt_norm (CRT digit product on tcgen05 + renormalisation)",
+                         "unit": "GB/s", "peak": hbm, "achieved": crt_bytes / (crt_ms * 1e-3) / 1e9,
+                         "frac": crt_bytes / (crt_ms * 1e-3) / 1e9 / hbm, "launch_ms_mean": crt_ms,
+                         "bytes_per_launch": crt_bytes, "tensor_tops": crt_ops / (crt_ms * 1e-3) / 1e12,
+                         "tensor_frac": crt_ops / (crt_ms * 1e-3) / 1e12 / peak},
+        "kernel_ms_per_step": {k: sum(tr.kernel_ms(k)) / args.steps for k in sorted(tr.timed) if tr.kernel_ms(k)},
+        "ms_per_step_traced": ms_traced / args.steps,
+        "e2e": {"value": world * gemm_ops() / (ms_e2e / args.steps * 1e-3) / 1e12, "unit": "TOPS",
+                "ms_per_step": ms_e2e / args.steps, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": tr.total_launches, "gpu_launches_per_step": tr.total_launches // args.steps,
+        "launches_by_entry": dict(tr.launches), "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = gemm_cpu_baseline(os.cpu_count() or 1)
     print(json.dumps(line), flush=True)
 
 
@@ -590,11 +722,15 @@ def run_sensitivity(args, rank, world, local_rank):
 
 
 # ------------------------------------------------------------------ full solver iterations (SDP s/iter)
+SOLVER_ITERS = 20
+
+
 def run_solver(args, rank, world, local_rank):
     """SDPB iterations on the Ising-structured synthetic SDP: 300 blocks (dims 1/2/3 = 180/90/30,
     degree d ~ U[20,40], K = d+1), N = 1000, L = 26 (the 768-bit precision rule).  A step is one
-    iteration; `--warmup` first iterations are excluded; metric s/iteration (lower is better)."""
-    line = solver_measurement(args.steps, args.warmup, local_rank, world)
+    iteration; the configuration's first 20 iterations run and the metric is the mean s/iteration of
+    iterations 2-20 (lower is better)."""
+    line = solver_measurement(local_rank, world)
     if args.precision_iters > 0:
         line["error_vs_2x_precision"] = solver_precision_check(args.precision_iters)
     if rank == 0:
@@ -638,7 +774,10 @@ def solver_precision_check(iters):
             "per_iteration": per_it, "y_rel_last": _rel_mpf_error(runs[26][1], runs[50][1])}
 
 
-def solver_measurement(steps, warmup, local_rank, world=1):
+def solver_measurement(local_rank, world=1, iters=SOLVER_ITERS):
+    """The configuration's run: the first `iters` (20) iterations from the start; the metric is the mean of
+    iterations 2 .. iters (the first records the CUDA graphs).  Also reported: the mean of iterations 4 ..
+    iters (after the chunk streams' memory pools are filled)."""
     import torch
     import mpmath as mp
     from sdpvibe_b200 import _trace
@@ -653,14 +792,15 @@ def solver_measurement(steps, warmup, local_rank, world=1):
     sol = Solver(sdp, Ls, timing=True)
     marks = []
 
-    warm = max(warmup, 3)                       # 1 records the graphs, 2-3 fill the chunk streams' pools
-    total_it = warm + steps
+    warm = 1                                    # iteration 1 records the graphs
+    steps = iters - warm
+    total_it = iters
 
     def rec(it, s, info):
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
         marks.append((it, ev, info["row"]))
-        if it == warm:                          # phase and kernel tables over the timed iterations only
+        if it == warm:                          # phase and kernel tables over iterations 2 .. iters only
             s.timer.marks.clear()
             tr.launches.clear()
             tr.events.clear()
@@ -679,6 +819,7 @@ def solver_measurement(steps, warmup, local_rank, world=1):
     per_it = [ev[i].elapsed_time(ev[i + 1]) * 1e-3 for i in range(len(ev) - 1)]
     timed = per_it[warm:]
     s_it = statistics.mean(timed)
+    steady = statistics.mean(per_it[3:]) if len(per_it) > 3 else s_it
     last = marks[-1][2]
     line = {"metric": "768-bit SDP s/iter (Ising-structured synthetic SDP, 300 blocks, N=1000)",
             "value": s_it, "unit": "s/iter", "n_gpus": world, "steps": len(timed), "warmup": warm,
@@ -691,6 +832,8 @@ def solver_measurement(steps, warmup, local_rank, world=1):
                        "chunks": [dict(dim=g.dim, nb=g.nb, K=g.K, h=g.h[0], P=g.P) for g in sdp.groups],
                        "l2": "working set of several GB; no flush"},
             "per_iteration_s": per_it, "build_s": t_build,
+            "iterations": len(per_it), "metric_over": f"mean of iterations 2..{len(per_it)}",
+            "steady_state_s_per_iter": steady, "steady_state_over": f"mean of iterations 4..{len(per_it)}",
             "last_row": {k: (mp.nstr(v, 6) if isinstance(v, mp.mpf) else v) for k, v in last.items()},
             "tables_over": f"the {steps} timed iterations (plus the residue phase of the final evaluation)",
             "phase_s_per_iter": {k: v / steps for k, v in sol.timer.totals().items()},
@@ -713,9 +856,9 @@ def main():
     ap.add_argument("--precision-iters", type=int, default=6,
                     help="solver / cholsolve: iterations (solver) compared with a run at twice the precision; 0 skips")
     ap.add_argument("--no-solver", action="store_true", help="gram: skip the SDP s/iteration measurement")
-    ap.add_argument("--workload", choices=("gram", "cholsolve", "solver", "sensitivity"), default="gram",
-                    help="gram: the residue Gram step (default); cholsolve: batched Cholesky + solve; "
-                         "solver: SDPB iterations (s/iter)")
+    ap.add_argument("--workload", choices=("gram", "gemm", "cholsolve", "solver", "sensitivity"), default="gram",
+                    help="gram: the residue Gram step (default); gemm: the mp-GEMM 256^3 at 768 bits; cholsolve: "
+                         "batched Cholesky + solve; solver: SDPB iterations (s/iter)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -729,7 +872,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run = {"gram": run_b200, "cholsolve": run_cholsolve, "solver": run_solver,
+        run = {"gram": run_b200, "gemm": run_gemm, "cholsolve": run_cholsolve, "solver": run_solver,
                "sensitivity": run_sensitivity}[args.workload]
         run(args, rank, world, local_rank)
     finally:

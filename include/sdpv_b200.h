@@ -246,13 +246,16 @@ int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* V, int64
 
 /* Allocation-free sdpv_trinv_tiles, for callers that cannot allocate device memory at the point of the call
  * (their process has handed all device memory to another allocator, or the calling code must not allocate).
- * No counterpart in the reference.  The product scratch is a fixed 16 MiB array inside the library image
- * (4 Mi 32-bit words, reserved on every device that loads the library until exit), so the call allocates
- * nothing: it needs ntiles * 32 * 32 * WL <= 4 Mi words and returns SDPV_EINVAL beyond that.  The first
- * call on a device looks up the array's device address; make that first call before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU (different streams, no ordering)
- * race on it.  Nothing in the array needs to start at zero; every word a call reads was written earlier
- * in the same call. */
+ * No counterpart in the reference.  For WL <= 64 the inverse runs in shared memory and uses no scratch, at
+ * any ntiles.  For WL > 64 the product scratch is a fixed 16 MiB array inside the library image (4 Mi 32-bit
+ * words): the call needs ntiles * 32 * 32 * WL <= 4 Mi words and returns SDPV_EINVAL beyond that.  The array
+ * is held on a device from the moment the library's tile module is loaded there -- with lazy module loading
+ * (the CUDA 12 default) at the first call of any tile entry point (sdpv_chol_tiles, sdpv_trinv_tiles,
+ * sdpv_trsv_tiles, this one) on that device -- until the process exits; make that first call before handing
+ * device memory to another allocator, and before any stream capture (it also looks up the array's device
+ * address).  All calls on a device share the array: calls with WL > 64 that overlap on the GPU (different
+ * streams, no ordering) race on it.  Nothing in the array needs to start at zero; every word a call reads was
+ * written earlier in the same call. */
 int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, int64_t ntiles, int bt, int WL,
                              int LF, void* stream);
 
@@ -260,6 +263,18 @@ int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV, uint32_t*
  * Read and clear the device error word (bits SDPV_ERRBIT_*) after synchronising `stream`.
  * Replaces limbops.check_errors (sdpvibe/limbops.py:156-169). */
 int sdpv_get_error(unsigned* flags_host, void* stream);
+
+/* Synchronise `stream`, read and clear the device error word, and return it as a status: SDPV_ETIMEOUT when a
+ * bounded device wait gave up, else SDPV_ENOTSPD, else SDPV_EOVERFLOW, else SDPV_OK.  The status form of
+ * limbops.check_errors (sdpvibe/limbops.py:156-169) that also reports the pipelines' wait timeouts. */
+int sdpv_device_status(void* stream);
+
+/* Launch one warp that waits on a shared-memory barrier with the pipelines' bounded wait, its limit shortened
+ * to limit_us microseconds (1 .. 2e6).  arrive != 0: the barrier completes and the wait returns at once;
+ * arrive == 0: nothing completes it, so the wait gives up after limit_us, sets SDPV_ERRBIT_TIMEOUT and the
+ * kernel returns (the context stays usable); sdpv_device_status then reports SDPV_ETIMEOUT.  Exercises the
+ * timeout path of every pipeline wait.  No counterpart in the reference (its kernels have no bounded waits). */
+int sdpv_wait_probe(unsigned limit_us, int arrive, void* stream);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,8 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <unistd.h>
 
 typedef uint32_t u32;
 typedef uint64_t u64;
@@ -286,32 +288,67 @@ void or_mpf_norm(int L, int LI, i64 n, const int32_t* X, const i64* eI, int32_t*
 
 /* Residues of X[:, :, k0:k0+kc] (L, rows, ld) modulo mods[0..G), centred to (-m/2, m/2] and split
  * r = 128*hi + lo, lo in [-64, 64); columns kc <= k < kp are residues of zero: rns.py:66-103,196-214. */
+struct res_job {
+  const int32_t* X;
+  int L, G, nthr, t;
+  i64 rows, ld, k0, kc, kp;
+  const int32_t* mods;
+  int8_t *Rhi, *Rlo;
+};
+
+/* Moduli t, t + nthr, ... of one or_residues call.  Per row, Horner over the limbs (most significant first,
+ * the top limb signed) on all kc entries of the row at once, so each limb row is read sequentially.
+ * |r| < m < 2^15 and 2^32 mod m < 2^15, so r * w32 + v stays inside int64 and one remainder per limb
+ * suffices. */
+static void* res_worker(void* arg) {
+  const struct res_job* J = (const struct res_job*)arg;
+  i64 plane = J->rows * J->ld, kc = J->kc, kp = J->kp;
+  i64* r = (i64*)malloc(sizeof(i64) * (size_t)(kc > 0 ? kc : 1));
+  for (int g = J->t; g < J->G; g += J->nthr) {
+    i64 m = J->mods[g];
+    i64 w32 = (i64)(((u64)1 << 32) % (u64)m); /* 2^32 mod m */
+    for (i64 i = 0; i < J->rows; i++) {
+      for (i64 k = 0; k < kc; k++) r[k] = 0;
+      for (int l = J->L - 1; l >= 0; l--) {
+        const int32_t* x = J->X + l * plane + i * J->ld + J->k0;
+        if (l == J->L - 1)
+          for (i64 k = 0; k < kc; k++) r[k] = (r[k] * w32 + (i64)x[k]) % m;
+        else
+          for (i64 k = 0; k < kc; k++) r[k] = (r[k] * w32 + (i64)(u32)x[k]) % m;
+      }
+      for (i64 k = 0; k < kp; k++) {
+        i64 v = 0;
+        if (k < kc) {
+          v = r[k];
+          if (v < 0) v += m;
+        }
+        if (v > m / 2) v -= m;
+        i64 lo = ((v + 64) & 127) - 64;
+        i64 hi = (v - lo) >> 7;
+        i64 o = ((i64)g * J->rows + i) * kp + k;
+        J->Rhi[o] = (int8_t)hi;
+        J->Rlo[o] = (int8_t)lo;
+      }
+    }
+  }
+  free(r);
+  return NULL;
+}
+
 void or_residues(const int32_t* X, int L, i64 rows, i64 ld, i64 k0, i64 kc, i64 kp, const int32_t* mods, int G,
                  int8_t* Rhi, int8_t* Rlo) {
-  i64 plane = rows * ld;
-  for (int g = 0; g < G; g++) {
-    i64 m = mods[g];
-    i64 w32 = (i64)(((u64)1 << 32) % (u64)m); /* 2^32 mod m */
-    for (i64 i = 0; i < rows; i++)
-      for (i64 k = 0; k < kp; k++) {
-        i64 r = 0;
-        if (k < kc) {
-          /* Horner over limbs, most significant first; the top limb is signed. */
-          for (int l = L - 1; l >= 0; l--) {
-            int32_t x = X[l * plane + i * ld + k0 + k];
-            i64 v = (l == L - 1) ? (i64)x : (i64)(u32)x;
-            r = ((r * w32) % m + v % m) % m;
-          }
-          if (r < 0) r += m;
-        }
-        if (r > m / 2) r -= m;
-        i64 lo = ((r + 64) & 127) - 64;
-        i64 hi = (r - lo) >> 7;
-        i64 o = ((i64)g * rows + i) * kp + k;
-        Rhi[o] = (int8_t)hi;
-        Rlo[o] = (int8_t)lo;
-      }
+  long nc = sysconf(_SC_NPROCESSORS_ONLN);
+  int nthr = (int)(nc < 1 ? 1 : (nc > 64 ? 64 : nc));
+  if (nthr > G) nthr = G > 0 ? G : 1;
+  if (rows * kc < 4096) nthr = 1;
+  struct res_job J[64];
+  pthread_t th[64];
+  for (int t = 0; t < nthr; t++) {
+    J[t] = (struct res_job){X, L, G, nthr, t, rows, ld, k0, kc, kp, mods, Rhi, Rlo};
+    if (t > 0) pthread_create(&th[t], NULL, res_worker, &J[t]);
   }
+  res_worker(&J[0]);
+  for (int t = 1; t < nthr; t++) pthread_join(th[t], NULL);
 }
 
 /* acc[g] <- (acc[g] + Ahi_g (2^14 Bhi_g^T) + 2^7 (Ahi_g Blo_g^T + Alo_g Bhi_g^T) + Alo_g Blo_g^T) mod m_g,

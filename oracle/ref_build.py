@@ -23,13 +23,17 @@ import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = os.environ.get("SDPV_REFERENCE_ROOT", "/root/reference")
+# The reference tree is named by SDPV_REFERENCE_ROOT (no default): without it the checkers that need the
+# reference's sources are not built, and extract_src refuses with a message.
+REFERENCE_ROOT = os.environ.get("SDPV_REFERENCE_ROOT")
 
 _KERNEL_RE = re.compile(r'extern\s+"C"\s+__global__\s+void\s+(\w+)\s*\(([^)]*)\)', re.S)
 
 
 def extract_src(relpath, name="_SRC"):
     """Return the string literal assigned to `name` in a reference module (parsed, not imported)."""
+    if not REFERENCE_ROOT:
+        raise RuntimeError("set SDPV_REFERENCE_ROOT to the reference (SDPviBe) source tree")
     path = os.path.join(REFERENCE_ROOT, relpath)
     tree = ast.parse(open(path).read(), path)
     for node in tree.body:
@@ -159,7 +163,7 @@ def prebuilt_path(kind, *key):
 
 def build_prebuilt():
     """Compile the reference kernels for the limb counts the tests use (needs the reference tree)."""
-    if not os.path.isdir(REFERENCE_ROOT):
+    if not REFERENCE_ROOT or not os.path.isdir(REFERENCE_ROOT):
         return False
     os.makedirs(REF_OUT, exist_ok=True)
     for L in PREBUILT_MPF_L:
@@ -188,8 +192,8 @@ MPF_BASELINE = os.path.join(REF_OUT, "mpf_baseline")
 def build_cpu_baseline():
     """cpu_baseline/mpf_baseline.c (GMP mpf + OpenMP, the reference's CPU comparison) compiled where it
     lies, as the reference documents: gcc -O2 -fopenmp mpf_baseline.c -l:libgmp.so.10 -lm."""
-    src = os.path.join(REFERENCE_ROOT, "cpu_baseline", "mpf_baseline.c")
-    if not os.path.exists(src):
+    src = os.path.join(REFERENCE_ROOT, "cpu_baseline", "mpf_baseline.c") if REFERENCE_ROOT else ""
+    if not src or not os.path.exists(src):
         return os.path.exists(MPF_BASELINE)
     os.makedirs(REF_OUT, exist_ok=True)
     if os.path.exists(MPF_BASELINE) and os.path.getmtime(MPF_BASELINE) >= os.path.getmtime(src):

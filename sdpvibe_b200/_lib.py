@@ -59,6 +59,8 @@ _SIGS = {
     "sdpv_trsv_tiles": [_P, _P, _P, _L, _I, _I, _I, _P],
     "sdpv_eig_sym_f64": [_P, _L, _I, _P, _P, _P, _P],
     "sdpv_get_error": [ctypes.POINTER(ctypes.c_uint), _P],
+    "sdpv_device_status": [_P],
+    "sdpv_wait_probe": [ctypes.c_uint, _I, _P],
 }
 
 _lib = None
@@ -149,6 +151,13 @@ def call(name, *args):
     check(getattr(lib(), name)(*args), name)
     if end is not None:
         end.record()
+
+
+def device_status():
+    """Synchronise the current stream and raise what the device error word holds (and clear it):
+    RuntimeError for a bounded wait that timed out, ValueError for a non-positive pivot, OverflowError
+    for a rounding overflow."""
+    check(lib().sdpv_device_status(stream()), "device status")
 
 
 def device_error_flags():

@@ -782,9 +782,13 @@ extern "C" int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32
 // ---------------------------------------------------------------- allocation-free variant of sdpv_trinv_tiles
 // Some callers cannot allocate device memory when they need the inverse: their process has already handed
 // all device memory to another allocator (a framework's caching pool or a fixed memory budget), or they
-// call from code that must not allocate.  This variant takes its product scratch from a fixed array that is
-// part of the library image: SDPV_TRINV_NOALLOC_WORDS 32-bit words (16 MiB), reserved on every device that
-// loads the library until the process exits.  A call needs ntiles * 32 * 32 * WL words of it.
+// call from code that must not allocate.  For WL <= FW the inverse runs in shared memory and needs no
+// scratch at all.  For WL > FW this variant takes the product scratch from a fixed array that is part of
+// the library image: SDPV_TRINV_NOALLOC_WORDS 32-bit words (16 MiB), held on every device that loads the
+// library's tile module until the process exits.  With lazy module loading (the CUDA 12 default) the module,
+// and so the array, is loaded on a device by the first call of any tile entry point there; a caller that
+// will hand its device memory away makes one such call first.  A call with WL > FW needs
+// ntiles * 32 * 32 * WL words of the array.
 #define SDPV_TRINV_NOALLOC_WORDS (4u << 20)
 static __device__ __align__(256) uint32_t g_trinv_scratch[SDPV_TRINV_NOALLOC_WORDS];
 
@@ -815,6 +819,13 @@ extern "C" int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV
                                         int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
+  if (WL <= FW) {                                   // shared-memory kernel: no scratch, no size limit
+    int st = smem_attributes();
+    if (st != SDPV_OK) return st;
+    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+        Lt, RINV, X, WL, LF);
+    return sdpv::launch_status();
+  }
   if ((uint64_t)ntiles * BT * BT * (uint64_t)WL > SDPV_TRINV_NOALLOC_WORDS) {
     sdpv::set_message("sdpv_trinv_tiles_noalloc: ntiles * 32 * 32 * WL exceeds the fixed scratch of 4 Mi words");
     return SDPV_EINVAL;

@@ -90,16 +90,21 @@ __device__ __forceinline__ u64 globaltimer_ns() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait for the given phase parity; on give-up sets the timeout bit and returns false.
-__device__ __forceinline__ bool mbar_wait(u64* bar, u32 phase, unsigned* err) {
+// Bounded wait for the given phase parity; after limit_ns of wall-clock time it gives up, sets the
+// timeout bit and returns false.
+__device__ __forceinline__ bool mbar_wait_ns(u64* bar, u32 phase, unsigned* err, u64 limit_ns) {
   if (mbar_try_wait(bar, phase)) return true;
   const u64 t0 = globaltimer_ns();
   for (u32 it = 1;; it++) {
     if (mbar_try_wait(bar, phase)) return true;
-    if ((it & 1023u) == 0 && globaltimer_ns() - t0 > SDPV_WAIT_NS) break;
+    if ((it & 1023u) == 0 && globaltimer_ns() - t0 > limit_ns) break;
   }
   atomicOr(err, SDPV_ERRBIT_TIMEOUT);
   return false;
+}
+// The pipelines' wait: gives up after SDPV_WAIT_NS.
+__device__ __forceinline__ bool mbar_wait(u64* bar, u32 phase, unsigned* err) {
+  return mbar_wait_ns(bar, phase, err, SDPV_WAIT_NS);
 }
 
 __device__ __forceinline__ void fence_proxy_async_smem() {

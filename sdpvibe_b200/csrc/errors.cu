@@ -68,3 +68,38 @@ extern "C" int sdpv_get_error(unsigned* flags_host, void* stream) {
   *flags_host = v;
   return SDPV_OK;
 }
+
+extern "C" int sdpv_device_status(void* stream) {
+  unsigned v = 0;
+  int st = sdpv_get_error(&v, stream);
+  if (st != SDPV_OK) return st;
+  if (v & SDPV_ERRBIT_TIMEOUT) return SDPV_ETIMEOUT;
+  if (v & SDPV_ERRBIT_NOTSPD) return SDPV_ENOTSPD;
+  if (v & SDPV_ERRBIT_OVERFLOW) return SDPV_EOVERFLOW;
+  return SDPV_OK;
+}
+
+namespace {
+// One warp waits on a shared-memory mbarrier expecting one arrival, with the pipelines' bounded wait
+// shortened to limit_ns.  With arrive set lane 0 arrives first and the wait succeeds at once; without it
+// nothing ever arrives, the wait gives up after limit_ns, sets the timeout bit and the kernel returns.
+__global__ void wait_probe_kernel(u64 limit_ns, int arrive, unsigned* err) {
+  __shared__ __align__(8) u64 bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  if (arrive && threadIdx.x == 0) mbar_arrive(&bar);
+  __syncwarp();
+  if (threadIdx.x == 0) mbar_wait_ns(&bar, 0, err, limit_ns);
+}
+}  // namespace
+
+extern "C" int sdpv_wait_probe(unsigned limit_us, int arrive, void* stream) {
+  if (limit_us == 0 || limit_us > 2000000u) return SDPV_EINVAL;
+  unsigned* err = sdpv::device_error_word();
+  if (!err) return SDPV_ECUDA;
+  wait_probe_kernel<<<1, 32, 0, sdpv::as_stream(stream)>>>((u64)limit_us * 1000ull, arrive, err);
+  return sdpv::launch_status();
+}

@@ -19,7 +19,9 @@ import sys
 os.environ["TRITON_INTERPRET"] = "1"
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_ROOT = os.environ.get("SDPV_REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("SDPV_REFERENCE_ROOT")
+if not REFERENCE_ROOT or not os.path.isdir(os.path.join(REFERENCE_ROOT, "sdpvibe")):
+    raise RuntimeError("set SDPV_REFERENCE_ROOT to the reference (SDPviBe) source tree to generate golden vectors")
 sys.path.insert(0, REPO)
 sys.path.insert(0, REFERENCE_ROOT)
 
