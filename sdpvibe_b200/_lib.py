@@ -59,6 +59,14 @@ _SIGS = {
     "sdpv_trsv_tiles": [_P, _P, _P, _L, _I, _I, _I, _P],
     "sdpv_eig_sym_f64": [_P, _L, _I, _P, _P, _P, _P],
     "sdpv_get_error": [ctypes.POINTER(ctypes.c_uint), _P],
+    "sdpv_rns_gemm_grouped": [_P, _P, _P, _L, _L, _P, _P, _L, _L, _L, _I, _I, _P, _L, _P, _L, _L, _I, _I, _P],
+    "sdpv_grp_copy": [_P, _P, _I, _P, _L, _I, _P, _L, _P],
+    "sdpv_grp_finish_fixed": [_P, _I, _L, _L, _P, _P, _I, _I, _P, _P, _L, _P],
+    "sdpv_grp_colexp": [_P, _L, _P, _L, _I, _P, _P, _L, _P, _P, _P],
+    "sdpv_grp_solve_finish": [_P, _I, _L, _L, _P, _L, _P, _L, _I, _P, _P, _P, _L, _P],
+    "sdpv_grp_merge": [_P, _L, _P, _L, _I, _P, _L, _P],
+    "sdpv_grp_tile_widen": [_P, _L, _I, _L, _I, _I, _P, _L, _P, _P],
+    "sdpv_grp_tile_narrow": [_P, _P, _I, _I, _P, _L, _I, _L, _P, _P, _L, _P, _P, _L, _P],
     "sdpv_device_status": [_P],
     "sdpv_wait_probe": [ctypes.c_uint, _I, _P],
 }

@@ -121,7 +121,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     int nfull, int ftail, int tfirst, int nmode, int nTB, int u8ops,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
-                    i64 tiles, i64 nitems, bool fresh, int pack, unsigned* __restrict__ err) {
+                    i64 tiles, i64 nitems, bool fresh, int pack, const int32_t* __restrict__ gtab,
+                    unsigned* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   GemmSmem& S = *reinterpret_cast<GemmSmem*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -161,11 +162,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x) {
         const i64 t = item % tiles, bg = item / tiles;
         int b, g, m0, n0;
+        int nki = nk;                             // K blocks of this item
         if (tailTB || nmode) {                    // syrk tail / narrow: big-side row block t against TB rows
           b = (int)(bg % nb);
           g = gofs + (int)(bg / nb);
           m0 = (int)(t + tfirst) * 128;
           n0 = tailTB ? nfull : 0;
+          if (gtab) {                             // grouped: the item's rows and K length from its table row
+            const int32_t* it = gtab + 8 * t;
+            m0 = it[0];
+            n0 = it[2];
+            nki = (it[4] + 127) / 128;
+          }
         } else if (pack > 1) {                    // packed: tile t holds blocks t*pack .. (rows stacked)
           b = 0;
           g = gofs + (int)bg;
@@ -199,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           continue;
         }
-        for (int kb = 0; kb < nk; kb++, kbg++) {
+        for (int kb = 0; kb < nki; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
             *(volatile int*)&S.abort = 1;
@@ -247,7 +255,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_after();
         const u32 tb = tmem + buf * 256;
         bool ok = true;
-        for (int kb = 0; kb < nk; kb++, kbg++) {
+        int nki = nk;
+        i64 klen = KC;
+        if (gtab) {
+          klen = gtab[8 * (item % tiles) + 4];
+          nki = (int)((klen + 127) / 128);
+        }
+        for (int kb = 0; kb < nki; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (!mbar_wait(&S.full[s], (kbg / kStages) & 1, err)) {
             ok = false;
@@ -267,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               mma_i8(tb + TB, dal + 2 * ks, bd, idesc, 1u);
             }
           };
-          const i64 krem = KC - kb * 128;                                 // K steps past KC are zero
+          const i64 krem = klen - kb * 128;                               // K steps past the item's K are zero
           if (krem >= 128) {
 #pragma unroll
             for (int ks = 0; ks < 4; ks++) step(ks);
@@ -412,10 +426,21 @@ __global__ void __launch_bounds__(kThreads, 1)
       const float minv = S.tminv[g];
       const u32 buf = li & 1;
       const int TB = nTB, half = nTB >> 1;
-      const i64 r = t * 128 + q * 32 + lane;
-      const i64 big = nmode == 1 ? M : N, small = nmode == 1 ? N : M;
-      const i64 rowA = (i64)gg * nb * M + (i64)b * M;                  // acc row of block row 0
-      int16_t* bp = nmode == 1 ? acc + (rowA + r) * ldc : acc + rowA * ldc + r;
+      i64 r = t * 128 + q * 32 + lane;
+      i64 big = nmode == 1 ? M : N, small = nmode == 1 ? N : M;
+      i64 rowA = (i64)gg * nb * M + (i64)b * M;                        // acc row of block row 0
+      i64 col0 = 0;
+      if (gtab) {
+        // grouped: big-side rows r < it[1] of the item against small-side rows j < it[3]; nmode 1 stores
+        // C[out_row0 + r][j], nmode 2 C[out_row0 + j][out_col0 + r] (acc planes of M rows per modulus)
+        const int32_t* it = gtab + 8 * t;
+        r = q * 32 + lane;
+        big = it[1];
+        small = it[3];
+        rowA = (i64)gg * M + it[5];
+        col0 = it[6];
+      }
+      int16_t* bp = nmode == 1 ? acc + (rowA + r) * ldc : acc + rowA * ldc + col0 + r;
       const i64 js = nmode == 1 ? 1 : ldc;
       const int j0 = ch * half;
       const bool ok_me = mbar_wait(&S.nacc_full[buf], (li >> 1) & 1, err);
@@ -788,10 +813,56 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
       rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
           mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
-          KC, mode, ntn, ptiles, nitems, fresh, pack, sdpv::device_error_word());
+          KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr, sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;
     }
+  }
+  return SDPV_OK;
+}
+
+// Grouped narrow products over a device item table: every item multiplies up to 128 rows of the big side
+// against up to TB rows of the small side over its own K length, and stores its output block at its own place
+// in the accumulator.  Items of different shapes and K run in one launch (one CTA per SM loops over
+// (item, modulus)); the operands are two stacked residue buffers (unsigned digits) with one row length KP.
+extern "C" int sdpv_rns_gemm_grouped(const sdpv_ctx* c, const uint8_t* bigHi, const uint8_t* bigLo, int64_t big_rows,
+                                     int64_t big_stride, const uint8_t* smallHi, const uint8_t* smallLo,
+                                     int64_t small_rows, int64_t small_stride, int64_t KP, int TB, int out_mode,
+                                     const int32_t* items, int64_t nitems, int16_t* acc, int64_t ldc, int64_t rows_out,
+                                     int g0, int G, void* stream) {
+  if (!c || g0 < 0 || G < 1 || g0 + G > c->d.n || G > 65535 || KP <= 0 || KP > 32768 || (KP & 15) || TB < 16 ||
+      TB > 64 || (TB & 15) || (out_mode != 1 && out_mode != 2) || nitems < 0 || nitems > 0x7fffffff || big_rows < 1 ||
+      small_rows < 1 || rows_out < 1 || ldc < 1 || !items)
+    return SDPV_EINVAL;
+  if (nitems == 0) return SDPV_OK;
+  if (big_stride < KP * big_rows || small_stride < KP * small_rows || (big_stride & 15) || (small_stride & 15) ||
+      (((uintptr_t)bigHi | (uintptr_t)bigLo | (uintptr_t)smallHi | (uintptr_t)smallLo) & 15))
+    return SDPV_EINVAL;
+  CUtensorMap mAh, mAl, mBh, mBl;
+  if (!make_map(&mAh, bigHi, KP, big_rows, 1, G, big_stride) || !make_map(&mAl, bigLo, KP, big_rows, 1, G, big_stride) ||
+      !make_map(&mBh, smallHi, KP, small_rows, 1, G, small_stride, TB) ||
+      !make_map(&mBl, smallLo, KP, small_rows, 1, G, small_stride, TB))
+    return SDPV_EINVAL;
+  size_t smem = sizeof(GemmSmem) + 1024;
+  static std::once_flag attr;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr, [&] {
+    attr_err = cudaFuncSetAttribute(rns_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+  if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  for (int gofs = 0; gofs < G; gofs += kMaxG) {
+    const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
+    const i64 n_all = nitems * Gl;
+    const unsigned gx = (unsigned)(n_all < sms ? n_all : sms);
+    // M = rows_out: the accumulator planes (one per modulus) hold rows_out rows of ldc entries
+    rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+        mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs,
+        Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
+    const int st = sdpv::launch_status();
+    if (st != SDPV_OK) return st;
   }
   return SDPV_OK;
 }

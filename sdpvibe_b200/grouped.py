@@ -1,0 +1,524 @@
+"""Grouped batched Cholesky factorisation and triangular solves over a device work list.
+
+Blocks of different sizes are factored and solved together: no bucket of equal sizes, no padding of a
+block beyond its own multiple of 32.  Every block's result is bit-identical to the reference's recursive
+bchol / btrsm_right / btrsm_left / btrsm_left_T on that block alone (sdpvibe/batched.py:243-352),
+because every product, rounding point and sum is the same:
+
+* Factorisation (fixed point at one exponent e).  With the split rule of the recursion (a range of s tiles
+  splits after ceil(s/2) tiles, sdpvibe/batched.py:265) the recursion hands tile (i, j), i >= j, one rounded
+  product  round_e(sum_{k in g} L_ik L_jk^T)  per range g = [lo, mid) of every tree node whose right half
+  holds j (`column_groups`): btrsm_right's update and bchol's Schur complement are both of that form.  The
+  subtractions are exact (fixed exponent, sdpvibe/batched.py:82-92), so their order is free.  A column j is
+  then: its updates, the base tile (chol_tiles + trinv_tiles), and the panel leaf X = round(B X_j^T) with
+  `refine` correction steps (sdpvibe/batched.py:291-299) -- the same column program for every block, so
+  column j of all blocks runs as one wave.
+* Solves (per-column exponents).  L^-1 B and L^-T B round per column over node-shaped row ranges and rescale
+  both halves of every node to a common exponent (sdpvibe/batched.py:313-352), so their rounding depends on
+  the tree: each block runs the program of its own tree (`solve_program`), and a greedy scheduler merges the
+  programs of all blocks into waves of one operation kind (the kind of the block with the longest remaining
+  program).
+
+A wave of products is: tile copies into two operand workspaces (grp_copy), their residues (sdpv_residues_u8),
+one grouped narrow residue GEMM over an item table (sdpv_rns_gemm_grouped: up to 128 rows of one side
+against up to 64 rows of the other, K per item), one CRT (sdpv_crt_block) and the rounding kernel of the wave
+(grp_finish_fixed, or grp_colexp + grp_solve_finish); base-tile waves are grp_tile_widen, sdpv_chol_tiles,
+sdpv_trinv_tiles and grp_tile_narrow; merges are grp_merge.  Plans (host tables uploaded once) are cached per
+block-size sequence.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .rns import dev
+from .mpmat import ctx
+
+BT = 32
+LI = 24                         # extra words of the base tiles' wide fixed point (sdpvibe/batched.py:243)
+F_AR, X_AR, Y_AR, R_AR = 0, 1, 2, 3          # factorisation arenas
+P_AR, PF_AR, PX_AR = 0, 1, 2                  # solve arenas: solve state, factor, inverses
+MAX_SOURCES = 7
+RES_BUDGET = 2 << 30            # residue bytes of one wave's operands before the moduli are split
+
+
+def split_point(lo, hi):
+    """The recursion's split of tiles [lo, hi): n1 = ceil((n // 2) / 32) * 32 for n = 32 (hi - lo)."""
+    return lo + (hi - lo + 1) // 2
+
+
+def column_groups(s, j):
+    """The tile ranges [lo, mid) whose rounded products tile column j of an s-tile block receives."""
+    out, lo, hi = [], 0, s
+    while hi - lo > 1:
+        mid = split_point(lo, hi)
+        if j >= mid:
+            out.append((lo, mid))
+            lo = mid
+        else:
+            hi = mid
+    return out
+
+
+def solve_program(s, lower):
+    """Operation sequence of one block's L^-1 B (lower) or L^-T B solve, in dependency order."""
+    ops = []
+
+    def rec(lo, hi):
+        if hi - lo == 1:
+            ops.append(("leaf", lo))
+            return
+        mid = split_point(lo, hi)
+        first, second = ((lo, mid), (mid, hi)) if lower else ((mid, hi), (lo, mid))
+        rec(*first)
+        ops.append(("upd", lo, mid, hi))
+        rec(*second)
+        ops.append(("merge", lo, mid, hi))
+    rec(0, s)
+    return ops
+
+
+def schedule(programs):
+    """Merge per-block programs into waves of one kind: each wave takes the next operation of every block
+    whose next operation has the kind of the block with the longest remaining program."""
+    pos = [0] * len(programs)
+    waves = []
+    while True:
+        live = [b for b, p in enumerate(programs) if pos[b] < len(p)]
+        if not live:
+            return waves
+        crit = max(live, key=lambda b: len(programs[b]) - pos[b])
+        kind = programs[crit][pos[crit]][0]
+        wave = [(b, programs[b][pos[b]]) for b in live if programs[b][pos[b]][0] == kind]
+        for b, _ in wave:
+            pos[b] += 1
+        waves.append((kind, wave))
+
+
+class Layout:
+    """Arena positions of the blocks: s[b] tiles per side; lower tile (b, i, j) of the factor arena,
+    diagonal tile / solve row tile (b, i)."""
+
+    def __init__(self, sizes):
+        self.s = [int(x) for x in sizes]
+        self.toff = np.concatenate([[0], np.cumsum([s * (s + 1) // 2 for s in self.s])]).astype(np.int64)
+        self.doff = np.concatenate([[0], np.cumsum(self.s)]).astype(np.int64)
+        self.T, self.D = int(self.toff[-1]), int(self.doff[-1])
+
+    def tile(self, b, i, j):
+        return int(self.toff[b]) + i * (i + 1) // 2 + j
+
+    def diag(self, b, i):
+        return int(self.doff[b]) + i
+
+
+def _chunks(seq, n):
+    return [seq[a:a + n] for a in range(0, len(seq), n)]
+
+
+class _Gemm:
+    """One wave of grouped products: operand bands gathered into a big-side and a small-side workspace,
+    the item table of the grouped residue GEMM and the accumulator rows of its outputs."""
+
+    def __init__(self, TB, out_mode, w):
+        self.TB, self.out_mode, self.w = TB, out_mode, w
+        self.copies = ([], [])          # (arena, src base, src ld, row, col, rows, cols, trans) per side
+        self.rows = [0, 0]
+        self.kp = 32
+        self.items = []
+        self.out_rows = 0
+
+    def band(self, side, srcs, trans=False):
+        """A band of 32 rows: srcs = [(arena, tile base entry, ld)] along K (32 columns each).  Returns its
+        first workspace row."""
+        r0 = self.rows[side]
+        for kk, (aid, base, ld) in enumerate(srcs):
+            self.copies[side].append((aid, base, ld, r0, 32 * kk, 32, 32, trans))
+        self.rows[side] += 32
+        self.kp = max(self.kp, 32 * len(srcs))
+        return r0
+
+    def rows_of(self, side, srcs, m):
+        """m rows from 32 x m solve tiles transposed: row c of the band is column c of the tiles; srcs along K."""
+        r0 = self.rows[side]
+        for kk, (aid, base, ld) in enumerate(srcs):
+            for c0 in range(0, m, 32):
+                self.copies[side].append((aid, base + c0, ld, r0 + c0, 32 * kk, 32, min(32, m - c0), True))
+        self.rows[side] += m
+        self.kp = max(self.kp, 32 * len(srcs))
+        return r0
+
+    def item(self, big_row0, big_rows, small_row0, small_rows, klen, out_row0, out_col0=0):
+        self.items.append((big_row0, big_rows, small_row0, small_rows, klen, out_row0, out_col0, 0))
+
+    def take_out_rows(self, n):
+        r0 = self.out_rows
+        self.out_rows += n
+        return r0
+
+    def finalize(self):
+        kp = self.kp
+        descs = []
+        for side in (0, 1):
+            d = np.array([(a, b, ld, r * kp + c, kp, rr, cc, int(t)) for a, b, ld, r, c, rr, cc, t in self.copies[side]],
+                         dtype=np.int64).reshape(-1, 8)
+            descs.append(d)
+        self.desc_big, self.desc_small = descs
+        self.items_np = np.array(self.items, dtype=np.int32).reshape(-1, 8)
+        self.RA, self.RB = max(self.rows[0], 1), max(self.rows[1], 1)
+        if self.out_mode == 1:
+            self.out_rows = self.RA
+        self.Rout = max(self.out_rows, 1)
+        return self
+
+
+def _np_desc(rows, width):
+    return np.array(rows, dtype=np.int64).reshape(-1, width)
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+# ------------------------------------------------------------------ factorisation plan
+class FactorPlan:
+    """Waves of the factorisation of blocks with s[b] tiles per side at limb count L, fixed-point exponent e."""
+
+    def __init__(self, sizes, L, e, refine):
+        self.lay = lay = Layout(sizes)
+        self.L, self.e, self.refine = L, e, refine
+        self.stages = []
+        nb, smax = len(lay.s), max(lay.s)
+        self.ntemp = 1
+        for j in range(smax):
+            blocks = [b for b in range(nb) if lay.s[b] > j]
+            self._update(j, blocks)
+            self.stages.append(("tile", {"fbase": _dev(np.array([lay.tile(b, j, j) * 1024 for b in blocks])),
+                                         "xidx": _dev(np.array([lay.diag(b, j) for b in blocks])),
+                                         "n": len(blocks)}))
+            leaf = [b for b in blocks if lay.s[b] > j + 1]
+            if leaf:
+                self._leaf(j, leaf)
+
+    def _gemm_stage(self, g, fin):
+        g.finalize()
+        g.finish = _dev(_np_desc(fin, 40)) if fin else None
+        g.nfin = len(fin)
+        self.stages.append(("gemm", _to_device(g)))
+
+    def _update(self, j, blocks):
+        lay, e = self.lay, self.e
+        g = _Gemm(TB=32, out_mode=1, w=32)
+        srcs = {}
+        for b in blocks:
+            for lo, mid in column_groups(lay.s[b], j):
+                srow = g.band(1, [(F_AR, lay.tile(b, j, k) * 1024, 32) for k in range(lo, mid)])
+                for ch in _chunks(list(range(j, lay.s[b])), 4):
+                    r0 = None
+                    for i in ch:
+                        r = g.band(0, [(F_AR, lay.tile(b, i, k) * 1024, 32) for k in range(lo, mid)])
+                        r0 = r if r0 is None else r0
+                        srcs.setdefault(lay.tile(b, i, j), []).append((r * 32, -1, -e, -1))
+                    g.item(r0, 32 * len(ch), srow, 32, 32 * (mid - lo), r0)
+        if not g.items:
+            return
+        fin = []
+        for t, ss in srcs.items():
+            assert len(ss) <= MAX_SOURCES
+            row = [F_AR, t * 1024, 32, F_AR, t * 1024, 32, 32, 32, len(ss)]
+            for s in ss:
+                row += list(s)
+            fin.append(row + [0] * (40 - len(row)))
+        self._gemm_stage(g, fin)
+
+    def _leaf(self, j, blocks):
+        """X = round(B X_j^T); refine x { R = B - round(X L_jj^T); X = X + round(R X_j^T) }  (B = tile (i, j))."""
+        lay, e = self.lay, self.e
+        tiles = [(b, i) for b in blocks for i in range(j + 1, lay.s[b])]
+        self.ntemp = max(self.ntemp, len(tiles))
+        tmp = {bi: q for q, bi in enumerate(tiles)}
+
+        def wave(small_of, big_of, out_of, base_of, sign, cst, eidx_of):
+            g = _Gemm(TB=32, out_mode=1, w=32)
+            fin = []
+            for b in blocks:
+                srow = g.band(1, [small_of(b)])
+                for ch in _chunks(list(range(j + 1, lay.s[b])), 4):
+                    r0 = None
+                    for i in ch:
+                        r = g.band(0, [big_of(b, i)])
+                        r0 = r if r0 is None else r0
+                        oa, ob = out_of(b, i)
+                        ba, bb = base_of(b, i)
+                        row = [oa, ob, 32, ba, bb, 32, 32, 32, 1, r * 32, sign, cst, eidx_of(b)]
+                        fin.append(row + [0] * (40 - len(row)))
+                    g.item(r0, 32 * len(ch), srow, 32, 32, r0)
+            self._gemm_stage(g, fin)
+
+        F = lambda b, i: (F_AR, lay.tile(b, i, j) * 1024)
+        Y = lambda b, i: (Y_AR, tmp[(b, i)] * 1024)
+        R = lambda b, i: (R_AR, tmp[(b, i)] * 1024)
+        Xj = lambda b: (X_AR, lay.diag(b, j) * 1024, 32)
+        Ljj = lambda b: (F_AR, lay.tile(b, j, j) * 1024, 32)
+        none = lambda b, i: (-1, 0)
+        xe = lambda b: lay.diag(b, j)
+        first_out = Y if self.refine else F
+        wave(Xj, lambda b, i: F(b, i) + (32,), first_out, none, 1, 0, xe)
+        for it in range(self.refine):
+            wave(Ljj, lambda b, i: Y(b, i) + (32,), R, F, -1, -e, lambda b: -1)
+            wave(Xj, lambda b, i: R(b, i) + (32,), F if it == self.refine - 1 else Y, Y, 1, 0, xe)
+
+
+class _DevGemm:
+    pass
+
+
+def _to_device(g):
+    d = _DevGemm()
+    for k in ("TB", "out_mode", "w", "kp", "RA", "RB", "Rout", "nfin"):
+        setattr(d, k, getattr(g, k))
+    d.desc_big, d.desc_small = _dev(g.desc_big), _dev(g.desc_small)
+    d.nbig, d.nsmall = len(g.desc_big), len(g.desc_small)
+    d.items, d.nitems = _dev(g.items_np), len(g.items_np)
+    d.finish = g.finish
+    for k in ("colexp", "ncolexp", "solve_fin", "nsolve_fin", "ngroups"):
+        setattr(d, k, getattr(g, k, None))
+    return d
+
+
+# ------------------------------------------------------------------ solve plan
+class SolvePlan:
+    """Waves of L^-1 B (lower) or L^-T B for blocks with s[b] tiles and m right-hand sides; refine = 0."""
+
+    def __init__(self, sizes, L, e, m, lower):
+        self.lay = lay = Layout(sizes)
+        self.L, self.e, self.m, self.lower = L, e, m, lower
+        progs = [solve_program(s, lower) for s in lay.s]
+        self.stages = []
+        for kind, wave in schedule(progs):
+            if kind == "merge":
+                d = []
+                for b, (_, lo, mid, hi) in wave:
+                    for c0 in range(0, m, 32):
+                        d.append((lay.diag(b, lo), hi - lo, c0, min(32, m - c0)))
+                self.stages.append(("merge", {"desc": _dev(_np_desc(d, 4)), "n": len(d)}))
+            else:
+                self._products(kind, wave)
+
+    def _products(self, kind, wave):
+        lay, m, e, lower = self.lay, self.m, self.e, self.lower
+        narrow_rhs = m <= 64
+        if narrow_rhs:
+            TB = -(-m // 16) * 16
+            g = _Gemm(TB=TB, out_mode=1, w=TB)
+        else:
+            g = _Gemm(TB=32 if kind == "leaf" else 64, out_mode=2, w=m)
+        colexp, fin = [], []
+        for q, (b, op) in enumerate(wave):
+            if kind == "leaf":
+                j = op[1]
+                a_bands = [[(PX_AR, lay.diag(b, j) * 1024, 32)]]
+                a_trans = not lower
+                p_tiles = [(P_AR, lay.diag(b, j) * 32 * m, m)]
+                out_rts = [lay.diag(b, j)]
+                eA, eA_idx, eB_rt, mode = 0, lay.diag(b, j), lay.diag(b, j), 0
+            else:
+                _, lo, mid, hi = op
+                if lower:
+                    out_range, k_range = range(mid, hi), range(lo, mid)
+                    a_bands = [[(PF_AR, lay.tile(b, i, k) * 1024, 32) for k in k_range] for i in out_range]
+                else:
+                    out_range, k_range = range(lo, mid), range(mid, hi)
+                    a_bands = [[(PF_AR, lay.tile(b, t, i) * 1024, 32) for t in k_range] for i in out_range]
+                a_trans = not lower
+                p_tiles = [(P_AR, lay.diag(b, k) * 32 * m, m) for k in k_range]
+                out_rts = [lay.diag(b, i) for i in out_range]
+                eA, eA_idx, eB_rt, mode = e, -1, lay.diag(b, k_range[0]), 1
+            klen = 32 * len(p_tiles)
+            if narrow_rhs:
+                srow = g.rows_of(1, p_tiles, m)
+                rows0 = []
+                for ch in _chunks(a_bands, 4):
+                    r0 = None
+                    for band in ch:
+                        r = g.band(0, band, a_trans)
+                        r0 = r if r0 is None else r0
+                        rows0.append(r)
+                    g.item(r0, 32 * len(ch), srow, m, klen, r0)
+            else:
+                prow = g.rows_of(0, p_tiles, m)
+                rows0 = []
+                for ch in _chunks(a_bands, 2):
+                    s0 = None
+                    for band in ch:
+                        r = g.band(1, band, a_trans)
+                        s0 = r if s0 is None else s0
+                    o0 = g.take_out_rows(32 * len(ch))
+                    rows0 += [o0 + 32 * u for u in range(len(ch))]
+                    for p0 in range(0, m, 128):
+                        g.item(prow + p0, min(128, m - p0), s0, 32 * len(ch), klen, o0, p0)
+            for c0 in range(0, m, 32):
+                nc = min(32, m - c0)
+                colexp.append((rows0[0], 32 * len(rows0), c0, nc, eA, eA_idx, eB_rt, q))
+                for r0, rt in zip(rows0, out_rts):
+                    fin.append((r0, c0, nc, q, mode, rt, rt, 32))
+        g.finalize()
+        g.colexp, g.ncolexp = _dev(_np_desc(colexp, 8)), len(colexp)
+        g.solve_fin, g.nsolve_fin = _dev(_np_desc(fin, 8)), len(fin)
+        g.ngroups = len(wave)
+        g.finish, g.nfin = None, 0
+        self.stages.append(("gemm", _to_device(g)))
+
+
+# ------------------------------------------------------------------ execution
+def _ptrs(tensors):
+    """host arrays of the arenas' device pointers and plane strides (entries), as the C ABI takes them"""
+    arr = (ctypes.c_void_p * 4)(*([t.data_ptr() for t in tensors] + [None] * (4 - len(tensors))))
+    planes = (ctypes.c_int64 * 4)(*([t[0].numel() for t in tensors] + [0] * (4 - len(tensors))))
+    keep = (arr, planes)
+    return ctypes.cast(arr, ctypes.c_void_p), ctypes.cast(planes, ctypes.c_void_p), len(tensors), keep
+
+
+def _residue_products(R, g, ws_big, ws_small, acc):
+    """acc <- residues of the wave's grouped products (moduli split into groups within the residue budget)."""
+    per_mod = 2 * g.kp * (g.RA + g.RB)
+    GR = R.n if R.n * per_mod <= RES_BUDGET else max(R.G, (RES_BUDGET // per_mod) // R.G * R.G)
+    for g0 in range(0, R.n, GR):
+        G = min(GR, R.n - g0)
+        bh, bl = R.residues(ws_big, 0, g.kp, g0, G, spread=True, unsigned=True)
+        sh, sl = R.residues(ws_small, 0, g.kp, g0, G, spread=True, unsigned=True)
+        _lib.call("sdpv_rns_gemm_grouped", R.handle, _lib.ptr_strided(bh), _lib.ptr_strided(bl), g.RA, bh.stride(0),
+                  _lib.ptr_strided(sh), _lib.ptr_strided(sl), g.RB, sh.stride(0), g.kp, g.TB, g.out_mode,
+                  _lib.ptr(g.items), g.nitems, _lib.ptr(acc), g.w, g.Rout, g0, G, _lib.stream())
+        del bh, bl, sh, sl
+
+
+def _gather(g, arenas, L):
+    arr, planes, n, _keep = _ptrs(arenas)
+    ws = []
+    for rows, desc, nd in ((g.RA, g.desc_big, g.nbig), (g.RB, g.desc_small, g.nsmall)):
+        w = torch.empty((L, rows, g.kp), dtype=torch.int32, device=dev)
+        _lib.call("sdpv_grp_copy", arr, planes, n, _lib.ptr(w), rows * g.kp, L, _lib.ptr(desc), nd, _lib.stream())
+        ws.append(w)
+    return ws
+
+
+def _product_wave(g, arenas, L):
+    """gather, residues, grouped GEMM, CRT: -> (CRT words (W, Rout * w), bit lengths)"""
+    R = ctx(L)
+    ws_big, ws_small = _gather(g, arenas, L)
+    acc = torch.empty((R.n, g.Rout, g.w), dtype=torch.int16, device=dev)
+    _residue_products(R, g, ws_big, ws_small, acc)
+    del ws_big, ws_small
+    Wd, bl, _ = R.crt_block(acc, g.w, 0, g.w, g.Rout)
+    return R, Wd, bl
+
+
+def run_factor(plan, Fa):
+    """Factor the blocks held in the factor arena Fa (L, T, 32, 32) in place; returns (X arena, xe)."""
+    L, e = plan.L, plan.e
+    lay = plan.lay
+    WL, LF = L + LI, L
+    Xa = torch.empty((L, lay.D, BT, BT), dtype=torch.int32, device=dev)
+    xe = torch.empty((lay.D,), dtype=torch.int64, device=dev)
+    Ya = torch.empty((L, plan.ntemp, BT, BT), dtype=torch.int32, device=dev)
+    Ra = torch.empty_like(Ya)
+    arenas = [Fa, Xa, Ya, Ra]
+    for kind, st in plan.stages:
+        if kind == "tile":
+            n = st["n"]
+            Wb = torch.empty((n, BT, BT, WL), dtype=torch.int32, device=dev)
+            _lib.call("sdpv_grp_tile_widen", _lib.ptr(Fa), Fa[0].numel(), L, e, WL, LF, _lib.ptr(st["fbase"]), n,
+                      _lib.ptr(Wb), _lib.stream())
+            RINV = torch.empty((n, BT, WL), dtype=torch.int32, device=dev)
+            _lib.call("sdpv_chol_tiles", _lib.ptr(Wb), _lib.ptr(RINV), n, BT, WL, LF, _lib.stream())
+            Xw = torch.empty_like(Wb)
+            scratch = Xw if WL <= 64 else torch.empty_like(Wb)   # the shared-memory inverse needs no scratch
+            _lib.call("sdpv_trinv_tiles", _lib.ptr(Wb), _lib.ptr(RINV), _lib.ptr(Xw), _lib.ptr(scratch), n, BT, WL, LF,
+                      _lib.stream())
+            _lib.call("sdpv_grp_tile_narrow", _lib.ptr(Wb), _lib.ptr(Xw), WL, LF, _lib.ptr(Fa), Fa[0].numel(), L, e,
+                      _lib.ptr(st["fbase"]), _lib.ptr(Xa), Xa[0].numel(), _lib.ptr(st["xidx"]), _lib.ptr(xe), n,
+                      _lib.stream())
+            continue
+        R, Wd, bl = _product_wave(st, arenas, L)
+        arr, planes, n, _keep = _ptrs(arenas)
+        _lib.call("sdpv_grp_finish_fixed", _lib.ptr(Wd), R.W, Wd.shape[1], st.w, arr, planes, n, L, _lib.ptr(xe),
+                  _lib.ptr(st.finish), st.nfin, _lib.stream())
+    return Xa, xe
+
+
+def run_solve(plan, Pa, Pe, Fa, Xa, xe):
+    """Solve in place on the solve arena Pa (L, RT, 32, m) with exponents Pe (RT, m)."""
+    L, m = plan.L, plan.m
+    arenas = [Pa, Fa, Xa]
+    for kind, st in plan.stages:
+        if kind == "merge":
+            _lib.call("sdpv_grp_merge", _lib.ptr(Pa), Pa[0].numel(), _lib.ptr(Pe), m, L, _lib.ptr(st["desc"]), st["n"],
+                      _lib.stream())
+            continue
+        R, Wd, bl = _product_wave(st, arenas, L)
+        sU = torch.empty((st.ngroups, m), dtype=torch.int64, device=dev)
+        eU = torch.empty_like(sU)
+        _lib.call("sdpv_grp_colexp", _lib.ptr(bl), st.w, _lib.ptr(Pe), m, L, _lib.ptr(xe), _lib.ptr(st.colexp),
+                  st.ncolexp, _lib.ptr(sU), _lib.ptr(eU), _lib.stream())
+        _lib.call("sdpv_grp_solve_finish", _lib.ptr(Wd), R.W, Wd.shape[1], st.w, _lib.ptr(Pa), Pa[0].numel(),
+                  _lib.ptr(Pe), m, L, _lib.ptr(sU), _lib.ptr(eU), _lib.ptr(st.solve_fin), st.nsolve_fin, _lib.stream())
+
+
+_PLANS = {}
+
+
+def factor_plan(sizes, L, e, refine):
+    key = ("f", tuple(sizes), L, e, refine, torch.cuda.current_device())
+    if key not in _PLANS:
+        _PLANS[key] = FactorPlan(sizes, L, e, refine)
+    return _PLANS[key]
+
+
+def solve_plan(sizes, L, e, m, lower):
+    key = ("s", tuple(sizes), L, e, m, lower, torch.cuda.current_device())
+    if key not in _PLANS:
+        _PLANS[key] = SolvePlan(sizes, L, e, m, lower)
+    return _PLANS[key]
+
+
+# ------------------------------------------------------------------ dense <-> arena
+_IDX = {}
+
+
+def _tile_index(s):
+    """flat positions (in an s*32 x s*32 row-major matrix) of the lower tiles' entries, tile-major"""
+    key = ("t", s, torch.cuda.current_device())
+    if key not in _IDX:
+        n = 32 * s
+        idx = []
+        for i in range(s):
+            for j in range(i + 1):
+                r = np.arange(32)[:, None] + 32 * i
+                c = np.arange(32)[None, :] + 32 * j
+                idx.append((r * n + c).reshape(-1))
+        _IDX[key] = torch.from_numpy(np.concatenate(idx)).to(dev)
+    return _IDX[key]
+
+
+def dense_to_arena(P, Fa, lay, b0):
+    """P (L, nb, n, n) fixed point -> the factor arena tiles of blocks b0 .. b0 + nb - 1 (all of s = n / 32)."""
+    L, nb, n, _ = P.shape
+    s = n // 32
+    T_b = s * (s + 1) // 2
+    t0 = int(lay.toff[b0])
+    idx = _tile_index(s)
+    Fa.view(L, -1)[:, t0 * 1024:(t0 + nb * T_b) * 1024].view(L, nb, T_b * 1024).copy_(
+        P.reshape(L, nb, n * n).index_select(2, idx))
+
+
+def arena_to_dense(Fa, lay, b0, nb, s):
+    """the lower tiles of blocks b0 .. b0 + nb - 1 -> dense (L, nb, 32 s, 32 s) with zero upper tiles"""
+    L = Fa.shape[0]
+    n = 32 * s
+    T_b = s * (s + 1) // 2
+    t0 = int(lay.toff[b0])
+    out = torch.zeros((L, nb, n * n), dtype=torch.int32, device=dev)
+    out.index_copy_(2, _tile_index(s), Fa.view(L, -1)[:, t0 * 1024:(t0 + nb * T_b) * 1024].view(L, nb, T_b * 1024))
+    return out.view(L, nb, n, n)
