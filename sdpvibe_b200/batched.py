@@ -1,11 +1,10 @@
 """Batched multiprecision linear algebra over many equal-sized blocks: drop-in for ``sdpvibe.batched``.
 
 A BMP holds a stack of nb matrices: limbs int32 (L, nb, R, C) limb planes and exp, a Python int
-(uniform) or an (nb, C) int64 tensor (sdpvibe/batched.py:16-42).  The recursive Cholesky and the
-triangular solves follow the reference's recursion, split points, refinement counts and rounding points
-exactly (batched.py:234-352), so results are bit-identical; every product is the exact residue GEMM of
-rns.py over all nb blocks in one launch, and the 32 x 32 diagonal tiles use the CUDA-core base case of
-basecase.py.
+(uniform) or an (nb, C) int64 tensor (sdpvibe/batched.py:16-42).  brescale / badd / bgemm_nt are one
+kernel each (bgemm_nt: the exact residue GEMM of rns.py over all nb blocks in one launch, then one CRT and
+one rounding).  bchol and the triangular solves keep the reference's signatures and results and run on the
+grouped work-list engine (``grouped``).
 """
 import torch
 
@@ -13,7 +12,6 @@ from . import _lib
 from .rns import dev
 from .mpmat import ctx, headroom_bits, residue_product
 from .limbops import shift_round, add_same, bitlen_words
-from .basecase import _soa_to_aos, _aos_to_soa, tile_factor
 
 
 class BMP:
@@ -135,121 +133,60 @@ def _bcrt_round(acc, nb, M, N, e_in, out_exp, L):
 
 
 class BTile:
+    """A diagonal tile of a factorisation: X (its inverse, one exponent per block) and Lmp (its factor)."""
     __slots__ = ("X", "Lmp")
 
 
-def bchol_tile(A, LI=24, threads=256):
-    """batched.py:243-262: A: BMP (nb, b, b) fixed point -> (L BMP, BTile with the inverse X)."""
-    nb, b, _ = A.shape
-    L, e = A.L, A.exp
-    LF, WL = L, L + LI
-    F = 32 * LF
-    Ws = brescale(A, -F, WL).limbs                                 # (WL, nb, b, b)
-    Lw, X, _ = tile_factor(_soa_to_aos(Ws), WL, LF)                # (nb, b, b, WL) each
-    Lout = brescale(BMP(_aos_to_soa(Lw), -F), e, L)
-    Xs = _aos_to_soa(X)
-    top = bitlen_words(Xs.reshape(WL, -1)).view(nb, b * b).amax(1) - F
-    ex = (top - headroom_bits(L))[:, None].expand(nb, b).contiguous()
-    t = BTile()
-    t.Lmp = Lout
-    t.X = brescale(BMP(Xs, torch.full((nb, b), -F, dtype=torch.int64, device=dev)), ex, L)
-    return Lout, t
+# ------------------------------------------------------------------ factorisation and solves (drop-in API)
+# The reference's recursive bchol / btrsm_* (sdpvibe/batched.py:274-352).  Here they run on the grouped
+# work-list engine (sdpvibe_b200.grouped), which computes the same products and roundings for every block.
 
-
-def _split(n, bt):
-    return (n // 2 + bt - 1) // bt * bt
-
-
-def _ntiles(n, bt):
-    if n <= bt:
-        return 1
-    n1 = _split(n, bt)
-    return _ntiles(n1, bt) + _ntiles(n - n1, bt)
+def _tiles_of(fac, e):
+    out = []
+    for j in range(fac.batches[0][1]):
+        Xm, xe, Lm = fac.diag_tile(0, j)
+        t = BTile()
+        t.X = BMP(Xm, xe[:, None].expand(Xm.shape[1], 32).contiguous())
+        t.Lmp = BMP(Lm, e)
+        out.append(t)
+    return out
 
 
 def bchol(A, bt=32, refine=1):
-    """batched.py:274-288: batched recursive Cholesky of equilibrated fixed-point blocks -> (L, tiles)."""
-    nb, n, _ = A.shape
-    L, e = A.L, A.exp
-    if n <= bt:
-        assert n == bt
-        Lt, t = bchol_tile(A)
-        return Lt, [t]
-    n1 = _split(n, bt)
-    L11, t1 = bchol(A[:n1, :n1], bt, refine)
-    L21 = btrsm_right(A[n1:, :n1], L11, t1, bt, refine)
-    S = badd(A[n1:, n1:], bgemm_nt(L21, L21, out_exp=e), -1, out_exp=e)
-    L22, t2 = bchol(S, bt, refine)
-    out = torch.zeros((L, nb, n, n), dtype=torch.int32, device=dev)
-    out[:, :, :n1, :n1] = L11.limbs
-    out[:, :, n1:, :n1] = L21.limbs
-    out[:, :, n1:, n1:] = L22.limbs
-    return BMP(out, e), t1 + t2
+    """batched.py:274-288: batched Cholesky of equilibrated fixed-point blocks -> (L, tiles)."""
+    from . import grouped
+    assert bt == 32 and isinstance(A.exp, int)
+    fac = grouped.Factorisation([A.limbs], A.exp, refine)
+    return BMP(fac.dense(0), A.exp), _tiles_of(fac, A.exp)
+
+
+def _factor(Lf, tiles):
+    from . import grouped
+    return grouped.factor_from_tiles(Lf.limbs, Lf.exp, [t.X.limbs for t in tiles], [t.X.exp[:, 0] for t in tiles])
 
 
 def btrsm_right(B, Lf, tiles, bt=32, refine=1):
-    """batched.py:291-305: X with X L^T = B (fixed point)."""
-    nb, m, n = B.shape
-    e = Lf.exp
-    if n <= bt:
-        t = tiles[0]
-        X = bgemm_nt(B, t.X, out_exp=e, bt_rowexp=t.X.exp)
-        for _ in range(refine):
-            Rr = badd(B, bgemm_nt(X, t.Lmp, out_exp=e), -1, out_exp=e)
-            X = badd(X, bgemm_nt(Rr, t.X, out_exp=e, bt_rowexp=t.X.exp), 1, out_exp=e)
-        return X
-    n1 = _split(n, bt)
-    k1 = _ntiles(n1, bt)
-    X1 = btrsm_right(B[:, :n1], Lf[:n1, :n1], tiles[:k1], bt, refine)
-    B2 = badd(B[:, n1:], bgemm_nt(X1, Lf[n1:, :n1], out_exp=e), -1, out_exp=e)
-    X2 = btrsm_right(B2, Lf[n1:, n1:], tiles[k1:], bt, refine)
-    return BMP(torch.cat([X1.limbs, X2.limbs], 3), e)
+    """batched.py:291-305: X with X L^T = B (fixed point, B at L's exponent)."""
+    from . import grouped
+    assert bt == 32
+    return BMP(grouped.right_solve(_factor(Lf, tiles), B.limbs, refine), Lf.exp)
 
 
-def _tr(B):
-    """limbs of B^T per block, as the 'Bt' operand (row exponents passed separately)"""
-    return BMP(B.limbs.transpose(2, 3).contiguous(), 0)
-
-
-def _bleaf(X, Lm, B, refine):
-    """batched.py:313-319: P = Lm^-1 B with the explicit tile inverse (+ refinement steps)."""
-    P = bgemm_nt(X, _tr(B), out_exp="col", bt_rowexp=B.expt())
-    for _ in range(refine):
-        Rr = badd(B, bgemm_nt(Lm, _tr(P), out_exp="col", bt_rowexp=P.expt()), -1, out_exp="align")
-        P = badd(P, bgemm_nt(X, _tr(Rr), out_exp="col", bt_rowexp=Rr.expt()), 1, out_exp="align")
-    return P
+def _left(Lf, B, tiles, refine, lower):
+    from . import grouped
+    if refine:
+        raise NotImplementedError("the grouped triangular solves implement refine = 0 (the solver's setting)")
+    nb, n, m = B.shape
+    out = grouped.solve(_factor(Lf, tiles), [(B.limbs.contiguous(), B.expt().contiguous())], lower)
+    Pm, pe = out[0]
+    return BMP(Pm[:, :, :n].contiguous(), pe)
 
 
 def btrsm_left(Lf, B, tiles, bt=32, refine=0):
     """batched.py:322-335: P = L^-1 B, B (nb, n, m) with per-(block, column) exponents."""
-    nb, n, m = B.shape
-    if n <= bt:
-        t = tiles[0]
-        return _bleaf(t.X, t.Lmp, B, refine)
-    n1 = _split(n, bt)
-    k1 = _ntiles(n1, bt)
-    P1 = btrsm_left(Lf[:n1, :n1], B[:n1, :], tiles[:k1], bt, refine)
-    U = bgemm_nt(Lf[n1:, :n1], _tr(P1), out_exp="col", bt_rowexp=P1.expt())
-    B2 = badd(B[n1:, :], U, -1, out_exp="align")
-    P2 = btrsm_left(Lf[n1:, n1:], B2, tiles[k1:], bt, refine)
-    ee = torch.maximum(P1.expt(), P2.expt())
-    P1, P2 = brescale(P1, ee), brescale(P2, ee)
-    return BMP(torch.cat([P1.limbs, P2.limbs], 2), ee)
+    return _left(Lf, B, tiles, refine, True)
 
 
-def btrsm_left_T(Lf, B, tiles, bt=32, refine=1):
-    """batched.py:338-352: P = L^-T B."""
-    nb, n, m = B.shape
-    if n <= bt:
-        t = tiles[0]
-        XT = BMP(t.X.limbs.transpose(2, 3).contiguous(), t.X.exp)    # per-block uniform exponent
-        return _bleaf(XT, t.Lmp.t(), B, refine)
-    n1 = _split(n, bt)
-    k1 = _ntiles(n1, bt)
-    P2 = btrsm_left_T(Lf[n1:, n1:], B[n1:, :], tiles[k1:], bt, refine)
-    U = bgemm_nt(Lf[n1:, :n1].t(), _tr(P2), out_exp="col", bt_rowexp=P2.expt())
-    B1 = badd(B[:n1, :], U, -1, out_exp="align")
-    P1 = btrsm_left_T(Lf[:n1, :n1], B1, tiles[:k1], bt, refine)
-    ee = torch.maximum(P1.expt(), P2.expt())
-    P1, P2 = brescale(P1, ee), brescale(P2, ee)
-    return BMP(torch.cat([P1.limbs, P2.limbs], 2), ee)
+def btrsm_left_T(Lf, B, tiles, bt=32, refine=0):
+    """batched.py:338-352: P = L^-T B (the solver calls it with refine = 0)."""
+    return _left(Lf, B, tiles, refine, False)

@@ -181,40 +181,86 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
 
-# ------------------------------------------------------------------ factorisation plan
-class FactorPlan:
-    """Waves of the factorisation of blocks with s[b] tiles per side at limb count L, fixed-point exponent e."""
+class _DevGemm:
+    pass
 
-    def __init__(self, sizes, L, e, refine):
+
+def _to_device(g):
+    d = _DevGemm()
+    for k in ("TB", "out_mode", "w", "kp", "RA", "RB", "Rout", "nfin", "ncolexp", "nsolve_fin", "ngroups"):
+        setattr(d, k, getattr(g, k, None))
+    d.desc_big, d.desc_small = _dev(g.desc_big), _dev(g.desc_small)
+    d.nbig, d.nsmall = len(g.desc_big), len(g.desc_small)
+    d.items, d.nitems = _dev(g.items_np), len(g.items_np)
+    for k in ("finish", "colexp", "solve_fin"):
+        v = getattr(g, k, None)
+        setattr(d, k, _dev(v) if v is not None else None)
+    return d
+
+
+class _Plan:
+    def device_stages(self):
+        """the stages with their tables on the current device (uploaded once)"""
+        key = torch.cuda.current_device()
+        cache = self.__dict__.setdefault("_dev_stages", {})
+        if key not in cache:
+            out = []
+            for kind, st in self.stages:
+                if kind == "gemm":
+                    out.append((kind, _to_device(st)))
+                else:
+                    out.append((kind, {k: (_dev(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}))
+            cache[key] = out
+        return cache[key]
+
+
+# ------------------------------------------------------------------ factorisation plan
+class FactorPlan(_Plan):
+    """Waves of the factorisation of blocks with s[b] tiles per side at limb count L, fixed-point exponent e.
+    With `tree` and `row0` (per block) only rows >= row0[b] are computed, against a factor of tree[b] tiles
+    already in the arena (columns j < tree[b]): the right solve X L^T = B of sdpvibe/batched.py:291-305 with
+    B's row tiles below the factor's."""
+
+    def __init__(self, sizes, L, e, refine, tree=None, row0=None):
         self.lay = lay = Layout(sizes)
         self.L, self.e, self.refine = L, e, refine
+        nb = len(lay.s)
+        self.tree = list(tree) if tree is not None else lay.s
+        self.row0 = list(row0) if row0 is not None else [0] * nb
         self.stages = []
-        nb, smax = len(lay.s), max(lay.s)
         self.ntemp = 1
-        for j in range(smax):
-            blocks = [b for b in range(nb) if lay.s[b] > j]
+        for j in range(max(self.tree)):
+            blocks = [b for b in range(nb) if self.tree[b] > j]
             self._update(j, blocks)
-            self.stages.append(("tile", {"fbase": _dev(np.array([lay.tile(b, j, j) * 1024 for b in blocks])),
-                                         "xidx": _dev(np.array([lay.diag(b, j) for b in blocks])),
-                                         "n": len(blocks)}))
-            leaf = [b for b in blocks if lay.s[b] > j + 1]
+            diag = [b for b in blocks if self.row0[b] <= j]
+            if diag:
+                self.stages.append(("tile", {"fbase": np.array([lay.tile(b, j, j) * 1024 for b in diag], np.int64),
+                                             "xidx": np.array([lay.diag(b, j) for b in diag], np.int64),
+                                             "n": len(diag)}))
+            leaf = [b for b in blocks if lay.s[b] > max(j + 1, self.row0[b])]
             if leaf:
                 self._leaf(j, leaf)
 
+    def _rows(self, b, first):
+        return list(range(max(first, self.row0[b]), self.lay.s[b]))
+
     def _gemm_stage(self, g, fin):
         g.finalize()
-        g.finish = _dev(_np_desc(fin, 40)) if fin else None
+        g.finish = _np_desc(fin, 40)
         g.nfin = len(fin)
-        self.stages.append(("gemm", _to_device(g)))
+        self.stages.append(("gemm", g))
 
     def _update(self, j, blocks):
         lay, e = self.lay, self.e
         g = _Gemm(TB=32, out_mode=1, w=32)
         srcs = {}
         for b in blocks:
-            for lo, mid in column_groups(lay.s[b], j):
+            rows = self._rows(b, j)
+            for lo, mid in column_groups(self.tree[b], j):
+                if not rows:
+                    continue
                 srow = g.band(1, [(F_AR, lay.tile(b, j, k) * 1024, 32) for k in range(lo, mid)])
-                for ch in _chunks(list(range(j, lay.s[b])), 4):
+                for ch in _chunks(rows, 4):
                     r0 = None
                     for i in ch:
                         r = g.band(0, [(F_AR, lay.tile(b, i, k) * 1024, 32) for k in range(lo, mid)])
@@ -235,7 +281,7 @@ class FactorPlan:
     def _leaf(self, j, blocks):
         """X = round(B X_j^T); refine x { R = B - round(X L_jj^T); X = X + round(R X_j^T) }  (B = tile (i, j))."""
         lay, e = self.lay, self.e
-        tiles = [(b, i) for b in blocks for i in range(j + 1, lay.s[b])]
+        tiles = [(b, i) for b in blocks for i in self._rows(b, j + 1)]
         self.ntemp = max(self.ntemp, len(tiles))
         tmp = {bi: q for q, bi in enumerate(tiles)}
 
@@ -244,7 +290,7 @@ class FactorPlan:
             fin = []
             for b in blocks:
                 srow = g.band(1, [small_of(b)])
-                for ch in _chunks(list(range(j + 1, lay.s[b])), 4):
+                for ch in _chunks(self._rows(b, j + 1), 4):
                     r0 = None
                     for i in ch:
                         r = g.band(0, [big_of(b, i)])
@@ -270,25 +316,8 @@ class FactorPlan:
             wave(Xj, lambda b, i: R(b, i) + (32,), F if it == self.refine - 1 else Y, Y, 1, 0, xe)
 
 
-class _DevGemm:
-    pass
-
-
-def _to_device(g):
-    d = _DevGemm()
-    for k in ("TB", "out_mode", "w", "kp", "RA", "RB", "Rout", "nfin"):
-        setattr(d, k, getattr(g, k))
-    d.desc_big, d.desc_small = _dev(g.desc_big), _dev(g.desc_small)
-    d.nbig, d.nsmall = len(g.desc_big), len(g.desc_small)
-    d.items, d.nitems = _dev(g.items_np), len(g.items_np)
-    d.finish = g.finish
-    for k in ("colexp", "ncolexp", "solve_fin", "nsolve_fin", "ngroups"):
-        setattr(d, k, getattr(g, k, None))
-    return d
-
-
 # ------------------------------------------------------------------ solve plan
-class SolvePlan:
+class SolvePlan(_Plan):
     """Waves of L^-1 B (lower) or L^-T B for blocks with s[b] tiles and m right-hand sides; refine = 0."""
 
     def __init__(self, sizes, L, e, m, lower):
@@ -302,7 +331,7 @@ class SolvePlan:
                 for b, (_, lo, mid, hi) in wave:
                     for c0 in range(0, m, 32):
                         d.append((lay.diag(b, lo), hi - lo, c0, min(32, m - c0)))
-                self.stages.append(("merge", {"desc": _dev(_np_desc(d, 4)), "n": len(d)}))
+                self.stages.append(("merge", {"desc": _np_desc(d, 4), "n": len(d)}))
             else:
                 self._products(kind, wave)
 
@@ -364,11 +393,11 @@ class SolvePlan:
                 for r0, rt in zip(rows0, out_rts):
                     fin.append((r0, c0, nc, q, mode, rt, rt, 32))
         g.finalize()
-        g.colexp, g.ncolexp = _dev(_np_desc(colexp, 8)), len(colexp)
-        g.solve_fin, g.nsolve_fin = _dev(_np_desc(fin, 8)), len(fin)
+        g.colexp, g.ncolexp = _np_desc(colexp, 8), len(colexp)
+        g.solve_fin, g.nsolve_fin = _np_desc(fin, 8), len(fin)
         g.ngroups = len(wave)
         g.finish, g.nfin = None, 0
-        self.stages.append(("gemm", _to_device(g)))
+        self.stages.append(("gemm", g))
 
 
 # ------------------------------------------------------------------ execution
@@ -415,17 +444,18 @@ def _product_wave(g, arenas, L):
     return R, Wd, bl
 
 
-def run_factor(plan, Fa):
+def run_factor(plan, Fa, Xa=None, xe=None):
     """Factor the blocks held in the factor arena Fa (L, T, 32, 32) in place; returns (X arena, xe)."""
     L, e = plan.L, plan.e
     lay = plan.lay
     WL, LF = L + LI, L
-    Xa = torch.empty((L, lay.D, BT, BT), dtype=torch.int32, device=dev)
-    xe = torch.empty((lay.D,), dtype=torch.int64, device=dev)
+    if Xa is None:
+        Xa = torch.empty((L, lay.D, BT, BT), dtype=torch.int32, device=dev)
+        xe = torch.empty((lay.D,), dtype=torch.int64, device=dev)
     Ya = torch.empty((L, plan.ntemp, BT, BT), dtype=torch.int32, device=dev)
     Ra = torch.empty_like(Ya)
     arenas = [Fa, Xa, Ya, Ra]
-    for kind, st in plan.stages:
+    for kind, st in plan.device_stages():
         if kind == "tile":
             n = st["n"]
             Wb = torch.empty((n, BT, BT, WL), dtype=torch.int32, device=dev)
@@ -452,7 +482,7 @@ def run_solve(plan, Pa, Pe, Fa, Xa, xe):
     """Solve in place on the solve arena Pa (L, RT, 32, m) with exponents Pe (RT, m)."""
     L, m = plan.L, plan.m
     arenas = [Pa, Fa, Xa]
-    for kind, st in plan.stages:
+    for kind, st in plan.device_stages():
         if kind == "merge":
             _lib.call("sdpv_grp_merge", _lib.ptr(Pa), Pa[0].numel(), _lib.ptr(Pe), m, L, _lib.ptr(st["desc"]), st["n"],
                       _lib.stream())
@@ -470,14 +500,14 @@ _PLANS = {}
 
 
 def factor_plan(sizes, L, e, refine):
-    key = ("f", tuple(sizes), L, e, refine, torch.cuda.current_device())
+    key = ("f", tuple(sizes), L, e, refine)
     if key not in _PLANS:
         _PLANS[key] = FactorPlan(sizes, L, e, refine)
     return _PLANS[key]
 
 
 def solve_plan(sizes, L, e, m, lower):
-    key = ("s", tuple(sizes), L, e, m, lower, torch.cuda.current_device())
+    key = ("s", tuple(sizes), L, e, m, lower)
     if key not in _PLANS:
         _PLANS[key] = SolvePlan(sizes, L, e, m, lower)
     return _PLANS[key]
@@ -487,18 +517,22 @@ def solve_plan(sizes, L, e, m, lower):
 _IDX = {}
 
 
+def tile_positions(s):
+    """flat positions (in an s*32 x s*32 row-major matrix) of the lower tiles' entries, in arena order"""
+    n = 32 * s
+    idx = []
+    for i in range(s):
+        for j in range(i + 1):
+            r = np.arange(32)[:, None] + 32 * i
+            c = np.arange(32)[None, :] + 32 * j
+            idx.append((r * n + c).reshape(-1))
+    return np.concatenate(idx)
+
+
 def _tile_index(s):
-    """flat positions (in an s*32 x s*32 row-major matrix) of the lower tiles' entries, tile-major"""
     key = ("t", s, torch.cuda.current_device())
     if key not in _IDX:
-        n = 32 * s
-        idx = []
-        for i in range(s):
-            for j in range(i + 1):
-                r = np.arange(32)[:, None] + 32 * i
-                c = np.arange(32)[None, :] + 32 * j
-                idx.append((r * n + c).reshape(-1))
-        _IDX[key] = torch.from_numpy(np.concatenate(idx)).to(dev)
+        _IDX[key] = torch.from_numpy(tile_positions(s)).to(dev)
     return _IDX[key]
 
 
@@ -522,3 +556,122 @@ def arena_to_dense(Fa, lay, b0, nb, s):
     out = torch.zeros((L, nb, n * n), dtype=torch.int32, device=dev)
     out.index_copy_(2, _tile_index(s), Fa.view(L, -1)[:, t0 * 1024:(t0 + nb * T_b) * 1024].view(L, nb, T_b * 1024))
     return out.view(L, nb, n, n)
+
+
+# ------------------------------------------------------------------ public objects
+class Factorisation:
+    """Cholesky factors of batches of equilibrated fixed-point blocks, all factored by one grouped plan.
+    batches: (L, nb_q, n_q, n_q) int32 limb planes at the fixed-point exponent e, n_q a multiple of 32; the
+    factorisation runs as one CUDA-graph replay per sequence of batch shapes (graphs.run)."""
+
+    def __init__(self, batches, e, refine=1):
+        from . import graphs
+        L = batches[0].shape[0]
+        self.L, self.e, self.refine = L, int(e), refine
+        self.batches = [(int(P.shape[1]), int(P.shape[2]) // BT) for P in batches]
+        self.sizes = [s for nb, s in self.batches for _ in range(nb)]
+        self.lay = lay = Layout(self.sizes)
+        self.b0 = [int(x) for x in np.cumsum([0] + [nb for nb, _ in self.batches])[:-1]]
+        plan = factor_plan(self.sizes, L, self.e, refine)
+
+        def fn(ins):
+            Fa = torch.empty((L, lay.T, BT, BT), dtype=torch.int32, device=dev)
+            for P, b0 in zip(ins, self.b0):
+                dense_to_arena(P.contiguous(), Fa, lay, b0)
+            Xa, xe = run_factor(plan, Fa)
+            return [Fa, Xa, xe]
+        self.Fa, self.Xa, self.xe = graphs.run(("gfactor", L, tuple(self.batches), self.e, refine), fn, list(batches))
+
+    def dense(self, q):
+        """batch q's factor as dense limb planes (L, nb, n, n), zero above the diagonal"""
+        nb, s = self.batches[q]
+        return arena_to_dense(self.Fa, self.lay, self.b0[q], nb, s)
+
+    def diag_tile(self, q, j):
+        """batch q's diagonal tile j: (inverse limbs (L, nb, 32, 32), its exponents (nb,), factor limbs)"""
+        nb, _ = self.batches[q]
+        bs = range(self.b0[q], self.b0[q] + nb)
+        di = torch.tensor([self.lay.diag(b, j) for b in bs], device=dev)
+        ti = torch.tensor([self.lay.tile(b, j, j) for b in bs], device=dev)
+        return self.Xa.index_select(1, di), self.xe.index_select(0, di), self.Fa.index_select(1, ti)
+
+    def diagonal(self, q):
+        """limbs of the diagonal of batch q's factor, (L, nb, n)"""
+        nb, s = self.batches[q]
+        pos = []
+        for b in range(self.b0[q], self.b0[q] + nb):
+            for i in range(BT * s):
+                pos.append(self.lay.tile(b, i // BT, i // BT) * 1024 + (i % BT) * (BT + 1))
+        idx = torch.tensor(pos, device=dev)
+        return self.Fa.view(self.L, -1).index_select(1, idx).view(self.L, nb, BT * s)
+
+
+def factor_from_tiles(Lf, e, Xs, xes):
+    """A Factorisation object over an existing factor: Lf (L, nb, n, n) at exponent e, the diagonal tiles'
+    inverses Xs[j] (L, nb, 32, 32) with exponents xes[j] (nb,) -- the form the reference's bchol returns."""
+    fac = Factorisation.__new__(Factorisation)
+    L, nb, n, _ = Lf.shape
+    s = n // BT
+    fac.L, fac.e, fac.refine = L, int(e), None
+    fac.batches = [(nb, s)]
+    fac.sizes = [s] * nb
+    fac.lay = lay = Layout(fac.sizes)
+    fac.b0 = [0]
+    fac.Fa = torch.empty((L, lay.T, BT, BT), dtype=torch.int32, device=dev)
+    dense_to_arena(Lf.contiguous(), fac.Fa, lay, 0)
+    fac.Xa = torch.empty((L, lay.D, BT, BT), dtype=torch.int32, device=dev)
+    fac.xe = torch.empty((lay.D,), dtype=torch.int64, device=dev)
+    for j in range(s):
+        di = torch.tensor([lay.diag(b, j) for b in range(nb)], device=dev)
+        fac.Xa.index_copy_(1, di, Xs[j].contiguous())
+        fac.xe.index_copy_(0, di, xes[j].contiguous())
+    return fac
+
+
+def right_solve(fac, Bm, refine=1):
+    """X with X L^T = B for fac's one batch: Bm (L, nb, mrows, n) at fac's exponent, n = fac's padded size
+    (sdpvibe/batched.py:291-305): the factorisation's column program on B's row tiles, placed below the
+    factor in a larger arena."""
+    L, nb, mr, n = Bm.shape
+    s = n // BT
+    rb = -(-mr // BT)
+    assert fac.batches == [(nb, s)]
+    lay = Layout([s + rb] * nb)
+    plan = FactorPlan([s + rb] * nb, L, fac.e, refine, tree=[s] * nb, row0=[s] * nb)
+    Fa = torch.zeros((L, lay.T, BT, BT), dtype=torch.int32, device=dev)
+    big = torch.zeros((L, nb, BT * (s + rb), BT * (s + rb)), dtype=torch.int32, device=dev)
+    big[:, :, :n, :n] = arena_to_dense(fac.Fa, fac.lay, 0, nb, s)
+    big[:, :, n:n + mr, :n] = Bm
+    dense_to_arena(big, Fa, lay, 0)
+    Xa = torch.zeros((L, lay.D, BT, BT), dtype=torch.int32, device=dev)
+    xe = torch.zeros((lay.D,), dtype=torch.int64, device=dev)
+    for b in range(nb):
+        Xa[:, lay.diag(b, 0):lay.diag(b, 0) + s] = fac.Xa[:, fac.lay.diag(b, 0):fac.lay.diag(b, 0) + s]
+        xe[lay.diag(b, 0):lay.diag(b, 0) + s] = fac.xe[fac.lay.diag(b, 0):fac.lay.diag(b, 0) + s]
+    run_factor(plan, Fa, Xa, xe)
+    return arena_to_dense(Fa, lay, 0, nb, s + rb)[:, :, n:n + mr, :n].contiguous()
+
+
+def solve(fac, rhs, lower, Fa=None, Xa=None, xe=None):
+    """L^-1 B (lower) or L^-T B for every batch of fac: rhs = [(limbs (L, nb_q, n_q, m), column exponents
+    (nb_q, m))] at the batches' padded sizes, all with the same m; returns the solutions in the same form
+    (sdpvibe/batched.py:322-352 with refine = 0, per block).  Fa, Xa, xe default to fac's arenas (a caller
+    replaying a graph passes its static copies)."""
+    Fa = fac.Fa if Fa is None else Fa
+    Xa = fac.Xa if Xa is None else Xa
+    xe = fac.xe if xe is None else xe
+    L, lay = fac.L, fac.lay
+    m = int(rhs[0][0].shape[-1])
+    plan = solve_plan(fac.sizes, L, fac.e, m, lower)
+    Pa = torch.empty((L, lay.D, BT, m), dtype=torch.int32, device=dev)
+    Pe = torch.empty((lay.D, m), dtype=torch.int64, device=dev)
+    for (Pm, pe), (nb, s), b0 in zip(rhs, fac.batches, fac.b0):
+        r0 = lay.diag(b0, 0)
+        Pa[:, r0:r0 + nb * s].view(L, nb, s * BT, m).copy_(Pm)
+        Pe[r0:r0 + nb * s].view(nb, s, m).copy_(pe[:, None, :].expand(nb, s, m))
+    run_solve(plan, Pa, Pe, Fa, Xa, xe)
+    out = []
+    for (nb, s), b0 in zip(fac.batches, fac.b0):
+        r0 = lay.diag(b0, 0)
+        out.append((Pa[:, r0:r0 + nb * s].reshape(L, nb, s * BT, m), Pe[r0:r0 + nb * s].view(nb, s, m)[:, 0].contiguous()))
+    return out

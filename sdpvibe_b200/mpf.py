@@ -527,122 +527,170 @@ def _fx_one(L, efx):
     return _FX_ONE[key]
 
 
-class Chol:
-    """A = L L^T per block, with L = D^-1 Lt, D = diag(2^-k): Lt fixed point, k integer
-    (sdpvibe/mpf.py:461-532).  A: MPF (n, n) or batched (nb, n, n); padded internally to a multiple of
-    bt with the fixed-point identity."""
+class _Prepared:
+    """One batch (nb, n, n) equilibrated as sdpvibe/mpf.py:467-492 does: k_i = floor((top_ii + 1) / 2), the
+    fixed-point matrix A_ij 2^-(k_i + k_j) at exponent fx_exp(L), padded to npad (a multiple of 32) with the
+    fixed-point identity."""
+
+    def __init__(self, A, bt):
+        L = A.L
+        nb, n, _ = A.shape
+        self.nb, self.n, self.L = nb, n, L
+        idx = torch.arange(n, device=dev)
+        tpd = _top(A)[:, idx, idx]                                  # (nb, n)
+        self.bad = ((A.m[-1][:, idx, idx] < 0) | (tpd <= EZ // 2)).any()
+        self.k = torch.div(tpd + 1, 2, rounding_mode="floor")      # A_ii < 2^(2k)
+        self.npad = max(bt, (n + bt - 1) // bt * bt)
+        efx = fx_exp(L)
+        s = (efx - (A.e - self.k[:, :, None] - self.k[:, None, :])).reshape(-1)
+        s = torch.where(A.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
+        Af = shift_round(A.m.reshape(L, -1), s, L).view(L, nb, n, n)
+        P = torch.zeros((L, nb, self.npad, self.npad), dtype=torch.int32, device=dev)
+        P[:, :, :n, :n] = Af
+        if self.npad > n:
+            ii = torch.arange(n, self.npad, device=dev)
+            P[:, :, ii, ii] = _fx_one(L, efx)[:, None, None]
+        self.P = P
+
+
+class CholGroup:
+    """Cholesky factors of several batches of blocks of different sizes, A_b = L_b L_b^T with L_b = D^-1 Lt_b,
+    D = diag(2^-k) (sdpvibe/mpf.py:461-532), factored together by the grouped work-list engine
+    (``grouped``): one launch sequence for all blocks, each block's factor bit-identical to the reference's
+    Chol of its own batch.  As: list of MPF (nb_i, n_i, n_i) (or (n, n))."""
 
     SOLVE_REFINE = int(os.environ.get("SDPB_GPU_SOLVE_REFINE", "0"))
 
-    def __init__(self, A, bt=32, refine=1, defer_check=False):
-        """defer_check: instead of raising here (one host synchronisation), leave the positivity flag of
-        the diagonal in self.bad (a device bool) for the caller to test later with others at once."""
-        from .batched import BMP, bchol
-        self.two_d = A.e.dim() == 2
-        if self.two_d:
-            A = MPF(A.m[:, None], A.e[None])
-        nb, n, _ = A.shape
-        L = A.L
-        self.nb, self.n, self.L, self.bt, self.refine = nb, n, L, bt, refine
-        idx = torch.arange(n, device=dev)
-        tpd = _top(A)[:, idx, idx]                                  # (nb, n)
-        bad = ((A.m[-1][:, idx, idx] < 0) | (tpd <= EZ // 2)).any()
-        self.bad = bad
-        if not defer_check and bool(bad):                           # one host sync
+    def __init__(self, As, bt=32, refine=1, defer_check=False):
+        from . import grouped
+        if bt != 32:
+            raise ValueError("the base tiles are 32 x 32")
+        if self.SOLVE_REFINE:
+            raise ValueError("SDPB_GPU_SOLVE_REFINE: the grouped triangular solves implement refine = 0 only")
+        self.two_d = [A.e.dim() == 2 for A in As]
+        As = [MPF(A.m[:, None], A.e[None]) if t else A for A, t in zip(As, self.two_d)]
+        self.L = L = As[0].L
+        self.bt, self.refine = bt, refine
+        self.efx = fx_exp(L)
+        self.prep = [_Prepared(A, bt) for A in As]
+        self.bad = torch.stack([p.bad for p in self.prep]).any() if len(self.prep) > 1 else self.prep[0].bad
+        if not defer_check and bool(self.bad):                      # one host sync
             raise ValueError("matrix is not positive definite (diagonal)")
-        k = torch.div(tpd + 1, 2, rounding_mode="floor")            # A_ii < 2^(2k)
-        self.k = k
-        npad = max(bt, (n + bt - 1) // bt * bt)
-        self.npad = npad
-        efx = fx_exp(L)
-        s = (efx - (A.e - k[:, :, None] - k[:, None, :])).reshape(-1)
-        s = torch.where(A.e.reshape(-1) == EZ, torch.full_like(s, 1 << 30), s)
-        Af = shift_round(A.m.reshape(L, -1), s, L).view(L, nb, n, n)
-        P = torch.zeros((L, nb, npad, npad), dtype=torch.int32, device=dev)
-        P[:, :, :n, :n] = Af
-        if npad > n:
-            onefx = _fx_one(L, efx)
-            ii = torch.arange(n, npad, device=dev)
-            P[:, :, ii, ii] = onefx[:, None, None]
-        self.Lt, self.tiles = graphs.run(("bchol", L, nb, npad, bt, refine, efx),
-                                         lambda ins: bchol(BMP(ins[0], efx), bt, refine), [P])
+        self.fac = grouped.Factorisation([p.P for p in self.prep], self.efx, refine)
 
-    def _to_bmp(self, B):
-        from .batched import BMP
+    def _solve_all(self, lower, Bs):
+        """L^-1 B (lower) or L^-T B for one right-hand-side batch per factored batch, all in one grouped solve"""
+        from . import grouped
+        Bs = [MPF(B.m[:, None], B.e[None]) if t else B for B, t in zip(Bs, self.two_d)]
+        m = Bs[0].shape[-1]
+        assert all(B.shape[-1] == m for B in Bs), "one right-hand-side count per grouped solve"
         L = self.L
-        Bm, cE = _align_rows(B.T)                                   # per column of B: (L, nb, m, n)
-        P = torch.zeros((L, self.nb, self.npad, B.shape[-1]), dtype=torch.int32, device=dev)
-        P[:, :, :self.n] = Bm.transpose(2, 3)
-        return BMP(P, cE)
-
-    def _from_bmp(self, P):
-        L = self.L
-        m = P.shape[2]
-        X = P.limbs[:, :, :self.n].reshape(L, -1)
-        ein = P.expt()[:, None, :].expand(self.nb, self.n, m).reshape(-1)
-        return normalize(X.contiguous(), ein.contiguous(), L).reshape(self.nb, self.n, m)
-
-    def _io(self, B, f):
-        if self.two_d:
-            r = f(MPF(B.m[:, None], B.e[None]))
-            return MPF(r.m[:, 0], r.e[0])
-        return f(B)
-
-    def _solve(self, lower, B):
-        """L^-1 B (lower) or L^-T B on batched B, replayed as a CUDA graph for repeated shapes"""
-        from .batched import btrsm_left, btrsm_left_T
-        state = []
-        sk = graphs._flatten((self.Lt, self.tiles), state)
+        state = [self.fac.Fa, self.fac.Xa, self.fac.xe]
+        ins = [t for B, p in zip(Bs, self.prep) for t in (B.m.contiguous(), B.e.contiguous(), p.k)] + state
+        shapes = tuple((p.nb, p.n, p.npad) for p in self.prep)
 
         def fn(ins):
-            Bm, Be, k = ins[0], ins[1], ins[2]
-            Lt, tiles = graphs._rebuild(sk, iter(ins[3:]))
-            if lower:                                               # Lt^-1 (D B)
-                P = btrsm_left(Lt, self._to_bmp(MPF(Bm, Be).shift(-k[:, :, None])), tiles, self.bt,
-                               self.SOLVE_REFINE)
-                return self._from_bmp(P)
-            P = btrsm_left_T(Lt, self._to_bmp(MPF(Bm, Be)), tiles, self.bt, self.SOLVE_REFINE)
-            return self._from_bmp(P).shift(-k[:, :, None])            # D (Lt^-T B)
-        key = ("solve", lower, self.L, self.nb, self.n, self.npad, self.bt, self.SOLVE_REFINE, B.shape, sk)
-        return graphs.run(key, fn, [B.m.contiguous(), B.e.contiguous(), self.k] + state)
+            rhs = []
+            for q, p in enumerate(self.prep):
+                Bm, Be, k = ins[3 * q:3 * q + 3]
+                B = MPF(Bm, Be).shift(-k[:, :, None]) if lower else MPF(Bm, Be)
+                Am, cE = _align_rows(B.T)                          # per column: (L, nb, m, n)
+                Pm = torch.zeros((L, p.nb, p.npad, m), dtype=torch.int32, device=dev)
+                Pm[:, :, :p.n] = Am.transpose(2, 3)
+                rhs.append((Pm, cE))
+            Fa, Xa, xe = ins[3 * len(self.prep):]
+            outs = grouped.solve(self.fac, rhs, lower, Fa, Xa, xe)
+            res = []
+            for p, (Pm, pe) in zip(self.prep, outs):
+                X = Pm[:, :, :p.n].reshape(L, -1)
+                ein = pe[:, None, :].expand(p.nb, p.n, m).reshape(-1)
+                Y = normalize(X.contiguous(), ein.contiguous(), L).reshape(p.nb, p.n, m)
+                res.append(Y.m)
+                res.append(Y.e)
+            return res
+
+        def post(q, Y):
+            return Y if lower else Y.shift(-self.prep[q].k[:, :, None])
+        key = ("gsolve", lower, L, shapes, m, self.efx)
+        flat = graphs.run(key, fn, ins)
+        out = []
+        for q, t in enumerate(self.two_d):
+            Y = post(q, MPF(flat[2 * q], flat[2 * q + 1]))
+            out.append(MPF(Y.m[:, 0], Y.e[0]) if t else Y)
+        return out
+
+    def solve_lower(self, Bs):
+        """L^-1 B = Lt^-1 (D B) for each batch"""
+        return self._solve_all(True, Bs)
+
+    def solve_upper(self, Bs):
+        """L^-T B = D (Lt^-T B) for each batch"""
+        return self._solve_all(False, Bs)
+
+    def solve(self, Bs):
+        """A^-1 B for each batch"""
+        return self.solve_upper(self.solve_lower(Bs))
+
+
+class Chol(CholGroup):
+    """A = L L^T per block, with L = D^-1 Lt, D = diag(2^-k): Lt fixed point, k integer
+    (sdpvibe/mpf.py:461-532).  A: MPF (n, n) or batched (nb, n, n); padded internally to a multiple of
+    bt with the fixed-point identity.  defer_check: instead of raising here (one host synchronisation),
+    leave the positivity flag of the diagonal in self.bad (a device bool) for the caller to test later."""
+
+    def __init__(self, A, bt=32, refine=1, defer_check=False):
+        super().__init__([A], bt, refine, defer_check)
+        p = self.prep[0]
+        self.nb, self.n, self.npad, self.k = p.nb, p.n, p.npad, p.k
+        if self.two_d[0]:
+            self.k = p.k                                           # (1, n): as the reference's 3-d view
+
+    @property
+    def Lt(self):
+        """the fixed-point factor as a BMP (L, nb, npad, npad) at exponent fx_exp(L) (zero above the diagonal)"""
+        from .batched import BMP
+        return BMP(self.fac.dense(0), self.efx)
+
+    @property
+    def tiles(self):
+        """the diagonal tiles' factors and inverses, in order (each a BTile: X with one exponent per block)"""
+        from .batched import BMP, BTile
+        out = []
+        for j in range(self.npad // 32):
+            Xm, xe, Lm = self.fac.diag_tile(0, j)
+            t = BTile()
+            t.X = BMP(Xm, xe[:, None].expand(self.nb, 32).contiguous())
+            t.Lmp = BMP(Lm, self.efx)
+            out.append(t)
+        return out
+
+    def diag_limbs(self):
+        """limbs of the diagonal of the fixed-point factor, (L, nb, n)"""
+        return self.fac.diagonal(0)[:, :, :self.n]
 
     def solve_lower(self, B):
         """L^-1 B = Lt^-1 (D B)"""
-        return self._io(B, lambda B: self._solve(True, B))
+        return self._solve_all(True, [B])[0]
 
     def solve_upper(self, B):
         """L^-T B = D (Lt^-T B)"""
-        return self._io(B, lambda B: self._solve(False, B))
+        return self._solve_all(False, [B])[0]
 
     def solve(self, B):
         """A^-1 B"""
         return self.solve_upper(self.solve_lower(B))
 
 
-_BUCKET_STREAMS = []
-
-
 def chol_solve_many(pairs):
-    """[(A_b, B_b)] -> [A_b^-1 B_b] for independent batched systems (the reference's callers make one
-    Chol + solve per bucket of blocks of equal padded size).  Each system runs on its own CUDA stream, so
-    the latency-bound factorisations of different buckets overlap; the results are those of the same calls
-    made one after the other.  The positivity checks of all factorisations are read at the end, in one
-    transfer (ValueError as Chol raises it)."""
-    main = torch.cuda.current_stream()
-    while len(_BUCKET_STREAMS) < len(pairs):
-        _BUCKET_STREAMS.append(torch.cuda.Stream())
-    start = torch.cuda.Event()
-    start.record(main)
-    outs, bads = [], []
-    for (A, B), st in zip(pairs, _BUCKET_STREAMS):
-        st.wait_event(start)
-        with torch.cuda.stream(st):
-            ch = Chol(A, defer_check=True)
-            bads.append(ch.bad.reshape(1))
-            outs.append(ch.solve(B))
-    for st in _BUCKET_STREAMS[:len(pairs)]:
-        main.wait_stream(st)
-    if bads and bool(torch.cat(bads).any()):
+    """[(A_b, B_b)] -> [A_b^-1 B_b] for independent batched systems of different block sizes (the reference's
+    callers make one Chol + solve per bucket of blocks of equal padded size).  All batches are factored and
+    solved together by the grouped engine -- one work-list launch sequence, no buckets; the results are those
+    of the separate calls.  The positivity checks are read at the end, in one transfer (ValueError as Chol
+    raises it)."""
+    if not pairs:
+        return []
+    ch = CholGroup([A for A, _ in pairs], defer_check=True)
+    out = ch.solve([B for _, B in pairs])
+    if bool(ch.bad):
         raise ValueError("matrix is not positive definite (diagonal)")
-    return outs
-
+    return out

@@ -460,10 +460,9 @@ def fmt_big(v, digits):
 def chol_log2_cond_parts(ch):
     """(max, min) over the diagonal of L (log2) of a factorisation (sdpvibe/solver.py:548-555)"""
     L = ch.L
-    i = torch.arange(ch.n, device=dev)
-    d = ch.Lt.limbs[:, :, i, i]
+    d = ch.diag_limbs()
     top = d[-1].double() * 2.0 ** 32 + (d[-2].double() % 2.0 ** 32) if L > 1 else d[-1].double()
-    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.Lt.exp + 32 * (L - 2)) + ch.k.double()
+    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.efx + 32 * (L - 2)) + ch.k.double()
     return float(lg.max()), float(lg.min())
 
 
@@ -471,10 +470,9 @@ def chol_log2_cond(ch, mask=None):
     """per block log2 of SDPB's Cholesky condition estimate (max / min diagonal of L)^2, over the rows
     where mask (nb, n) is True (sdpvibe/solver.py:563-576)"""
     L = ch.L
-    i = torch.arange(ch.n, device=dev)
-    d = ch.Lt.limbs[:, :, i, i]
+    d = ch.diag_limbs()
     top = d[-1].double() * 2.0 ** 32 + (d[-2].double() % 2.0 ** 32) if L > 1 else d[-1].double()
-    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.Lt.exp + 32 * (L - 2)) + ch.k.double()
+    lg = torch.log2(torch.clamp(top, min=1e-300)) + (ch.efx + 32 * (L - 2)) + ch.k.double()
     if mask is None:
         mask = torch.ones_like(lg, dtype=torch.bool)
     hi = torch.where(mask, lg, torch.full_like(lg, -1e300)).amax(1)
