@@ -508,6 +508,13 @@ def run_gemm(args, rank, world, local_rank):
 
 # ------------------------------------------------------------------ batched Cholesky + solve workload
 CS_BLOCKS, CS_NMIN, CS_NMAX, CS_NRHS, CS_L = 600, 8, 160, 8, 26
+# library entry points whose launches the per-kernel tables time
+TRACE_NAMES = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows",
+               "sdpv_rns_gemm", "sdpv_rns_gemm_grouped", "sdpv_crt_norm", "sdpv_crt_block", "sdpv_shift_round",
+               "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align", "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add",
+               "sdpv_top_max", "sdpv_align", "sdpv_align_t", "sdpv_align_rows", "sdpv_grp_copy", "sdpv_grp_finish_fixed",
+               "sdpv_grp_solve_round", "sdpv_grp_merge", "sdpv_grp_tile_widen",
+               "sdpv_grp_tile_narrow")
 
 
 def cholsolve_macs(ns):
@@ -542,8 +549,10 @@ def cholsolve_cpu_baseline(ns, threads, every=20):
 
 def run_cholsolve(args, rank, world, local_rank):
     """600 SPD blocks A = G G^T + n I (n ~ U[8,160], numpy seed 0, float64 values exact in MPF), L = 26,
-    8 right-hand sides: one batched Chol + solve per padded size (32..160), as the reference's callers
-    group blocks.  Metric: mp-MAC/s over the unpadded work sum n^3/6 + 2 * 8 n^2 / 2."""
+    8 right-hand sides, each block padded to its own multiple of 32 (the reference's callers make one batched
+    Chol + solve per padded size 32..160; here all 600 blocks are factored and solved together by the grouped
+    work-list engine, with every block's result that of its own bucket's call).  Metric: mp-MAC/s over the
+    unpadded work sum n^3/6 + 2 * 8 n^2 / 2."""
     import torch
     from sdpvibe_b200 import mpf, _trace
     from sdpvibe_b200.kernel_bench import cholsolve_inputs, cholsolve_buckets
@@ -559,7 +568,7 @@ def run_cholsolve(args, rank, world, local_rank):
     h2d = sum(sum(t.numel() * t.element_size() for t in p) for p in pinned)
     d2h = sum(a.numel() * 4 + b.numel() * 8 for a, b in outs)
 
-    def step():                                  # the buckets' systems on concurrent streams
+    def step():                                  # all blocks in one grouped factorisation and solve
         mpf.chol_solve_many([(A, B) for _, _, A, B in buckets])
 
     def step_e2e():
@@ -581,10 +590,7 @@ def run_cholsolve(args, rank, world, local_rank):
         return s.elapsed_time(e)
     for _ in range(max(args.warmup, 3)):
         step()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
-             "sdpv_crt_norm",
-             "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_t", "sdpv_align_rows")
+    names = TRACE_NAMES
     tr = _trace.Trace(timed=names)
     with ClockSampler(local_rank) as clk:
         ms = timed(step, args.steps, tr)
@@ -592,7 +598,7 @@ def run_cholsolve(args, rank, world, local_rank):
     # per-kernel device time: one eager step (graphs off), every launch bracketed by CUDA events
     from sdpvibe_b200 import graphs
     graphs.ENABLED = False
-    step()                                       # eager allocations on the bucket streams' pools
+    step()                                       # eager allocations
     tr_e = _trace.Trace(timed=names)
     ms_eager = timed(step, 1, tr_e)
     graphs.ENABLED = True
@@ -609,7 +615,7 @@ def run_cholsolve(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32 wide fixed point + int8 residue GEMM",
             "data": "synthetic",
             "config": {"workload": "cholsolve: 600 SPD blocks A = G G^T + n I, n~U[8,160] (numpy seed 0), "
-                                   "8 RHS U(-1,1), L=26, one Chol + solve per padded size (buckets on concurrent streams)",
+                                   "8 RHS U(-1,1), L=26, all blocks in one grouped Chol + solve (no buckets)",
                        "buckets": {int(b[0]): len(b[1]) for b in buckets}, "limbs": CS_LIMBS_NOTE,
                        "l2": "inputs 0.88 GB (larger than L2), no flush"},
             "kernel_ms_per_step_eager": kms, "ms_per_step_eager": ms_eager, "top_kernel": top,
@@ -740,6 +746,40 @@ def run_solver(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_plain(args, rank, world, local_rank):
+    """--impl plain: the reference's own solver and GPU kernels (Triton + its CUDA C strings, per-bucket
+    Cholesky) on this GPU, on the same Ising-structured SDP as --workload solver (baseline/plain_gpu.py);
+    the metric is the same mean s/iteration over iterations 2-20.  Rank 0 only."""
+    if rank != 0 or args.workload != "solver":
+        if rank == 0:
+            print(json.dumps({"impl": "plain", "unavailable": "the plain GPU path is measured for --workload solver"}))
+        return
+    import torch
+    torch.cuda.set_device(local_rank)
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    try:
+        import plain_gpu
+        with ClockSampler(local_rank) as clk:
+            per_it, walls = plain_gpu.run_plain_solver(SOLVER_ITERS)
+    except Exception as ex:                       # noqa: BLE001 -- reported, not raised: a baseline only
+        print(json.dumps({"impl": "plain", "unavailable": f"{type(ex).__name__}: {ex}"[:400]}), flush=True)
+        return
+    timed = per_it[1:]
+    s_it = statistics.mean(timed)
+    line = {"metric": "768-bit SDP s/iter (Ising-structured synthetic SDP, 300 blocks, N=1000)", "impl": "plain",
+            "value": s_it, "unit": "s/iter", "n_gpus": 1, "steps": len(timed), "warmup": 1,
+            "ms_per_step": s_it * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "the reference's int8 residue GEMM (Triton) + int32 fixed point, 832-bit MPF (L=26)",
+            "data": "synthetic",
+            "config": {"workload": "solver: the reference SDPviBe's Solver.run (its Triton and CUDA C kernels, "
+                                   "per-bucket Cholesky, unmodified; CuPy stand-in compiles its CUDA strings with "
+                                   "nvcc; CRT digit-sum tl.dot given out_dtype=int32 in a wrapper) on the same "
+                                   "ising_like SDP (300 blocks, N=1000, L=26)",
+                       "metric_over": f"mean of iterations 2..{len(per_it)}"},
+            "per_iteration_s": per_it, "wall_s_at_iteration": walls, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def _rel_mpf_error(A26, A50):
     """max |A26 - A50| / max |A50| over the entries (A26 widened exactly to A50's limbs, the difference
     formed in MPF on the device)"""
@@ -807,11 +847,7 @@ def solver_measurement(local_rank, world=1, iters=SOLVER_ITERS):
             s.timer.marks.clear()
             tr.launches.clear()
             tr.events.clear()
-    names = ("sdpv_chol_tiles", "sdpv_trinv_tiles", "sdpv_residues", "sdpv_residues_u8", "sdpv_residues_rows", "sdpv_rns_gemm",
-             "sdpv_crt_norm",
-             "sdpv_crt_block", "sdpv_shift_round", "sdpv_add_same", "sdpv_bitlen", "sdpv_badd_align",
-             "sdpv_mpf_norm", "sdpv_mpf_mul", "sdpv_mpf_add", "sdpv_top_max", "sdpv_align", "sdpv_align_t", "sdpv_align_rows")
-    tr = _trace.Trace(timed=names)              # graph replays are timed whole, one entry per graph key
+    tr = _trace.Trace(timed=TRACE_NAMES)        # graph replays are timed whole, one entry per graph key
     with ClockSampler(local_rank) as clk, tr:
         torch.cuda.synchronize()
         start = torch.cuda.Event(enable_timing=True)
@@ -852,7 +888,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--impl", choices=("b200", "reference", "plain"), default="b200",
+                    help="reference: the reference's CPU path; plain: the reference's own GPU solver (solver workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--iters", type=int, default=20, help="sensitivity: solver iterations before the sensitivities")
     ap.add_argument("--fd-dirs", type=int, default=8, help="sensitivity: directions checked by finite differences")
@@ -868,6 +905,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.impl == "plain":
+        return run_plain(args, rank, world, local_rank)
     if world > 1:
         import datetime
         import torch

@@ -259,6 +259,68 @@ int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* V, int64
 int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, int64_t ntiles, int bt, int WL,
                              int LF, void* stream);
 
+/* ---------------------------------------------------------------- grouped Cholesky / triangular solves
+ * The batched Cholesky factorisation and triangular solves of blocks of different sizes run as waves over a
+ * device work list (the host plan of sdpvibe_b200/grouped.py): every entry point below takes a device table
+ * of descriptors whose rows may belong to blocks of any size, so one launch serves all blocks of a wave.
+ * Together they replace the reference's per-bucket recursion bchol / btrsm_right / btrsm_left /
+ * btrsm_left_T (sdpvibe/batched.py:243-352, called per padded block size by mpf.Chol, sdpvibe/mpf.py:461-532)
+ * with results identical block by block.  Arenas are limb planes (plane stride = entries per plane):
+ * factor tiles (L, T, 32, 32), tile inverses (L, D, 32, 32) with exponents xe (D), solve row tiles
+ * (L, RT, 32, m) with exponents Pe (RT, m).
+ *
+ * Grouped narrow residue products (the work-list form of sdpv_rns_gemm): items (8 int32 each: big-side row0,
+ * big rows <= 128, small-side row0, small rows <= TB, K length (multiple of 32, <= KP), output row0, output
+ * column0, 0) multiply rows of the big side (unsigned residue digits, (G, big_rows, KP) planes big_stride
+ * bytes apart) against rows of the small side over their own K; out_mode 1 stores acc[g][out_row0 + r][j],
+ * out_mode 2 acc[g][out_row0 + j][out_col0 + r] (acc (n, rows_out, ldc) int16, fresh).  TB in 16..64,
+ * multiple of 16. */
+int sdpv_rns_gemm_grouped(const sdpv_ctx* ctx, const uint8_t* bigHi, const uint8_t* bigLo, int64_t big_rows,
+                          int64_t big_stride, const uint8_t* smallHi, const uint8_t* smallLo, int64_t small_rows,
+                          int64_t small_stride, int64_t KP, int TB, int out_mode, const int32_t* items, int64_t nitems,
+                          int16_t* acc, int64_t ldc, int64_t rows_out, int g0, int G, void* stream);
+
+/* Block copies into a workspace (L, ., .): desc (8 int64 each: source arena, source base entry, source row
+ * stride, destination base entry, destination row stride, rows <= 32, cols <= 32, transpose); src_host /
+ * src_planes_host: HOST arrays of nsrc (<= 4) arena device pointers and their plane strides. */
+int sdpv_grp_copy(int32_t* const* src_host, const int64_t* src_planes_host, int nsrc, int32_t* dst, int64_t dst_plane,
+                  int L, const int64_t* desc, int64_t ndesc, void* stream);
+
+/* Fixed-exponent rounding of CRT words (W words, planes Ntot apart, entry = row * w + column) combined into
+ * arena blocks: desc (40 int64 each: out arena, out base, out ld, base arena or -1, base base, base ld, rows,
+ * cols, nsrc <= 7, then per source CRT entry base, sign, shift constant, exponent index or -1):
+ * out = base + sum sign round(W / 2^(cst - xe[idx])) mod 2^(32L) -- btrsm_right's and bchol's rounded
+ * products and exact differences (sdpvibe/batched.py:274-305, 82-92). */
+int sdpv_grp_finish_fixed(const int32_t* Wd, int W, int64_t Ntot, int64_t w, int32_t* const* ar_host,
+                          const int64_t* planes_host, int nar, int L, const int64_t* xe, const int64_t* desc,
+                          int64_t ndesc, void* stream);
+
+/* Per-column ('col') rounding of a group of solve outputs: desc (10 int64 each: CRT row0, rows, column0,
+ * ncols <= 32, eA constant, eA index or -1, B row tile, mode, base row tile0, destination row tile0); the
+ * group's column exponent from its rows' maximal bit length, then store (mode 0) or the aligned difference /
+ * sum with the base rows (modes 1 / 2) -- btrsm_left's leaf, update and badd 'align' (sdpvibe/batched.py:
+ * 200-231, 313-352, 55-92). */
+int sdpv_grp_solve_round(const int32_t* Wd, const int64_t* bl, int W, int64_t Ntot, int64_t w, int32_t* P,
+                         int64_t Pplane, int64_t* Pe, int64_t m, int L, const int64_t* xe, const int64_t* desc,
+                         int64_t ndesc, void* stream);
+
+/* Common column exponents of a tree node's row tiles: desc (4 int64 each: row tile0, row tiles, column0,
+ * ncols <= 32); both halves re-rounded to the larger exponent (sdpvibe/batched.py:332-335, 349-352). */
+int sdpv_grp_merge(int32_t* P, int64_t Pplane, int64_t* Pe, int64_t m, int L, const int64_t* desc, int64_t ndesc,
+                   void* stream);
+
+/* Diagonal tiles of the factor arena (entry bases fbase, exponent e) -> wide fixed point (ntiles, 32, 32, WL)
+ * at exponent -32 LF, zero above the diagonal (sdpvibe/batched.py:250). */
+int sdpv_grp_tile_widen(const int32_t* Fa, int64_t Fplane, int L, int64_t e, int WL, int LF, const int64_t* fbase,
+                        int64_t ntiles, uint32_t* out, void* stream);
+
+/* Factored wide tiles (Lw) and their inverses (Xw) back to the arenas: the factor at e (zero above the
+ * diagonal), the inverse at xe[xidx] = max bit length - 32 LF - (32 L - 32) per tile (sdpvibe/batched.py:
+ * 256-262). */
+int sdpv_grp_tile_narrow(const uint32_t* Lw, const uint32_t* Xw, int WL, int LF, int32_t* Fa, int64_t Fplane, int L,
+                         int64_t e, const int64_t* fbase, int32_t* Xa, int64_t Xplane, const int64_t* xidx,
+                         int64_t* xe, int64_t ntiles, void* stream);
+
 /* ---------------------------------------------------------------- errors
  * Read and clear the device error word (bits SDPV_ERRBIT_*) after synchronising `stream`.
  * Replaces limbops.check_errors (sdpvibe/limbops.py:156-169). */

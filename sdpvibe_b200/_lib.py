@@ -62,9 +62,8 @@ _SIGS = {
     "sdpv_rns_gemm_grouped": [_P, _P, _P, _L, _L, _P, _P, _L, _L, _L, _I, _I, _P, _L, _P, _L, _L, _I, _I, _P],
     "sdpv_grp_copy": [_P, _P, _I, _P, _L, _I, _P, _L, _P],
     "sdpv_grp_finish_fixed": [_P, _I, _L, _L, _P, _P, _I, _I, _P, _P, _L, _P],
-    "sdpv_grp_colexp": [_P, _L, _P, _L, _I, _P, _P, _L, _P, _P, _P],
-    "sdpv_grp_solve_finish": [_P, _I, _L, _L, _P, _L, _P, _L, _I, _P, _P, _P, _L, _P],
     "sdpv_grp_merge": [_P, _L, _P, _L, _I, _P, _L, _P],
+    "sdpv_grp_solve_round": [_P, _P, _I, _L, _L, _P, _L, _P, _L, _I, _P, _P, _L, _P],
     "sdpv_grp_tile_widen": [_P, _L, _I, _L, _I, _I, _P, _L, _P, _P],
     "sdpv_grp_tile_narrow": [_P, _P, _I, _I, _P, _L, _I, _L, _P, _P, _L, _P, _P, _L, _P],
     "sdpv_device_status": [_P],

@@ -9,8 +9,8 @@
 //   workspaces     (L, rows, KP)   operand rows gathered for one grouped residue product.
 // The kernels: tile copies into workspaces (grp_copy, optional transpose, shared-memory staged), the rounding
 // of CRT outputs to a fixed exponent combined into a destination (grp_finish_fixed), the solves' per-column
-// exponents, rounding, aligned sums and rescales (grp_colexp, grp_solve_finish, grp_merge), and the tile
-// conversions around the base-case kernels (grp_tile_widen, grp_tile_narrow).  Roundings are the reference's:
+// exponents, rounding and aligned sums (grp_solve_round) and rescales (grp_merge), and the tile conversions
+// around the base-case kernels (grp_tile_widen, grp_tile_narrow).  Roundings are the reference's:
 // floor(x / 2^s + 1/2) on two's-complement words (sdpvibe/limbops.py:31-62), the aligned sum of two operands
 // rounded independently to max(ea, eb) + 1 (sdpvibe/batched.py:55-79), per-column output exponents from the
 // maximal bit length (sdpvibe/batched.py:200-231).
@@ -78,8 +78,8 @@ __device__ __forceinline__ int bitlen_words(const u32* x, int n) {
 
 // ---------------------------------------------------------------- tile copies into a workspace
 // desc (8 int64): src arena, src base entry, src row stride, dst base entry, dst row stride, rows, cols (<= 32),
-// transpose.  One CTA per descriptor; dst[r][c] = src[r][c], or dst[c][r] = src[r][c] staged through shared
-// memory so that both sides are read / written along rows.
+// transpose.  One CTA per descriptor and limb plane (grid y); dst[r][c] = src[r][c], or dst[c][r] = src[r][c]
+// staged through shared memory so that both sides are read / written along rows.
 __global__ void __launch_bounds__(256) grp_copy_kernel(Arenas src, int32_t* __restrict__ dst, i64 dplane, int L,
                                                        const i64* __restrict__ desc) {
   __shared__ int32_t t[32][33];
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256) grp_copy_kernel(Arenas src, int32_t* __re
   const int sid = (int)d[0], rows = (int)d[5], cols = (int)d[6], trans = (int)d[7];
   const i64 sbase = d[1], sld = d[2], dbase = d[3], dld = d[4];
   const int tid = threadIdx.x;
-  for (int k = 0; k < L; k++) {
+  for (int k = blockIdx.y; k < L; k += gridDim.y) {
     const int32_t* S = src.p[sid] + (i64)k * src.plane[sid] + sbase;
     int32_t* D = dst + (i64)k * dplane + dbase;
     if (!trans) {
@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(256) grp_copy_kernel(Arenas src, int32_t* __re
 // desc (40 int64): out arena, out base, out ld, base arena (-1: zero), base base, base ld, rows, cols, nsrc (<= 7),
 // then per source: CRT entry base, sign (+1 / -1), shift constant, exponent index (-1: none).  Entry (r, c):
 //   out = base + sum_i sign_i round(W_i[r][c] / 2^s_i) mod 2^(32 L),  s_i = cst_i - xe[idx_i]
-// where W_i[r][c] is the CRT value (W words, planes Ntot apart) at entry crt_base_i + r * w + c.
+// where W_i[r][c] is the CRT value (W words, planes Ntot apart) at entry crt_base_i + r * w + c.  Four CTAs
+// per descriptor (grid y), each a quarter of the rows: one entry per thread for a 32 x 32 block.
 __global__ void __launch_bounds__(256) grp_finish_fixed_kernel(const int32_t* __restrict__ Wd, int W, i64 Ntot, i64 w,
                                                                Arenas ar, int L, const i64* __restrict__ xe,
                                                                const i64* __restrict__ desc) {
@@ -122,8 +123,10 @@ __global__ void __launch_bounds__(256) grp_finish_fixed_kernel(const int32_t* __
   const int oid = (int)d[0], bid = (int)d[3], rows = (int)d[6], cols = (int)d[7];
   const int ns = (int)d[8] < kMaxSrc ? (int)d[8] : kMaxSrc;
   const i64 obase = d[1], old_ = d[2], bbase = d[4], bld = d[5];
-  for (int idx = threadIdx.x; idx < rows * cols; idx += blockDim.x) {
-    const int r = idx / cols, c = idx - r * cols;
+  const int rpart = (rows + gridDim.y - 1) / gridDim.y, rlo = blockIdx.y * rpart;   // this CTA's rows
+  const int rhi = rlo + rpart < rows ? rlo + rpart : rows;
+  for (int idx = threadIdx.x; idx < (rhi - rlo) * cols; idx += blockDim.x) {
+    const int r = rlo + idx / cols, c = idx % cols;
     ShiftStream st[kMaxSrc];
     i64 sg[kMaxSrc];
     const int32_t* src[kMaxSrc];
@@ -151,90 +154,89 @@ __global__ void __launch_bounds__(256) grp_finish_fixed_kernel(const int32_t* __
   }
 }
 
-// ---------------------------------------------------------------- triangular solves: per-column exponents
-// desc (8 int64): CRT row0, rows, column c0, ncols (<= 32), eA constant, eA index (-1 none, else + xe[idx]),
-// B row tile (its column exponents Pe[rt][c]), group.  For each column c:
-//   mx = max over the rows of the CRT bit length;  s = mx - (32 L - 32);  e_in = eA + Pe[rt][c];
-//   sU[group][c] = s, eU[group][c] = e_in + s          ('col' rounding, sdpvibe/batched.py:200-231)
-__global__ void grp_colexp_kernel(const i64* __restrict__ bl, i64 w, const i64* __restrict__ Pe, i64 m, int L,
-                                  const i64* __restrict__ xe, const i64* __restrict__ desc, i64* __restrict__ sU,
-                                  i64* __restrict__ eU) {
-  const i64* d = desc + 8 * (i64)blockIdx.x;
-  const int c = threadIdx.x;
-  if (c >= (int)d[3]) return;
-  const i64 row0 = d[0], rows = d[1], col = d[2] + c, g = d[7];
+// ---------------------------------------------------------------- triangular solves: fused 'col' rounding
+// desc (10 int64): CRT row0, rows (32 nrt), column c0, ncols (<= 32), eA constant, eA index (-1 none, else +
+// xe[idx]), B row tile (its column exponents), mode, base row tile 0, destination row tile 0.  One CTA per
+// group and column chunk: for each column c, mx = max over the group's rows of the CRT bit length,
+// s = mx - (32 L - 32), e_in = eA + Pe[B row tile][c], eU = e_in + s ('col' rounding, sdpvibe/batched.py:
+// 200-231); then every entry u = round(U / 2^s) goes to the destination row tiles dst0 .. dst0 + nrt - 1:
+// mode 0 stores it (exponent eU), modes 1 / 2 form the aligned difference / sum with the base row tiles
+// base0 .. (exponent eb): e2 = max(eb, eU) + 1, round(b / 2^(e2 - eb)) -/+ round(u / 2^(e2 - eU))
+// (sdpvibe/batched.py:82-92).
+__global__ void __launch_bounds__(256) grp_solve_round_kernel(const int32_t* __restrict__ Wd, const i64* __restrict__ bl,
+                                                              int W, i64 Ntot, i64 w, int32_t* __restrict__ P,
+                                                              i64 Pplane, i64* __restrict__ Pe, i64 m, int L,
+                                                              const i64* __restrict__ xe,
+                                                              const i64* __restrict__ desc) {
+  __shared__ i64 s_part[8][32];
+  __shared__ i64 s_su[32], s_eu[32];
+  const i64* d = desc + 10 * (i64)blockIdx.x;
+  const i64 row0 = d[0], rows = d[1], c0 = d[2], brt0 = d[8], drt0 = d[9];
+  const int ncols = (int)d[3], mode = (int)d[7];
+  const int tid = threadIdx.x, c = tid & 31, rg = tid >> 5;
   i64 mx = 0;
-  for (i64 r = 0; r < rows; r++) {
-    const i64 v = bl[(row0 + r) * w + col];
-    mx = v > mx ? v : mx;
-  }
-  const i64 eA = d[4] + (d[5] >= 0 ? xe[d[5]] : 0);
-  const i64 s = mx - (32 * (i64)L - 32);
-  sU[g * m + col] = s;
-  eU[g * m + col] = eA + Pe[d[6] * m + col] + s;
-}
-
-// ---------------------------------------------------------------- triangular solves: rounding into the arena
-// desc (8 int64): CRT row0 of the row tile, column c0, ncols (<= 32), group, mode, base row tile, destination
-// row tile, rows (32).  Solve arena entry (rt, r, c) at rt * 32 m + r * m + c of each limb plane.
-//   mode 0: P[dst] = round(U / 2^sU), Pe[dst] = eU                         (a leaf's product)
-//   mode 1 / 2: with u = round(U / 2^sU) at eU and the base operand b at eb = Pe[base]:
-//      e2 = max(eb, eU) + 1;  P[dst] = round(b / 2^(e2-eb)) -/+ round(u / 2^(e2-eU));  Pe[dst] = e2
-//   (the aligned difference / sum of sdpvibe/batched.py:82-92).  A CTA handles its 32 columns of one row tile,
-//   so the exponents it reads and writes are its own.
-__global__ void __launch_bounds__(256) grp_solve_finish_kernel(const int32_t* __restrict__ Wd, int W, i64 Ntot, i64 w,
-                                                               int32_t* __restrict__ P, i64 Pplane, i64* __restrict__ Pe,
-                                                               i64 m, int L, const i64* __restrict__ sU,
-                                                               const i64* __restrict__ eU,
-                                                               const i64* __restrict__ desc) {
-  __shared__ i64 s_eb[32], s_e2[32], s_su[32], s_eu[32];
-  const i64* d = desc + 8 * (i64)blockIdx.x;
-  const i64 row0 = d[0], c0 = d[1], g = d[3], brt = d[5], drt = d[6];
-  const int ncols = (int)d[2], mode = (int)d[4], rows = (int)d[7];
-  if (threadIdx.x < ncols) {
-    const int c = threadIdx.x;
-    const i64 su = sU[g * m + c0 + c], eu = eU[g * m + c0 + c];
-    s_su[c] = su;
-    s_eu[c] = eu;
-    if (mode) {
-      const i64 eb = Pe[brt * m + c0 + c];
-      s_eb[c] = eb;
-      s_e2[c] = (eb > eu ? eb : eu) + 1;
+  if (c < ncols)
+    for (i64 r = rg; r < rows; r += 8) {
+      const i64 v = bl[(row0 + r) * w + c0 + c];
+      mx = v > mx ? v : mx;
     }
+  s_part[rg][c] = mx;
+  __syncthreads();
+  if (tid < ncols) {
+    i64 v = s_part[0][tid];
+    for (int q = 1; q < 8; q++) v = s_part[q][tid] > v ? s_part[q][tid] : v;
+    const i64 s = v - (32 * (i64)L - 32);
+    const i64 eA = d[4] + (d[5] >= 0 ? xe[d[5]] : 0);
+    s_su[tid] = s;
+    s_eu[tid] = eA + Pe[d[6] * m + c0 + tid] + s;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < rows * ncols; idx += blockDim.x) {
-    const int r = idx / ncols, c = idx - r * ncols;
-    const int32_t* u = Wd + (row0 + r) * w + c0 + c;
+  const i64 nrt = rows / 32;
+  for (i64 idx = tid; idx < rows * ncols; idx += blockDim.x) {
+    const int cc = (int)(idx % ncols);
+    const i64 rr = idx / ncols, t = rr / 32, r = rr % 32;
+    const int32_t* u = Wd + (row0 + rr) * w + c0 + cc;
     auto uat = [&](i64 k) { return (u32)u[k * Ntot]; };
-    int32_t* dst = P + drt * 32 * m + (i64)r * m + c0 + c;
+    int32_t* dst = P + (drt0 + t) * 32 * m + r * m + c0 + cc;
     if (mode == 0) {
       ShiftStream st;
-      shr_begin(st, uat, W, s_su[c]);
+      shr_begin(st, uat, W, s_su[cc]);
       for (int k = 0; k < L; k++) dst[(i64)k * Pplane] = (int32_t)shr_next(st, uat, W, k);
       continue;
     }
     u32 uv[kLMax];
-    shr_all(uat, W, s_su[c], uv, L);
-    const int32_t* b = P + brt * 32 * m + (i64)r * m + c0 + c;
+    shr_all(uat, W, s_su[cc], uv, L);
+    const i64 eb = Pe[(brt0 + t) * m + c0 + cc];
+    const i64 eu = s_eu[cc];
+    const i64 e2 = (eb > eu ? eb : eu) + 1;
+    const int32_t* b = P + (brt0 + t) * 32 * m + r * m + c0 + cc;
     auto bat = [&](i64 k) { return (u32)b[k * Pplane]; };
     auto vat = [&](i64 k) { return uv[k]; };
     ShiftStream sb, su;
-    shr_begin(sb, bat, L, s_e2[c] - s_eb[c]);
-    shr_begin(su, vat, L, s_e2[c] - s_eu[c]);
+    shr_begin(sb, bat, L, e2 - eb);
+    shr_begin(su, vat, L, e2 - eu);
     const i64 sgn = mode == 1 ? -1 : 1;
     i64 carry = 0;
     u32 out[kLMax];
     for (int k = 0; k < L; k++) {
       const u32 x = shr_next(sb, bat, L, k), y = shr_next(su, vat, L, k);
-      const i64 t = (i64)x + sgn * (i64)y + carry;
-      out[k] = (u32)t;
-      carry = t >> 32;
+      const i64 tt = (i64)x + sgn * (i64)y + carry;
+      out[k] = (u32)tt;
+      carry = tt >> 32;
     }
-    for (int k = 0; k < L; k++) dst[(i64)k * Pplane] = (int32_t)out[k];   // after every read of the base
+    for (int k = 0; k < L; k++) dst[(i64)k * Pplane] = (int32_t)out[k];
   }
   __syncthreads();
-  if (threadIdx.x < ncols) Pe[drt * m + c0 + threadIdx.x] = mode ? s_e2[threadIdx.x] : s_eu[threadIdx.x];
+  if (tid < ncols) {
+    for (i64 t = 0; t < nrt; t++) {
+      i64 e = s_eu[tid];
+      if (mode) {
+        const i64 eb = Pe[(brt0 + t) * m + c0 + tid];
+        e = (eb > e ? eb : e) + 1;
+      }
+      Pe[(drt0 + t) * m + c0 + tid] = e;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- triangular solves: common column exponents
@@ -363,8 +365,9 @@ extern "C" int sdpv_grp_copy(int32_t* const* src_host, const int64_t* src_planes
       ndesc > 0x7fffffff || (ndesc && !desc))
     return SDPV_EINVAL;
   if (ndesc == 0) return SDPV_OK;
-  grp_copy_kernel<<<(unsigned)ndesc, 256, 0, sdpv::as_stream(stream)>>>(make_arenas(src_host, src_planes_host, nsrc),
-                                                                         dst, dst_plane, L, desc);
+  const dim3 grid((unsigned)ndesc, (unsigned)(L < 65535 ? L : 65535));
+  grp_copy_kernel<<<grid, 256, 0, sdpv::as_stream(stream)>>>(make_arenas(src_host, src_planes_host, nsrc), dst,
+                                                              dst_plane, L, desc);
   return sdpv::launch_status();
 }
 
@@ -375,29 +378,20 @@ extern "C" int sdpv_grp_finish_fixed(const int32_t* Wd, int W, int64_t Ntot, int
       ndesc > 0x7fffffff || (ndesc && !desc))
     return SDPV_EINVAL;
   if (ndesc == 0) return SDPV_OK;
-  grp_finish_fixed_kernel<<<(unsigned)ndesc, 256, 0, sdpv::as_stream(stream)>>>(
+  grp_finish_fixed_kernel<<<dim3((unsigned)ndesc, 4), 256, 0, sdpv::as_stream(stream)>>>(
       Wd, W, Ntot, w, make_arenas(ar_host, planes_host, nar), L, xe, desc);
   return sdpv::launch_status();
 }
 
-extern "C" int sdpv_grp_colexp(const int64_t* bl, int64_t w, const int64_t* Pe, int64_t m, int L, const int64_t* xe,
-                               const int64_t* desc, int64_t ndesc, int64_t* sU, int64_t* eU, void* stream) {
-  if (!bl || !Pe || !sU || !eU || m < 1 || L < 1 || ndesc < 0 || ndesc > 0x7fffffff || (ndesc && !desc))
-    return SDPV_EINVAL;
-  if (ndesc == 0) return SDPV_OK;
-  grp_colexp_kernel<<<(unsigned)ndesc, 32, 0, sdpv::as_stream(stream)>>>(bl, w, Pe, m, L, xe, desc, sU, eU);
-  return sdpv::launch_status();
-}
-
-extern "C" int sdpv_grp_solve_finish(const int32_t* Wd, int W, int64_t Ntot, int64_t w, int32_t* P, int64_t Pplane,
-                                     int64_t* Pe, int64_t m, int L, const int64_t* sU, const int64_t* eU,
-                                     const int64_t* desc, int64_t ndesc, void* stream) {
-  if (!Wd || W < 1 || !P || !Pe || m < 1 || L < 1 || L > kLMax || ndesc < 0 || ndesc > 0x7fffffff ||
+extern "C" int sdpv_grp_solve_round(const int32_t* Wd, const int64_t* bl, int W, int64_t Ntot, int64_t w, int32_t* P,
+                                    int64_t Pplane, int64_t* Pe, int64_t m, int L, const int64_t* xe, const int64_t* desc,
+                                    int64_t ndesc, void* stream) {
+  if (!Wd || !bl || W < 1 || !P || !Pe || m < 1 || L < 1 || L > kLMax || ndesc < 0 || ndesc > 0x7fffffff ||
       (ndesc && !desc))
     return SDPV_EINVAL;
   if (ndesc == 0) return SDPV_OK;
-  grp_solve_finish_kernel<<<(unsigned)ndesc, 256, 0, sdpv::as_stream(stream)>>>(Wd, W, Ntot, w, P, Pplane, Pe, m, L,
-                                                                                 sU, eU, desc);
+  grp_solve_round_kernel<<<(unsigned)ndesc, 256, 0, sdpv::as_stream(stream)>>>(Wd, bl, W, Ntot, w, P, Pplane, Pe, m, L,
+                                                                                xe, desc);
   return sdpv::launch_status();
 }
 

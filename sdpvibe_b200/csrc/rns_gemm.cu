@@ -447,15 +447,57 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool fail = epi_sync_or(!ok_me);
       if (fail) break;
       tc_fence_after();
+      if (gtab && (q * 32 >= big || j0 >= small)) {       // no valid output in this warp's lanes / columns
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
+        continue;
+      }
       u32 hh[32], hx[32], ll[32];
       const u32 base = tmem + buf * 256 + ((u32)(q * 32) << 16) + j0;
-      tmem_ld32(base, hh);
-      tmem_ld32(base + TB, hx);
-      tmem_ld32(base + 2 * TB, ll);
+      if (half <= 16) {                                  // TB <= 32: a 16-column load suffices
+        tmem_ld16(base, *reinterpret_cast<u32(*)[16]>(hh));
+        tmem_ld16(base + TB, *reinterpret_cast<u32(*)[16]>(hx));
+        tmem_ld16(base + 2 * TB, *reinterpret_cast<u32(*)[16]>(ll));
+      } else {
+        tmem_ld32(base, hh);
+        tmem_ld32(base + TB, hx);
+        tmem_ld32(base + 2 * TB, ll);
+      }
       tmem_ld_wait();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
+      if (gtab && nmode == 1 && half == 16 && fresh && u8ops && gtab[8 * t + 4] <= 64) {
+        // grouped items of 32 small-side rows and K <= 64 on unsigned digits: ll < K 127^2 < 2^20 and
+        // hx = hl + lh < 2 K 255 127 < 2^22, so (hh mod m) 2^14 + 128 hx + ll stays below 2^30 and needs one
+        // reduction after hh's; the thread's 16 results of its row leave as two 16-byte stores
+        u32 pk[8];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int a = (int)hh[u];
+          const int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+          const int v = ra * c14 + (int)hx[u] * 128 + (int)ll[u];
+          int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+          rr += (rr < 0) ? m : 0;
+          rr -= (rr >= m) ? m : 0;
+          if (u & 1)
+            pk[u >> 1] |= ((u32)rr & 0xffffu) << 16;
+          else
+            pk[u >> 1] = (u32)rr & 0xffffu;
+        }
+        if (r < big) {
+          if (j0 + 16 <= small && (ldc & 7) == 0 && (((uintptr_t)acc) & 15) == 0) {
+            uint4* dst = reinterpret_cast<uint4*>(bp + j0);
+            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          } else {
+            for (int u = 0; u < 16; u++)
+              if (j0 + u < small) bp[j0 + u] = (int16_t)(pk[u >> 1] >> (16 * (u & 1)));
+          }
+        }
+        continue;
+      }
 #pragma unroll
       for (int u = 0; u < 32; u++) {
         const int j = j0 + u;
@@ -720,6 +762,29 @@ bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G
   return r == CUDA_SUCCESS;
 }
 
+// A non-blocking side stream and two timing-free events per device (created once), for launches that may
+// run beside the caller's stream; joined back with an event before the entry point returns.
+int side_stream(int dev, cudaStream_t* s, cudaEvent_t* fork_ev, cudaEvent_t* join_ev) {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  static cudaEvent_t evs[64][2] = {};
+  if (dev < 0 || dev >= 64) return SDPV_EINVAL;
+  std::lock_guard<std::mutex> g(mu);
+  if (!streams[dev]) {
+    cudaError_t e = cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evs[dev][0], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evs[dev][1], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      streams[dev] = nullptr;
+      return sdpv::set_cuda_error(e);
+    }
+  }
+  *s = streams[dev];
+  *fork_ev = evs[dev][0];
+  *join_ev = evs[dev][1];
+  return SDPV_OK;
+}
+
 }  // namespace
 
 extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t* Alo, const int8_t* Bhi,
@@ -800,9 +865,20 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // The corner launch of a fused-tail syrk runs on a side stream beside the full-tile launch (they write
+  // different accumulator entries): its CTAs take the SMs that the full-tile launch's last partial wave leaves.
+  cudaStream_t main_s = sdpv::as_stream(stream), side_s = main_s;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  if (tailTB) {
+    const int st = side_stream(dev, &side_s, &fork_ev, &join_ev);
+    if (st != SDPV_OK) return st;
+    cudaError_t e = cudaEventRecord(fork_ev, main_s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side_s, fork_ev, 0);
+    if (e != cudaSuccess) return sdpv::set_cuda_error(e);
+  }
   for (int gofs = 0; gofs < G; gofs += kMaxG) {        // at most kMaxG moduli per launch
     const int Gl = G - gofs < kMaxG ? G - gofs : kMaxG;
-    for (int part = 0; part < (tailTB ? 2 : 1); part++) {
+    for (int part = (tailTB ? 1 : 0); part >= 0; part--) {   // the corner first, on the side stream
       const int tb = part ? tailTB : 0;
       // the diagonal items of the full tiles also take the tail rows against their row block (fused tail);
       // the tail launch is left with the last row block against the tail rows (the corner)
@@ -811,12 +887,17 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       const i64 nitems = ptiles * (pack > 1 ? 1 : nb) * Gl;
       if (nitems == 0) continue;
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
-      rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+      rns_gemm_kernel<<<gx, kThreads, smem, part ? side_s : main_s>>>(
           mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
           KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr, sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;
     }
+  }
+  if (tailTB) {
+    cudaError_t e = cudaEventRecord(join_ev, side_s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(main_s, join_ev, 0);
+    if (e != cudaSuccess) return sdpv::set_cuda_error(e);
   }
   return SDPV_OK;
 }

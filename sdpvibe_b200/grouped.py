@@ -19,11 +19,12 @@ because every product, rounding point and sum is the same:
   programs of all blocks into waves of one operation kind (the kind of the block with the longest remaining
   program).
 
-A wave of products is: tile copies into two operand workspaces (grp_copy), their residues (sdpv_residues_u8),
-one grouped narrow residue GEMM over an item table (sdpv_rns_gemm_grouped: up to 128 rows of one side
-against up to 64 rows of the other, K per item), one CRT (sdpv_crt_block) and the rounding kernel of the wave
-(grp_finish_fixed, or grp_colexp + grp_solve_finish); base-tile waves are grp_tile_widen, sdpv_chol_tiles,
-sdpv_trinv_tiles and grp_tile_narrow; merges are grp_merge.  Plans (host tables uploaded once) are cached per
+A wave of products is: tile copies of both operand sides into one workspace (grp_copy), its residues
+(sdpv_residues_u8), one grouped narrow residue GEMM over an item table (sdpv_rns_gemm_grouped: up to 128
+rows of one side against up to 64 rows of the other, K per item), one CRT (sdpv_crt_block) and the rounding
+kernel of the wave (grp_finish_fixed, or grp_solve_round: column exponents and rounding of a group in one
+CTA); base-tile waves are grp_tile_widen, sdpv_chol_tiles, sdpv_trinv_tiles and grp_tile_narrow; merges
+are grp_merge.  Plans (host tables uploaded once) are cached per
 block-size sequence.
 """
 import ctypes
@@ -158,15 +159,15 @@ class _Gemm:
         return r0
 
     def finalize(self):
+        """one copy table for both sides: the small side's rows follow the big side's RA rows in one
+        workspace (one gather, one residue decomposition)"""
         kp = self.kp
-        descs = []
-        for side in (0, 1):
-            d = np.array([(a, b, ld, r * kp + c, kp, rr, cc, int(t)) for a, b, ld, r, c, rr, cc, t in self.copies[side]],
-                         dtype=np.int64).reshape(-1, 8)
-            descs.append(d)
-        self.desc_big, self.desc_small = descs
+        self.RA, self.RB = -(-max(self.rows[0], 1) // 32) * 32, max(self.rows[1], 1)
+        off = (0, self.RA)
+        self.desc = np.array([(a, b, ld, (r + off[side]) * kp + c, kp, rr, cc, int(t))
+                              for side in (0, 1) for a, b, ld, r, c, rr, cc, t in self.copies[side]],
+                             dtype=np.int64).reshape(-1, 8)
         self.items_np = np.array(self.items, dtype=np.int32).reshape(-1, 8)
-        self.RA, self.RB = max(self.rows[0], 1), max(self.rows[1], 1)
         if self.out_mode == 1:
             self.out_rows = self.RA
         self.Rout = max(self.out_rows, 1)
@@ -187,12 +188,11 @@ class _DevGemm:
 
 def _to_device(g):
     d = _DevGemm()
-    for k in ("TB", "out_mode", "w", "kp", "RA", "RB", "Rout", "nfin", "ncolexp", "nsolve_fin", "ngroups"):
+    for k in ("TB", "out_mode", "w", "kp", "RA", "RB", "Rout", "nfin", "nround"):
         setattr(d, k, getattr(g, k, None))
-    d.desc_big, d.desc_small = _dev(g.desc_big), _dev(g.desc_small)
-    d.nbig, d.nsmall = len(g.desc_big), len(g.desc_small)
+    d.desc, d.ndesc = _dev(g.desc), len(g.desc)
     d.items, d.nitems = _dev(g.items_np), len(g.items_np)
-    for k in ("finish", "colexp", "solve_fin"):
+    for k in ("finish", "round"):
         v = getattr(g, k, None)
         setattr(d, k, _dev(v) if v is not None else None)
     return d
@@ -343,7 +343,7 @@ class SolvePlan(_Plan):
             g = _Gemm(TB=TB, out_mode=1, w=TB)
         else:
             g = _Gemm(TB=32 if kind == "leaf" else 64, out_mode=2, w=m)
-        colexp, fin = [], []
+        rnd = []
         for q, (b, op) in enumerate(wave):
             if kind == "leaf":
                 j = op[1]
@@ -387,15 +387,12 @@ class SolvePlan(_Plan):
                     rows0 += [o0 + 32 * u for u in range(len(ch))]
                     for p0 in range(0, m, 128):
                         g.item(prow + p0, min(128, m - p0), s0, 32 * len(ch), klen, o0, p0)
+            assert all(b - a == 32 for a, b in zip(rows0, rows0[1:])), "a group's output rows are consecutive"
             for c0 in range(0, m, 32):
-                nc = min(32, m - c0)
-                colexp.append((rows0[0], 32 * len(rows0), c0, nc, eA, eA_idx, eB_rt, q))
-                for r0, rt in zip(rows0, out_rts):
-                    fin.append((r0, c0, nc, q, mode, rt, rt, 32))
+                rnd.append((rows0[0], 32 * len(rows0), c0, min(32, m - c0), eA, eA_idx, eB_rt, mode, out_rts[0],
+                            out_rts[0]))
         g.finalize()
-        g.colexp, g.ncolexp = _np_desc(colexp, 8), len(colexp)
-        g.solve_fin, g.nsolve_fin = _np_desc(fin, 8), len(fin)
-        g.ngroups = len(wave)
+        g.round, g.nround = _np_desc(rnd, 10), len(rnd)
         g.finish, g.nfin = None, 0
         self.stages.append(("gemm", g))
 
@@ -409,37 +406,33 @@ def _ptrs(tensors):
     return ctypes.cast(arr, ctypes.c_void_p), ctypes.cast(planes, ctypes.c_void_p), len(tensors), keep
 
 
-def _residue_products(R, g, ws_big, ws_small, acc):
-    """acc <- residues of the wave's grouped products (moduli split into groups within the residue budget)."""
-    per_mod = 2 * g.kp * (g.RA + g.RB)
+def _residue_products(R, g, ws, acc):
+    """acc <- residues of the wave's grouped products: the workspace's rows decomposed once (moduli split into
+    groups within the residue budget), the big side its first RA rows, the small side the rest."""
+    rows = g.RA + g.RB
+    per_mod = 2 * g.kp * rows
     GR = R.n if R.n * per_mod <= RES_BUDGET else max(R.G, (RES_BUDGET // per_mod) // R.G * R.G)
+    small_off = g.RA * g.kp
     for g0 in range(0, R.n, GR):
         G = min(GR, R.n - g0)
-        bh, bl = R.residues(ws_big, 0, g.kp, g0, G, spread=True, unsigned=True)
-        sh, sl = R.residues(ws_small, 0, g.kp, g0, G, spread=True, unsigned=True)
-        _lib.call("sdpv_rns_gemm_grouped", R.handle, _lib.ptr_strided(bh), _lib.ptr_strided(bl), g.RA, bh.stride(0),
-                  _lib.ptr_strided(sh), _lib.ptr_strided(sl), g.RB, sh.stride(0), g.kp, g.TB, g.out_mode,
-                  _lib.ptr(g.items), g.nitems, _lib.ptr(acc), g.w, g.Rout, g0, G, _lib.stream())
-        del bh, bl, sh, sl
-
-
-def _gather(g, arenas, L):
-    arr, planes, n, _keep = _ptrs(arenas)
-    ws = []
-    for rows, desc, nd in ((g.RA, g.desc_big, g.nbig), (g.RB, g.desc_small, g.nsmall)):
-        w = torch.empty((L, rows, g.kp), dtype=torch.int32, device=dev)
-        _lib.call("sdpv_grp_copy", arr, planes, n, _lib.ptr(w), rows * g.kp, L, _lib.ptr(desc), nd, _lib.stream())
-        ws.append(w)
-    return ws
+        rh, rl = R.residues(ws, 0, g.kp, g0, G, spread=True, unsigned=True)
+        hp, lp = rh.data_ptr(), rl.data_ptr()
+        _lib.call("sdpv_rns_gemm_grouped", R.handle, ctypes.c_void_p(hp), ctypes.c_void_p(lp), g.RA, rh.stride(0),
+                  ctypes.c_void_p(hp + small_off), ctypes.c_void_p(lp + small_off), g.RB, rh.stride(0), g.kp, g.TB,
+                  g.out_mode, _lib.ptr(g.items), g.nitems, _lib.ptr(acc), g.w, g.Rout, g0, G, _lib.stream())
+        del rh, rl
 
 
 def _product_wave(g, arenas, L):
-    """gather, residues, grouped GEMM, CRT: -> (CRT words (W, Rout * w), bit lengths)"""
+    """gather (both sides, one launch), residues (one launch), grouped GEMM, CRT -> (CRT words (W, Rout w),
+    bit lengths)"""
     R = ctx(L)
-    ws_big, ws_small = _gather(g, arenas, L)
+    arr, planes, n, _keep = _ptrs(arenas)
+    ws = torch.empty((L, g.RA + g.RB, g.kp), dtype=torch.int32, device=dev)
+    _lib.call("sdpv_grp_copy", arr, planes, n, _lib.ptr(ws), ws[0].numel(), L, _lib.ptr(g.desc), g.ndesc, _lib.stream())
     acc = torch.empty((R.n, g.Rout, g.w), dtype=torch.int16, device=dev)
-    _residue_products(R, g, ws_big, ws_small, acc)
-    del ws_big, ws_small
+    _residue_products(R, g, ws, acc)
+    del ws
     Wd, bl, _ = R.crt_block(acc, g.w, 0, g.w, g.Rout)
     return R, Wd, bl
 
@@ -488,12 +481,8 @@ def run_solve(plan, Pa, Pe, Fa, Xa, xe):
                       _lib.stream())
             continue
         R, Wd, bl = _product_wave(st, arenas, L)
-        sU = torch.empty((st.ngroups, m), dtype=torch.int64, device=dev)
-        eU = torch.empty_like(sU)
-        _lib.call("sdpv_grp_colexp", _lib.ptr(bl), st.w, _lib.ptr(Pe), m, L, _lib.ptr(xe), _lib.ptr(st.colexp),
-                  st.ncolexp, _lib.ptr(sU), _lib.ptr(eU), _lib.stream())
-        _lib.call("sdpv_grp_solve_finish", _lib.ptr(Wd), R.W, Wd.shape[1], st.w, _lib.ptr(Pa), Pa[0].numel(),
-                  _lib.ptr(Pe), m, L, _lib.ptr(sU), _lib.ptr(eU), _lib.ptr(st.solve_fin), st.nsolve_fin, _lib.stream())
+        _lib.call("sdpv_grp_solve_round", _lib.ptr(Wd), _lib.ptr(bl), R.W, Wd.shape[1], st.w, _lib.ptr(Pa), Pa[0].numel(),
+                  _lib.ptr(Pe), m, L, _lib.ptr(xe), _lib.ptr(st.round), st.nround, _lib.stream())
 
 
 _PLANS = {}
@@ -587,22 +576,31 @@ class Factorisation:
         nb, s = self.batches[q]
         return arena_to_dense(self.Fa, self.lay, self.b0[q], nb, s)
 
+    def _index(self, key, make):
+        """a device index tensor of this layout, made once (no host-device copy on later calls)"""
+        ck = (tuple(self.batches), key, torch.cuda.current_device())
+        if ck not in _IDX:
+            _IDX[ck] = torch.from_numpy(np.ascontiguousarray(make(), dtype=np.int64)).to(dev)
+        return _IDX[ck]
+
     def diag_tile(self, q, j):
         """batch q's diagonal tile j: (inverse limbs (L, nb, 32, 32), its exponents (nb,), factor limbs)"""
         nb, _ = self.batches[q]
         bs = range(self.b0[q], self.b0[q] + nb)
-        di = torch.tensor([self.lay.diag(b, j) for b in bs], device=dev)
-        ti = torch.tensor([self.lay.tile(b, j, j) for b in bs], device=dev)
+        di = self._index(("d", q, j), lambda: [self.lay.diag(b, j) for b in bs])
+        ti = self._index(("t", q, j), lambda: [self.lay.tile(b, j, j) for b in bs])
         return self.Xa.index_select(1, di), self.xe.index_select(0, di), self.Fa.index_select(1, ti)
 
     def diagonal(self, q):
         """limbs of the diagonal of batch q's factor, (L, nb, n)"""
         nb, s = self.batches[q]
-        pos = []
-        for b in range(self.b0[q], self.b0[q] + nb):
-            for i in range(BT * s):
-                pos.append(self.lay.tile(b, i // BT, i // BT) * 1024 + (i % BT) * (BT + 1))
-        idx = torch.tensor(pos, device=dev)
+
+        def make():
+            b = np.arange(self.b0[q], self.b0[q] + nb)[:, None]
+            i = np.arange(BT * s)[None, :]
+            t = self.lay.toff[b] + (i // BT) * (i // BT + 1) // 2 + i // BT
+            return (t * 1024 + (i % BT) * (BT + 1)).reshape(-1)
+        idx = self._index(("diag", q), make)
         return self.Fa.view(self.L, -1).index_select(1, idx).view(self.L, nb, BT * s)
 
 

@@ -34,10 +34,9 @@ def copy(desc, srcs, dst):
 def product_wave(g, srcs, L):
     """grp_copy x 2, residues, sdpv_rns_gemm_grouped, sdpv_crt_block -> (CRT words (W, Rout w), bit lengths)"""
     T = O.tables(L)
-    big = np.zeros((L, g.RA, g.kp), np.int32)
-    small = np.zeros((L, g.RB, g.kp), np.int32)
-    copy(g.desc_big, srcs, big)
-    copy(g.desc_small, srcs, small)
+    ws = np.zeros((L, g.RA + g.RB, g.kp), np.int32)       # big side rows, then the small side's from row RA
+    copy(g.desc, srcs, ws)
+    big, small = ws[:, :g.RA], ws[:, g.RA:]
     Wd = np.zeros((T.W, g.Rout * g.w), np.int32)
     bl = np.zeros((g.Rout * g.w,), np.int64)
     for b0, nbig, s0, nsmall, klen, o0, c0, _ in g.items_np.tolist():
@@ -128,28 +127,24 @@ def run_solve(plan, Pa, Pe, Fa, Xa, xe):
                         Pe[t, c] = ee
             continue
         T, Wd, bl = product_wave(st, ar, L)
-        sU = np.zeros((st.ngroups, m), np.int64)
-        eU = np.zeros_like(sU)
-        # grp_colexp: 'col' exponents over the group's rows
-        for row0, rows, c0, nc, eA, eidx, ebrt, q in st.colexp.tolist():
+        # grp_solve_round: a group's 'col' exponents over all its rows, then its entries rounded into the
+        # destination row tiles (leaf store, or the aligned difference with the base rows)
+        for row0, rows, c0, nc, eA, eidx, ebrt, mode, brt0, drt0 in st.round.tolist():
             for c in range(c0, c0 + nc):
                 mx = int(bl[(row0 + np.arange(rows)) * st.w + c].max())
-                s = mx - hr
-                sU[q, c] = s
-                eU[q, c] = eA + (int(xe[eidx]) if eidx >= 0 else 0) + int(Pe[ebrt, c]) + s
-        # grp_solve_finish: leaf store, or the aligned difference with the base rows
-        for row0, c0, nc, q, mode, brt, drt, rows in st.solve_fin.tolist():
-            for c in range(c0, c0 + nc):
-                u, _ = O.shift_round(Wd[:, (row0 + np.arange(rows)) * st.w + c], np.full(rows, sU[q, c], np.int64), L)
-                pos = np.array([ent(drt, r, c) for r in range(rows)])
-                if mode == 0:
-                    P2[:, pos] = u
-                    Pe[drt, c] = eU[q, c]
-                    continue
-                bpos = np.array([ent(brt, r, c) for r in range(rows)])
-                eb = int(Pe[brt, c])
-                e2 = max(eb, int(eU[q, c])) + 1
-                bv, _ = O.shift_round(P2[:, bpos], np.full(rows, e2 - eb, np.int64), L)
-                uv, _ = O.shift_round(u, np.full(rows, e2 - int(eU[q, c]), np.int64), L)
-                P2[:, pos] = O.add_same(bv, uv, -1 if mode == 1 else 1)
-                Pe[drt, c] = e2
+                su = mx - hr
+                eu = eA + (int(xe[eidx]) if eidx >= 0 else 0) + int(Pe[ebrt, c]) + su
+                for t in range(rows // 32):
+                    u, _ = O.shift_round(Wd[:, (row0 + 32 * t + np.arange(32)) * st.w + c], np.full(32, su, np.int64), L)
+                    pos = np.array([ent(drt0 + t, r, c) for r in range(32)])
+                    if mode == 0:
+                        P2[:, pos] = u
+                        Pe[drt0 + t, c] = eu
+                        continue
+                    bpos = np.array([ent(brt0 + t, r, c) for r in range(32)])
+                    eb = int(Pe[brt0 + t, c])
+                    e2 = max(eb, eu) + 1
+                    bv, _ = O.shift_round(P2[:, bpos], np.full(32, e2 - eb, np.int64), L)
+                    uv, _ = O.shift_round(u, np.full(32, e2 - eu, np.int64), L)
+                    P2[:, pos] = O.add_same(bv, uv, -1 if mode == 1 else 1)
+                    Pe[drt0 + t, c] = e2
