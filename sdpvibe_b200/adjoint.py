@@ -30,9 +30,14 @@ The plain linear-response (envelope) value  dc . x - x^T dB y  is computed besid
   iter_directions(sdp, count)     Gaussian unit directions in (B, c) from one numpy generator
   envelope_sensitivity            the plain linear-response value
 
-torch's autograd tracks floating-point tensors only; the MPF limb planes are int32, so these adjoints are
-explicit functions rather than torch.autograd.Function subclasses (a float64 carrier would round the
-832-bit cotangents).  Everything stays in MPF on the GPU; scalar results are mpmath numbers.
+  ObjectiveFunction / objective      the same f behind torch.autograd.Function: float64 carrier tensors of the
+                                  chunks' (B, c) enter the graph, f comes out as a float64 scalar, and
+                                  backward() gives the carriers the adjoint gradient rounded to float64;
+                                  the exact MPF gradient stays on the objective (`last_gradient`)
+
+torch's autograd tracks floating-point tensors only and the MPF limb planes are int32, so the exact 832-bit
+cotangents travel as MPF payloads beside the float64 graph.  Everything stays in MPF on the GPU; scalar
+results are mpmath numbers.
 """
 import mpmath as mp
 import numpy as np
@@ -272,3 +277,35 @@ def envelope_sensitivity(solver, directions):
             tot = tot + dot(dc, x) - dot(dBy, x)
         res.append(tot)
     return res
+
+
+class ObjectiveFunction(torch.autograd.Function):
+    """f(B, c) of a NewtonObjective in torch's autograd.  Inputs: the objective, then per chunk float64
+    carriers (B_g (nb, P, N), c_g (nb, P, 1)) -- their values are not read: f is evaluated exactly at the
+    objective's MPF data.  Output: f rounded to float64.  Backward: grad_out times the adjoint gradient
+    (grad_B, grad_c) of every chunk, rounded to float64 from the exact MPF values, which are kept on the
+    objective as `last_gradient`."""
+
+    @staticmethod
+    def forward(ctx, fo, *carriers):
+        f = fo.forward()
+        ctx.fo = fo
+        ctx.n = len(carriers)
+        ctx.dev = carriers[0].device if carriers else torch.device("cuda")
+        return torch.tensor(float(f), dtype=torch.float64, device=ctx.dev)
+
+    @staticmethod
+    def backward(ctx, gout):
+        grads = ctx.fo.backward()
+        ctx.fo.last_gradient = grads
+        out = [None]
+        for gB, gc in grads:
+            for G in (gB, gc):
+                out.append(gout * torch.from_numpy(np.ascontiguousarray(G.to_float())).to(ctx.dev))
+        return tuple(out[:ctx.n + 1])
+
+
+def objective(fo, carriers):
+    """f as a float64 tensor in torch's graph: carriers = [(B_g, c_g)] float64 tensors (requires_grad)"""
+    flat = [t for pair in carriers for t in pair]
+    return ObjectiveFunction.apply(fo, *flat)

@@ -499,6 +499,107 @@ __device__ void fx_rmw(u32* dst, const u32* x, int tx, const u32* y, int ty, boo
 }
 
 
+// fx_rmw for operands of at most LFT + 1 words (top <= LFT: fixed-point magnitudes <= 2^(F+32), as the
+// Cholesky columns |l_ik| <= 1 are): both operands are loaded into registers once and every column sum runs
+// from registers (fx_rmw reads two shared-memory words per multiply-add).  The same columns LF - 2 ..
+// (zero beyond the tops), the same carries and kept words, so the same result.
+template <int LFT>
+__device__ __forceinline__ void fx_rmw_reg(u32* dst, const u32* x, const u32* y, bool add, int WL) {
+  constexpr int NW = LFT + 1;
+  u32 xr[NW], yr[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) {
+    xr[i] = x[i];
+    yr[i] = y[i];
+  }
+  u32 c0 = 0, c1 = 0, c2 = 0, cy = 0;
+  int w = 0;
+  auto emit = [&](u32 d) {
+    if (w < WL) {
+      const u32 o = dst[w];
+      if (add) {
+        const u64 r = (u64)o + d + cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 32);
+      } else {
+        const u64 r = (u64)o - d - cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 63);
+      }
+      w++;
+    }
+  };
+#pragma unroll
+  for (int k = LFT - 2; k <= 2 * LFT; k++) {
+    constexpr int dummy = 0;
+    (void)dummy;
+    u32 d0 = 0, d1 = 0, d2 = 0;                         // a second carry chain (odd terms)
+    const int i0 = k - LFT > 0 ? k - LFT : 0, i1 = k < LFT ? k : LFT;
+#pragma unroll
+    for (int i = i0; i <= i1; i += 2) {
+      mac96(c0, c1, c2, xr[i], yr[k - i]);
+      if (i + 1 <= i1) mac96(d0, d1, d2, xr[i + 1], yr[k - i - 1]);
+    }
+    add96(c0, c1, c2, d0, d1, d2);
+    if (k >= LFT) emit(c0);
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  emit(c0);                                              // columns 2 LFT + 1, 2 LFT + 2: no new terms
+  emit(c1);
+  while (cy && w < WL) emit(0);
+}
+
+// fx_rmw with only the first operand bounded (top <= LFT, kept in registers) and the second read from shared
+// memory (one load per multiply-add instead of two): the triangular inverse's products |l_ij| |x_jk|.
+template <int LFT>
+__device__ __forceinline__ void fx_rmw_lreg(u32* dst, const u32* x, const u32* y, int ty, bool add, int WL) {
+  constexpr int NW = LFT + 1;
+  u32 xr[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) xr[i] = x[i];
+  u32 c0 = 0, c1 = 0, c2 = 0, cy = 0;
+  int w = 0;
+  auto emit = [&](u32 d) {
+    if (w < WL) {
+      const u32 o = dst[w];
+      if (add) {
+        const u64 r = (u64)o + d + cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 32);
+      } else {
+        const u64 r = (u64)o - d - cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 63);
+      }
+      w++;
+    }
+  };
+  const int kmax = LFT + ty;
+  for (int k = LFT - 2; k <= kmax; k++) {
+    u32 d0 = 0, d1 = 0, d2 = 0;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      const int jj = k - i;
+      if (jj >= 0 && jj <= ty) {
+        if (i & 1)
+          mac96(d0, d1, d2, xr[i], y[jj]);
+        else
+          mac96(c0, c1, c2, xr[i], y[jj]);
+      }
+    }
+    add96(c0, c1, c2, d0, d1, d2);
+    if (k >= LFT) emit(c0);
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  emit(c0);
+  emit(c1);
+  while (cy && w < WL) emit(0);
+}
+
 // Warp-parallel WL-word arithmetic for the Newton steps (words lane and lane + 32 of each operand).
 __device__ __forceinline__ void warp_addsub(u32* r, const u32* a, const u32* b, bool sub, int WL) {
   const int lane = threadIdx.x & 31;
@@ -614,8 +715,15 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
         while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
         while (ii * (ii + 1) / 2 > p) ii--;
         const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
-        fx_rmw(T + (size_t)tri(i, j) * WP, colmag + (size_t)i * WP, coltop[i], colmag + (size_t)j * WP, coltop[j],
-               colsign[i] != colsign[j], WL, LF);
+        u32* dst = T + (size_t)tri(i, j) * WP;
+        const u32 *xi = colmag + (size_t)i * WP, *xj = colmag + (size_t)j * WP;
+        const bool add = colsign[i] != colsign[j];
+        if (LF == 26 && coltop[i] <= 26 && coltop[j] <= 26)
+          fx_rmw_reg<26>(dst, xi, xj, add, WL);
+        else if (LF == 24 && coltop[i] <= 24 && coltop[j] <= 24)
+          fx_rmw_reg<24>(dst, xi, xj, add, WL);
+        else
+          fx_rmw(dst, xi, coltop[i], xj, coltop[j], add, WL, LF);
       }
     }
     __syncthreads();
@@ -672,8 +780,15 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
     for (int p = tid; p < np; p += kThreadsS) {                  // slot (i, k) += l_ij x_jk
       const int i = j + 1 + p / nk, k = p % nk;
       const int e = tri(j, k);
-      fx_rmw(Xm + (size_t)tri(i, k) * WP, Lcol + (size_t)i * WP, lt[i], Xm + (size_t)e * WP, xt[e], ls[i] == xs[e],
-             WL, LF);
+      u32* dst = Xm + (size_t)tri(i, k) * WP;
+      const u32 *xl = Lcol + (size_t)i * WP, *yx = Xm + (size_t)e * WP;
+      const bool add = ls[i] == xs[e];
+      if (LF == 26 && lt[i] <= 26)
+        fx_rmw_lreg<26>(dst, xl, yx, xt[e], add, WL);
+      else if (LF == 24 && lt[i] <= 24)
+        fx_rmw_lreg<24>(dst, xl, yx, xt[e], add, WL);
+      else
+        fx_rmw(dst, xl, lt[i], yx, xt[e], add, WL, LF);
     }
     __syncthreads();
     for (int k = warp; k <= j; k += kWarpsS) {                   // x_{j+1,k} = -(sum) r_{j+1}

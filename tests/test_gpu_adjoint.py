@@ -179,3 +179,29 @@ def test_newton_objective_derivative_is_envelope_value_at_optimum():
     for d in iter_directions(sdp, 3, seed=1):
         da, de = fo.directional([dB for dB, _ in d], [dc for _, dc in d])
         assert abs(da - de) <= mp.mpf(10) ** -12 * abs(de), (mp.nstr(da, 20), mp.nstr(de, 20))
+
+
+def test_objective_behind_autograd_function():
+    """f through torch.autograd: backward() gives the float64 carriers the adjoint gradient; its directional
+    derivative matches the exact adjoint's to float64 accuracy, and the exact MPF gradient is kept."""
+    import torch
+    from sdpvibe_b200.adjoint import NewtonObjective, iter_directions, objective
+    from sdpvibe_b200.solver import Solver
+    from sdpvibe_b200.synthetic import ising_like_sdp
+    L = 16
+    sdp, _ = ising_like_sdp(L, nblocks=10, N=20)
+    sol = Solver(sdp, L)
+    sol.run(max_iter=3)
+    fo = NewtonObjective(sol)
+    carriers = [(torch.from_numpy(g.B.to_float()).cuda().requires_grad_(),
+                 torch.from_numpy(g.c.to_float()).cuda().requires_grad_()) for g in sdp.groups]
+    f = objective(fo, carriers)
+    assert abs(float(f) - float(fo.forward())) <= 1e-12 * abs(float(f))
+    f.backward()
+    host = next(iter_directions(sdp, 1, seed=3, host=True))
+    dev = next(iter_directions(sdp, 1, seed=3))
+    lin = sum(float((B.grad.cpu().numpy() * dB).sum() + (c.grad.cpu().numpy() * dc).sum())
+              for (B, c), (dB, dc) in zip(carriers, host))
+    exact, _ = fo.directional(*zip(*dev))
+    assert abs(lin - float(exact)) <= 1e-9 * (abs(float(exact)) + 1e-30)
+    assert len(fo.last_gradient) == len(sdp.groups)
