@@ -498,13 +498,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         continue;
       }
+      // grouped items with K <= 64 on unsigned digits: hx < 2 K 255 127 < 2^22, so 128 hx needs no reduction
+      // of its own (the sum below stays under 2^30 with an old residue < 2^15)
+      const bool small_k = gtab && u8ops && gtab[8 * t + 4] <= 64;
 #pragma unroll
       for (int u = 0; u < 32; u++) {
         const int j = j0 + u;
         if (u >= half) break;
         int a = (int)hh[u], x = (int)hx[u];
         int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-        int rx = x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+        int rx = small_k ? x : x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
         const bool in = r < big && j < small;
         const int o = (!fresh && in) ? (int)bp[j * js] : 0;                // old residue (rare: K chunks)
         int v = ra * c14 + rx * 128 + (int)ll[u] + o;
