@@ -1,17 +1,23 @@
 // Cholesky base case on CUDA cores: 32 x 32 tiles in wide fixed point.
 //
 // A tile entry is WL 32-bit words (two's complement) with F = 32*LF fraction bits; tiles are entry-major
-// (tiles, 32, 32, WL), the layout of sdpvibe/basecase.py.  The arithmetic is the reference's, so results
-// are bit-identical (sdpvibe/basecase.py:31-226):
+// (tiles, 32, 32, WL), the layout of sdpvibe/basecase.py.  The results are the reference's bit for bit
+// (sdpvibe/basecase.py:31-226), because every product is the reference's truncated product and every sum
+// of products is exact:
 //   * fx product: |a| * |b| summed by product columns from column max(LF-2, la+lb) upward (columns below
 //     are never formed), exact carries, words >= LF kept (truncation), sign applied last; t > 0 keeps only
 //     the top t words of each operand;
 //   * d^-1/2: double seed 1/sqrt(d) converted exactly, then r += r (1 - d r^2) / 2 with products truncated
 //     to the top 100, 200, 400, ... bits until full width;
 //   * Cholesky by columns (pivot, column scaled by the pivot reciprocal, trailing update of the lower
-//     triangle); inverse X = L^-1 row by row with the pivot reciprocals.
-// One CTA (256 threads) per tile.  The Newton steps run warp-cooperatively (each lane forms product
-// columns, lane 0 carries); column scaling and the trailing update give one product to each thread.
+//     triangle); inverse X = L^-1 with the pivot reciprocals.
+// How they are computed is this library's own, organised for latency: one CTA of 16 warps per tile; serial
+// products (Newton, pivot-column scaling, the inverse's row finishing) run warp-cooperatively with one
+// product column per lane and carries resolved by warp ballots; the bulk products (trailing update, inverse
+// row products) run one per thread on 96-bit column accumulators (mad.cc carry chains), the operands of the
+// common limb counts held in registers.  WL <= 64: the tile lives in shared memory; 64 < WL <= 96: the same
+// kernels keep it in global memory (the factor in place, the inverse's sums in a scratch), three words per
+// lane.  The batched substitution L y = v reuses the warp product and a thread product of a signed operand.
 #include <cmath>
 #include <mutex>
 
@@ -22,6 +28,10 @@ namespace {
 constexpr int BT = 32;
 constexpr int kThreads = 256;
 constexpr int WMAX = 96;                  // WL <= 96 (L <= 72)
+constexpr int FW = 64;                    // WL <= FW: the tile in shared memory
+constexpr int kThreadsS = 512;            // tile kernels: 16 warps per tile
+constexpr int kWarpsS = kThreadsS / 32;
+constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ int top_word(const u32* a, int WL) {
   for (int i = WL - 1; i > 0; i--)
@@ -36,91 +46,6 @@ __device__ __forceinline__ void negate_words(u32* a, int n) {
     c = (c && t == 0) ? 1u : 0u;
     a[k] = t;
   }
-}
-
-// Column sums of x * y restricted to i in [la, ta], j in [lb, tb], from column kmin; carried into r
-// (words LF .. LF+WL-1).  Pure function of the magnitudes, shared by the thread and warp versions.
-__device__ __forceinline__ void column_sum(const u32* x, const u32* y, int k, int la, int ta, int lb, int tb,
-                                           u64& lo, u64& hi) {
-  lo = 0;
-  hi = 0;
-  int i0 = max(la, k - tb), i1 = min(ta, k - lb);
-  for (int i = i0; i <= i1; i++) {
-    u64 p = (u64)x[i] * y[k - i];
-    lo += (u32)p;
-    hi += p >> 32;
-  }
-}
-
-// r = (a * b) >> F truncated (thread-serial); r may alias a or b.
-__device__ void fx_mul(u32* r, const u32* a, const u32* b, int t, int WL, int LF) {
-  u32 x[WMAX], y[WMAX];
-  for (int i = 0; i < WL; i++) {
-    x[i] = a[i];
-    y[i] = b[i];
-  }
-  const bool sa = x[WL - 1] >> 31, sb = y[WL - 1] >> 31;
-  if (sa) negate_words(x, WL);
-  if (sb) negate_words(y, WL);
-  const int ta = top_word(x, WL), tb = top_word(y, WL);
-  const int la = t ? max(0, ta - t + 1) : 0, lb = t ? max(0, tb - t + 1) : 0;
-  const int kmin = max(LF - 2, la + lb), kmax = ta + tb;
-  for (int i = 0; i < WL; i++) r[i] = 0;
-  u64 carry = 0, hprev = 0;
-  for (int k = kmin; k <= kmax + 2 && k < LF + WL; k++) {
-    u64 lo = 0, hi = 0;
-    if (k <= kmax) column_sum(x, y, k, la, ta, lb, tb, lo, hi);
-    u64 s = lo + hprev + carry;
-    if (k >= LF) r[k - LF] = (u32)s;
-    carry = s >> 32;
-    hprev = hi;
-  }
-  if (sa ^ sb) negate_words(r, WL);
-}
-
-// Warp-cooperative version: operands and result in shared memory (r must not alias a or b);
-// sx, sy: WL words of scratch, col: 2*(2*WL+4) u64.
-__device__ void fx_mul_warp(u32* r, const u32* a, const u32* b, int t, int WL, int LF, u32* sx, u32* sy, u64* col) {
-  const int lane = threadIdx.x & 31;
-  for (int i = lane; i < WL; i += 32) {
-    sx[i] = a[i];
-    sy[i] = b[i];
-  }
-  __syncwarp();
-  const bool sa = sx[WL - 1] >> 31, sb = sy[WL - 1] >> 31;
-  __syncwarp();
-  if (lane == 0) {
-    if (sa) negate_words(sx, WL);
-    if (sb) negate_words(sy, WL);
-  }
-  __syncwarp();
-  const int ta = top_word(sx, WL), tb = top_word(sy, WL);
-  const int la = t ? max(0, ta - t + 1) : 0, lb = t ? max(0, tb - t + 1) : 0;
-  const int kmin = max(LF - 2, la + lb), kmax = ta + tb;
-  for (int k = kmin + lane; k <= kmax; k += 32) {
-    u64 lo, hi;
-    column_sum(sx, sy, k, la, ta, lb, tb, lo, hi);
-    col[2 * (k - kmin)] = lo;
-    col[2 * (k - kmin) + 1] = hi;
-  }
-  for (int i = lane; i < WL; i += 32) r[i] = 0;
-  __syncwarp();
-  if (lane == 0) {
-    u64 carry = 0, hprev = 0;
-    for (int k = kmin; k <= kmax + 2 && k < LF + WL; k++) {
-      u64 lo = 0, hi = 0;
-      if (k <= kmax) {
-        lo = col[2 * (k - kmin)];
-        hi = col[2 * (k - kmin) + 1];
-      }
-      u64 s = lo + hprev + carry;
-      if (k >= LF) r[k - LF] = (u32)s;
-      carry = s >> 32;
-      hprev = hi;
-    }
-    if (sa ^ sb) negate_words(r, WL);
-  }
-  __syncwarp();
 }
 
 __device__ double fx_to_double(const u32* a, int WL, int LF) {
@@ -151,150 +76,6 @@ __device__ void fx_from_double(u32* r, double v, int WL, int LF) {   // v > 0
   u32 w[4] = {(u32)lo, (u32)(lo >> 32), (u32)hi, (u32)(hi >> 32)};
   for (int k = 0; k < 4 && li + k < WL; k++) r[li + k] = w[k];
 }
-
-// ---- batched Cholesky of 32 x 32 tiles, in place (lower), plus the pivot reciprocals
-__global__ void __launch_bounds__(kThreads) chol_tiles_kernel(u32* __restrict__ A, u32* __restrict__ RINV, int WL,
-                                                              int LF, unsigned* __restrict__ err) {
-  __shared__ u32 sd[WMAX], sr[WMAX], st1[WMAX], st2[WMAX], sone[WMAX], sx[WMAX], sy[WMAX];
-  __shared__ u64 scol[2 * (2 * WMAX + 4)];
-  u32* T = A + (size_t)blockIdx.x * BT * BT * WL;
-  u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
-  const int tid = threadIdx.x, lane = tid & 31;
-#define AT(i, j) (T + ((size_t)(i) * BT + (j)) * WL)
-  for (int k = 0; k < BT; k++) {
-    if (tid < 32) {
-      for (int i = lane; i < WL; i += 32) sd[i] = AT(k, k)[i];
-      __syncwarp();
-      if (lane == 0) {
-        if ((sd[WL - 1] >> 31) || top_word(sd, WL) == 0 && sd[0] == 0) atomicOr(err, SDPV_ERRBIT_NOTSPD);
-        fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
-        for (int i = 0; i < WL; i++) sone[i] = 0;
-        sone[LF] = 1;
-      }
-      __syncwarp();
-      for (int bits = 100;; bits *= 2) {                 // r <- r + r (1 - d r^2) / 2
-        int t = bits / 32 + 2;
-        if (t >= WL) t = 0;
-        fx_mul_warp(st1, sr, sr, t, WL, LF, sx, sy, scol);
-        fx_mul_warp(st2, st1, sd, t, WL, LF, sx, sy, scol);
-        if (lane == 0) {
-          i64 br = 0;                                     // st1 = 1 - st2
-          for (int i = 0; i < WL; i++) {
-            i64 v = (i64)sone[i] - (i64)st2[i] + br;
-            st1[i] = (u32)v;
-            br = v >> 32;
-          }
-        }
-        __syncwarp();
-        fx_mul_warp(st2, sr, st1, t, WL, LF, sx, sy, scol);
-        if (lane == 0) {
-          for (int i = 0; i < WL - 1; i++) st2[i] = (st2[i] >> 1) | (st2[i + 1] << 31);
-          st2[WL - 1] = (u32)(((int32_t)st2[WL - 1]) >> 1);
-          u64 c = 0;
-          for (int i = 0; i < WL; i++) {
-            u64 v = (u64)sr[i] + st2[i] + c;
-            sr[i] = (u32)v;
-            c = v >> 32;
-          }
-        }
-        __syncwarp();
-        if (t == 0) break;
-      }
-      fx_mul_warp(st1, sd, sr, 0, WL, LF, sx, sy, scol);  // l_kk = d * d^-1/2
-      for (int i = lane; i < WL; i += 32) {
-        AT(k, k)[i] = st1[i];
-        RI[(size_t)k * WL + i] = sr[i];
-      }
-    }
-    __syncthreads();
-    const u32* rk = RI + (size_t)k * WL;
-    for (int i = k + 1 + tid; i < BT; i += kThreads) fx_mul(AT(i, k), AT(i, k), rk, 0, WL, LF);
-    __syncthreads();
-    const int m = BT - k - 1, npairs = m * (m + 1) / 2;
-    for (int p = tid; p < npairs; p += kThreads) {
-      int ii = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
-      while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
-      while (ii * (ii + 1) / 2 > p) ii--;
-      const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
-      u32 v[WMAX];
-      fx_mul(v, AT(i, k), AT(j, k), 0, WL, LF);
-      u32* aij = AT(i, j);
-      i64 br = 0;
-      for (int w = 0; w < WL; w++) {
-        i64 d = (i64)aij[w] - (i64)v[w] + br;
-        aij[w] = (u32)d;
-        br = d >> 32;
-      }
-    }
-    __syncthreads();
-  }
-#undef AT
-}
-
-// ---- batched inverse X = L^-1 of lower tiles (upper part of Lt must be zero), row by row:
-// x_ii = 1/l_ii, x_ik = -(1/l_ii) sum_{j=k}^{i-1} l_ij x_jk.  S: per-tile scratch for the products.
-__global__ void __launch_bounds__(kThreads) trinv_tiles_kernel(const u32* __restrict__ Lt, const u32* __restrict__ RINV,
-                                                               u32* __restrict__ X, u32* __restrict__ S, int WL, int LF) {
-  const size_t tsz = (size_t)BT * BT * WL;
-  const u32* T = Lt + blockIdx.x * tsz;
-  const u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
-  u32* XT = X + blockIdx.x * tsz;
-  u32* SC = S + blockIdx.x * tsz;                        // SC[k][j] = l_ij x_jk for the current row i
-  const int tid = threadIdx.x;
-  for (size_t w = tid; w < tsz; w += kThreads) XT[w] = 0;
-  __syncthreads();
-  for (int i = 0; i < BT; i++) {
-    const int np = i * (i + 1) / 2;                      // pairs k <= j < i
-    for (int p = tid; p < np; p += kThreads) {
-      int j = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
-      while ((j + 1) * (j + 2) / 2 <= p) j++;
-      while (j * (j + 1) / 2 > p) j--;
-      const int k = p - j * (j + 1) / 2;
-      fx_mul(SC + ((size_t)k * BT + j) * WL, T + ((size_t)i * BT + j) * WL, XT + ((size_t)j * BT + k) * WL, 0, WL,
-             LF);
-    }
-    __syncthreads();
-    for (int k = tid; k <= i; k += kThreads) {
-      u32* xik = XT + ((size_t)i * BT + k) * WL;
-      if (k == i) {
-        for (int w = 0; w < WL; w++) xik[w] = RI[(size_t)i * WL + w];
-        continue;
-      }
-      u32 acc[WMAX];
-      for (int w = 0; w < WL; w++) acc[w] = 0;
-      for (int j = k; j < i; j++) {
-        const u32* s = SC + ((size_t)k * BT + j) * WL;
-        u64 c = 0;
-        for (int w = 0; w < WL; w++) {
-          u64 v = (u64)acc[w] + s[w] + c;
-          acc[w] = (u32)v;
-          c = v >> 32;
-        }
-      }
-      fx_mul(acc, acc, RI + (size_t)i * WL, 0, WL, LF);
-      negate_words(acc, WL);
-      for (int w = 0; w < WL; w++) xik[w] = acc[w];
-    }
-    __syncthreads();
-  }
-}
-
-
-// ================================================================ shared-memory tile kernels (WL <= 64)
-// The same arithmetic as the kernels above, organised for latency: the tile lives in shared memory,
-// serial products (Newton, pivot-column scaling, the row sums of the inverse) run warp-cooperatively with
-// one product column per lane and carries resolved by warp ballots, and the bulk products (trailing update,
-// inverse row products) run one per thread on 96-bit column accumulators (mad.cc carry chains) straight
-// from shared-memory magnitudes.  Every product is the same truncated product (same columns, same kept
-// words), and sums of products are exact in WL words, so the results are bit-identical to the kernels above.
-constexpr int FW = 64;                    // fast path: WL <= FW
-constexpr int kThreadsS = 512;            // shared-memory kernels: 16 warps per tile
-constexpr int kWarpsS = kThreadsS / 32;
-constexpr unsigned kFull = 0xffffffffu;
-
-struct WarpScratch {                      // per-warp product scratch
-  u32 xa[FW], xb[FW], acc[FW];
-};
 
 // c += d (96-bit)
 __device__ __forceinline__ void add96(u32& c0, u32& c1, u32& c2, u32 d0, u32 d1, u32 d2) {
@@ -367,34 +148,53 @@ __device__ __forceinline__ u32 chain_carry(bool g, bool p, u32 cin, u32& cout) {
   return (((u32)sum ^ X ^ G) >> (threadIdx.x & 31)) & 1u;
 }
 
-// Words lane and lane+32 of a two's-complement WL-word number negated (mod 2^(32 WL)): ~x plus a carry that
-// enters word w when every lower word is zero.
-__device__ __forceinline__ void warp_negate(u32& v0, u32& v1, int WL) {
+// Per-warp product scratch for WL <= 32 NPL: the operands' magnitudes and the product.
+template <int NPL>
+struct WarpScratchT {
+  u32 xa[32 * NPL], xb[32 * NPL], acc[32 * NPL];
+};
+
+// Words lane + 32 c (c < NPL) of a two's-complement WL-word number negated (mod 2^(32 WL)): ~x plus a carry
+// that enters word w when every lower word is zero.
+template <int NPL>
+__device__ __forceinline__ void warp_negate(u32 (&v)[NPL], int WL) {
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  const unsigned nz0 = __ballot_sync(kFull, lane < WL && v0 != 0);
-  const unsigned nz1 = __ballot_sync(kFull, lane + 32 < WL && v1 != 0);
-  v0 = ~v0 + (((nz0 & lower) == 0) ? 1u : 0u);
-  v1 = ~v1 + ((nz0 == 0 && (nz1 & lower) == 0) ? 1u : 0u);
+  bool below_zero = true;                                     // every word of the lower lane groups is zero
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    const unsigned nz = __ballot_sync(kFull, lane + 32 * c < WL && v[c] != 0);
+    v[c] = ~v[c] + ((below_zero && (nz & lower) == 0) ? 1u : 0u);
+    below_zero = below_zero && nz == 0;
+  }
 }
 
-__device__ __forceinline__ int warp_top(u32 v0, u32 v1, int WL) {
+template <int NPL>
+__device__ __forceinline__ int warp_top(const u32 (&v)[NPL], int WL) {
   const int lane = threadIdx.x & 31;
-  const unsigned b0 = __ballot_sync(kFull, lane < WL && v0 != 0);
-  const unsigned b1 = __ballot_sync(kFull, lane + 32 < WL && v1 != 0);
-  return b1 ? 63 - __clz(b1) : (b0 ? 31 - __clz(b0) : 0);
+  int top = 0;
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    const unsigned b = __ballot_sync(kFull, lane + 32 * c < WL && v[c] != 0);
+    if (b) top = 32 * c + 31 - __clz(b);
+  }
+  return top;
 }
 
 // Magnitude of a two's-complement WL-word operand (shared or global memory) into m[0..WL); returns its sign,
 // top = index of its highest nonzero word (0 for zero).  Warp-collective.
+template <int NPL>
 __device__ __forceinline__ int load_mag(const u32* src, u32* m, int WL, int& top) {
   const int lane = threadIdx.x & 31;
   const int sign = (int)(src[WL - 1] >> 31);
-  u32 v0 = lane < WL ? src[lane] : 0u, v1 = lane + 32 < WL ? src[lane + 32] : 0u;
-  if (sign) warp_negate(v0, v1, WL);
-  if (lane < WL) m[lane] = v0;
-  if (lane + 32 < WL) m[lane + 32] = v1;
-  top = warp_top(v0, v1, WL);
+  u32 v[NPL];
+#pragma unroll
+  for (int c = 0; c < NPL; c++) v[c] = lane + 32 * c < WL ? src[lane + 32 * c] : 0u;
+  if (sign) warp_negate<NPL>(v, WL);
+#pragma unroll
+  for (int c = 0; c < NPL; c++)
+    if (lane + 32 * c < WL) m[lane + 32 * c] = v[c];
+  top = warp_top<NPL>(v, WL);
   return sign;
 }
 
@@ -402,15 +202,16 @@ __device__ __forceinline__ int load_mag(const u32* src, u32* m, int WL, int& top
 // column per lane, columns kmin .. min(kmax + 2, LF + WL - 1), each a 96-bit exact sum; the column sums are
 // added with their 32- and 64-bit shifts and the carries resolved by chain_carry.  Outputs (any may be
 // null): out = signed result (may alias a or b), omag = magnitude, *osign / *otop (written by lane 0).
-__device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScratch& s, u32* out, u32* omag,
+template <int NPL>
+__device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScratchT<NPL>& s, u32* out, u32* omag,
                      uint8_t* osign, uint8_t* otop) {
   const int lane = threadIdx.x & 31;
   int ta, tb;
-  const int sa = load_mag(a, s.xa, WL, ta);
-  const int sb = load_mag(b, s.xb, WL, tb);
+  const int sa = load_mag<NPL>(a, s.xa, WL, ta);
+  const int sb = load_mag<NPL>(b, s.xb, WL, tb);
   __syncwarp();
-  s.acc[lane] = 0;
-  s.acc[lane + 32] = 0;
+#pragma unroll
+  for (int c = 0; c < NPL; c++) s.acc[lane + 32 * c] = 0;
   const int la = t ? max(0, ta - t + 1) : 0, lb = t ? max(0, tb - t + 1) : 0;
   const int kmin = max(LF - 2, la + lb), kmax = ta + tb;
   const int ncol = min(kmax + 2, LF + WL - 1) - kmin + 1;
@@ -442,21 +243,25 @@ __device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScra
     cin = cout;
   }
   __syncwarp();
-  u32 m0 = lane < WL ? s.acc[lane] : 0u, m1 = lane + 32 < WL ? s.acc[lane + 32] : 0u;
+  u32 m[NPL];
+#pragma unroll
+  for (int c = 0; c < NPL; c++) m[c] = lane + 32 * c < WL ? s.acc[lane + 32 * c] : 0u;
   const int sg = sa ^ sb;
   if (omag) {
-    if (lane < WL) omag[lane] = m0;
-    if (lane + 32 < WL) omag[lane + 32] = m1;
+#pragma unroll
+    for (int c = 0; c < NPL; c++)
+      if (lane + 32 * c < WL) omag[lane + 32 * c] = m[c];
   }
   if (otop) {
-    const int tp = warp_top(m0, m1, WL);
+    const int tp = warp_top<NPL>(m, WL);
     if (lane == 0) *otop = (uint8_t)tp;
   }
   if (osign && lane == 0) *osign = (uint8_t)sg;
   if (out) {
-    if (sg) warp_negate(m0, m1, WL);
-    if (lane < WL) out[lane] = m0;
-    if (lane + 32 < WL) out[lane + 32] = m1;
+    if (sg) warp_negate<NPL>(m, WL);
+#pragma unroll
+    for (int c = 0; c < NPL; c++)
+      if (lane + 32 * c < WL) out[lane + 32 * c] = m[c];
   }
   __syncwarp();
 }
@@ -600,11 +405,60 @@ __device__ __forceinline__ void fx_rmw_lreg(u32* dst, const u32* x, const u32* y
   while (cy && w < WL) emit(0);
 }
 
+// dst (two's complement, WL words) -= trunc(x y) for a signed two's-complement operand x (read in place,
+// e.g. from global memory) and a magnitude y (top ty) with sign ysign: x's magnitude is read word by word
+// (~x plus the carry that enters at its lowest nonzero word z), then the product columns from LF - 2 as in
+// fx_rmw.  One thread.
+__device__ void fx_rmw_signed(u32* dst, const u32* x, const u32* y, int ty, int ysign, int WL, int LF) {
+  const int xs = (int)(x[WL - 1] >> 31);
+  int z = 0;
+  while (z < WL - 1 && x[z] == 0) z++;
+  auto xw = [&](int k) -> u32 {
+    const u32 v = x[k];
+    return !xs ? v : (k < z ? 0u : (k == z ? 0u - v : ~v));
+  };
+  int tx = WL - 1;
+  while (tx > 0 && xw(tx) == 0) tx--;
+  const bool add = xs != ysign;                                 // dst - sign(x) sign(y) |x||y|
+  const int kmin = LF - 2, kmax = tx + ty;
+  u32 c0 = 0, c1 = 0, c2 = 0, cy = 0;
+  int w = 0;
+  auto emit = [&](u32 d) {
+    if (w < WL) {
+      const u32 o = dst[w];
+      if (add) {
+        const u64 r = (u64)o + d + cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 32);
+      } else {
+        const u64 r = (u64)o - d - cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 63);
+      }
+      w++;
+    }
+  };
+  for (int k = kmin; k <= kmax; k++) {
+    for (int i = max(0, k - ty); i <= min(tx, k); i++) mac96(c0, c1, c2, xw(i), y[k - i]);
+    if (k >= LF) emit(c0);
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  for (int k = max(kmax + 1, kmin); k <= kmax + 2; k++) {
+    if (k >= LF) emit(c0);
+    c0 = c1;
+    c1 = 0;
+  }
+  while (cy && w < WL) emit(0);
+}
+
 // Warp-parallel WL-word arithmetic for the Newton steps (words lane and lane + 32 of each operand).
+template <int NPL>
 __device__ __forceinline__ void warp_addsub(u32* r, const u32* a, const u32* b, bool sub, int WL) {
   const int lane = threadIdx.x & 31;
   u32 carry = sub ? 1u : 0u;                                  // a - b = a + ~b + 1
-  for (int c = 0; c < 2; c++) {
+  for (int c = 0; c < NPL; c++) {
     const int w = lane + 32 * c;
     const u32 av = w < WL ? a[w] : 0u, bv = w < WL ? (sub ? ~b[w] : b[w]) : 0u;
     const u64 v = (u64)av + bv;
@@ -618,17 +472,18 @@ __device__ __forceinline__ void warp_addsub(u32* r, const u32* a, const u32* b, 
   __syncwarp();
 }
 
+template <int NPL>
 __device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arithmetic shift right by one bit
   const int lane = threadIdx.x & 31;
-  u32 n[2];
-  for (int c = 0; c < 2; c++) {
+  u32 n[NPL];
+  for (int c = 0; c < NPL; c++) {
     const int w = lane + 32 * c;
     n[c] = 0;
     if (w < WL - 1) n[c] = (x[w] >> 1) | (x[w + 1] << 31);
     else if (w == WL - 1) n[c] = (u32)(((int32_t)x[w]) >> 1);
   }
   __syncwarp();
-  for (int c = 0; c < 2; c++)
+  for (int c = 0; c < NPL; c++)
     if (lane + 32 * c < WL) x[lane + 32 * c] = n[c];
   __syncwarp();
 }
@@ -636,38 +491,46 @@ __device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arit
 // Entries sit in shared memory at an odd pitch of WP = WL | 1 words: the thread products read one operand
 // word per lane from different entries, and an odd pitch puts those words in distinct banks.
 __host__ __device__ constexpr int pitch(int WL) { return WL | 1; }
+template <int NPL, bool GLOBAL>
 __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
-  return (size_t)(528 + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratch) + 5 * FW * 4 + 64;
+  return (size_t)((GLOBAL ? 0 : 528) + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 5 * 32 * NPL * 4 + 64;
 }
+template <int NPL, bool GLOBAL>
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
-  return (size_t)(528 + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratch) + 2 * 528 + 64;
+  return (size_t)((GLOBAL ? 0 : 528) + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 2 * 528 + 64;
 }
 
 __device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
 
-__global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restrict__ A, u32* __restrict__ RINV,
-                                                                   int WL, int LF, unsigned* __restrict__ err) {
+// NPL words per lane (WL <= 32 NPL); GLOBAL: the working triangle is the tile itself in global memory (entry
+// (i, j) at (32 i + j) WL), else a copy in shared memory (entry (i, j) at tri(i, j), odd pitch WP).
+template <int NPL, bool GLOBAL>
+__global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u32* __restrict__ RINV, int WL, int LF,
+                                                          unsigned* __restrict__ err) {
   extern __shared__ __align__(16) u32 sm[];
+  const int WP = pitch(WL), NWD = 32 * NPL;
+  u32* G = A + (size_t)blockIdx.x * BT * BT * WL;
   u32* T = sm;                                                   // lower triangle, entry (i, j) at tri(i, j)
-  const int WP = pitch(WL);
-  u32* colmag = T + 528 * WP;                                    // |l_ik| of the current column
-  WarpScratch* ws = reinterpret_cast<WarpScratch*>(colmag + 32 * WP);
+  auto ent = [&](int i, int j) -> u32* {
+    return GLOBAL ? G + ((size_t)i * BT + j) * WL : T + tri(i, j) * WP;
+  };
+  u32* colmag = GLOBAL ? sm : sm + 528 * WP;                     // |l_ik| of the current column
+  WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(colmag + 32 * WP);
   u32* nw = reinterpret_cast<u32*>(ws + kWarpsS);
-  u32 *sd = nw, *sr = nw + FW, *st1 = nw + 2 * FW, *st2 = nw + 3 * FW, *sone = nw + 4 * FW;
-  uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * FW);
+  u32 *sd = nw, *sr = nw + NWD, *st1 = nw + 2 * NWD, *st2 = nw + 3 * NWD, *sone = nw + 4 * NWD;
+  uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * NWD);
   uint8_t* coltop = colsign + 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  u32* G = A + (size_t)blockIdx.x * BT * BT * WL;
   u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
-  for (int i = 0; i < BT; i++) {
+  for (int i = 0; i < BT && !GLOBAL; i++) {
     const u32* src = G + (size_t)i * BT * WL;
-    u32* dst = T + (size_t)tri(i, 0) * WP;
+    u32* dst = ent(i, 0);
     for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[(w / WL) * WP + w % WL] = src[w];
   }
   __syncthreads();
   // Pivot k (warp 0): r = d^-1/2 by the Newton schedule, l_kk = d r, r kept in sr and RINV.
   auto pivot = [&](int k) {
-    u32* akk = T + (size_t)tri(k, k) * WP;
+    u32* akk = ent(k, k);
     for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
     for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
     __syncwarp();
@@ -679,15 +542,15 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
     for (int bits = 100;; bits *= 2) {                             // r <- r + r (1 - d r^2) / 2
       int t = bits / 32 + 2;
       if (t >= WL) t = 0;
-      wmul(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
-      wmul(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-      warp_addsub(st1, sone, st2, true, WL);
-      wmul(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-      warp_shr1(st2, WL);
-      warp_addsub(sr, sr, st2, false, WL);
+      wmul<NPL>(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+      wmul<NPL>(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+      warp_addsub<NPL>(st1, sone, st2, true, WL);
+      wmul<NPL>(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+      warp_shr1<NPL>(st2, WL);
+      warp_addsub<NPL>(sr, sr, st2, false, WL);
       if (t == 0) break;
     }
-    wmul(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);     // l_kk = d * d^-1/2
+    wmul<NPL>(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);     // l_kk = d * d^-1/2
     for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
   };
   if (warp == 0) pivot(0);
@@ -697,16 +560,16 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
   // the same truncated products as without look-ahead (their exact sum is order-free).
   for (int k = 0; k < BT; k++) {
     for (int i = k + 1 + warp; i < BT; i += kWarpsS) {           // l_ik = a_ik * r_k
-      u32* aik = T + (size_t)tri(i, k) * WP;
-      wmul(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
+      u32* aik = ent(i, k);
+      wmul<NPL>(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
     }
     __syncthreads();
     if (k == BT - 1) break;
     if (warp == 0) {
-      u32* dn = T + (size_t)tri(k + 1, k + 1) * WP;                // a_{k+1,k+1} -= l_{k+1,k}^2
+      u32* dn = ent(k + 1, k + 1);                // a_{k+1,k+1} -= l_{k+1,k}^2
       const u32* lk = colmag + (size_t)(k + 1) * WP;
-      wmul(lk, lk, 0, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
-      warp_addsub(dn, dn, st1, true, WL);
+      wmul<NPL>(lk, lk, 0, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+      warp_addsub<NPL>(dn, dn, st1, true, WL);
       pivot(k + 1);
     } else {
       const int m = BT - k - 1, npairs = m * (m + 1) / 2;
@@ -715,7 +578,7 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
         while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
         while (ii * (ii + 1) / 2 > p) ii--;
         const int i = k + 1 + ii, j = k + 1 + (p - ii * (ii + 1) / 2);
-        u32* dst = T + (size_t)tri(i, j) * WP;
+        u32* dst = ent(i, j);
         const u32 *xi = colmag + (size_t)i * WP, *xj = colmag + (size_t)j * WP;
         const bool add = colsign[i] != colsign[j];
         if (LF == 26 && coltop[i] <= 26 && coltop[j] <= 26)
@@ -728,9 +591,9 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
     }
     __syncthreads();
   }
-  for (int i = 0; i < BT; i++) {
+  for (int i = 0; i < BT && !GLOBAL; i++) {
     u32* dst = G + (size_t)i * BT * WL;
-    const u32* src = T + (size_t)tri(i, 0) * WP;
+    const u32* src = ent(i, 0);
     for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[(w / WL) * WP + w % WL];
   }
 }
@@ -740,14 +603,15 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_smem_kernel(u32* __restr
 // Step j forms all (31 - j)(j + 1) <= 256 products l_ij x_jk (i > j, k <= j) in one round of threads, so
 // the critical path is one product round and one warp product per row.  The products and the final
 // products are the reference's; only the order of the exact sums differs.
-__global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* __restrict__ Lt,
-                                                                    const u32* __restrict__ RINV,
-                                                                    u32* __restrict__ X, int WL, int LF) {
+// NPL words per lane; GLOBAL: the slots in the scratch S (528 WP words per tile) instead of shared memory.
+template <int NPL, bool GLOBAL>
+__global__ void __launch_bounds__(kThreadsS) trinv_tiles_k(const u32* __restrict__ Lt, const u32* __restrict__ RINV,
+                                                           u32* __restrict__ X, u32* __restrict__ S, int WL, int LF) {
   extern __shared__ __align__(16) u32 sm[];
-  u32* Xm = sm;                                                  // slots tri(i, k), lower triangle
   const int WP = pitch(WL);
-  u32* Lcol = Xm + 528 * WP;                                     // |l_ij| of the current column j, by row i
-  WarpScratch* ws = reinterpret_cast<WarpScratch*>(Lcol + 32 * WP);
+  u32* Xm = GLOBAL ? S + (size_t)blockIdx.x * 528 * WP : sm;     // slots tri(i, k), lower triangle
+  u32* Lcol = GLOBAL ? sm : sm + 528 * WP;                       // |l_ij| of the current column j, by row i
+  WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(Lcol + 32 * WP);
   uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of finished x
   uint8_t* xt = xs + 528;
   uint8_t* ls = xt + 528;                                        // signs, tops of the column of L
@@ -760,7 +624,7 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
   __syncthreads();
   for (int i = warp; i < BT; i += kWarpsS) {                     // x_ii = r_i
     int top;
-    const int sg = load_mag(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WP, WL, top);
+    const int sg = load_mag<NPL>(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WP, WL, top);
     if (lane == 0) {
       xs[tri(i, i)] = (uint8_t)sg;
       xt[tri(i, i)] = (uint8_t)top;
@@ -769,7 +633,7 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
   for (int j = 0; j < BT - 1; j++) {
     for (int i = j + 1 + warp; i < BT; i += kWarpsS) {
       int top;
-      const int sg = load_mag(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WP, WL, top);
+      const int sg = load_mag<NPL>(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WP, WL, top);
       if (lane == 0) {
         ls[i] = (uint8_t)sg;
         lt[i] = (uint8_t)top;
@@ -793,7 +657,7 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
     __syncthreads();
     for (int k = warp; k <= j; k += kWarpsS) {                   // x_{j+1,k} = -(sum) r_{j+1}
       const int ei = tri(j + 1, k);
-      wmul(Xm + (size_t)ei * WP, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WP,
+      wmul<NPL>(Xm + (size_t)ei * WP, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WP,
            xs + ei, xt + ei);
       if (lane == 0) xs[ei] ^= 1;                                // the negation
       __syncwarp();
@@ -808,74 +672,95 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_smem_kernel(const u32* 
       continue;
     }
     const int ei = tri(i, k);
-    u32 v0 = lane < WL ? Xm[(size_t)ei * WP + lane] : 0u, v1 = lane + 32 < WL ? Xm[(size_t)ei * WP + lane + 32] : 0u;
-    if (xs[ei]) warp_negate(v0, v1, WL);
-    if (lane < WL) dst[lane] = v0;
-    if (lane + 32 < WL) dst[lane + 32] = v1;
+    u32 v[NPL];
+#pragma unroll
+    for (int c = 0; c < NPL; c++) v[c] = lane + 32 * c < WL ? Xm[(size_t)ei * WP + lane + 32 * c] : 0u;
+    if (xs[ei]) warp_negate<NPL>(v, WL);
+#pragma unroll
+    for (int c = 0; c < NPL; c++)
+      if (lane + 32 * c < WL) dst[lane + 32 * c] = v[c];
   }
 }
 
 
 // ---- batched triangular solve L y = v with one factored tile (sdpvibe/basecase.py:228-245): one warp per
-// vector, lane i owns v_i; for each j, lane j forms y_j = v_j r_j and broadcasts it, lanes i > j subtract
-// l_ij y_j.  V (nvec, 32, WL) is overwritten by y.
-__global__ void __launch_bounds__(kThreads) trsv_tiles_kernel(const u32* __restrict__ Lt, const u32* __restrict__ RINV,
-                                                              u32* __restrict__ V, i64 nvec, int WL, int LF) {
-  __shared__ u32 sp[kThreads / 32][WMAX];
+// vector; for each j the warp forms y_j = v_j r_j (warp product, written over v_j, its magnitude kept in
+// shared memory), then lane i > j subtracts l_ij y_j from its v_i (thread product of the signed l_ij read in
+// place).  V (nvec, 32, WL) is overwritten by y.
+template <int NPL>
+constexpr size_t trsv_smem_bytes() {
+  return (kThreads / 32) * (sizeof(WarpScratchT<NPL>) + 32 * NPL * 4 + 16);
+}
+template <int NPL>
+__global__ void __launch_bounds__(kThreads) trsv_tiles_k(const u32* __restrict__ Lt, const u32* __restrict__ RINV,
+                                                         u32* __restrict__ V, i64 nvec, int WL, int LF) {
+  extern __shared__ __align__(16) u32 sm[];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(sm) + wi;
+  u32* ymag = reinterpret_cast<u32*>(reinterpret_cast<WarpScratchT<NPL>*>(sm) + kThreads / 32) + wi * 32 * NPL;
+  uint8_t* yinfo = reinterpret_cast<uint8_t*>(reinterpret_cast<u32*>(reinterpret_cast<WarpScratchT<NPL>*>(sm) +
+                                                                    kThreads / 32) + (kThreads / 32) * 32 * NPL) + wi * 16;
   const i64 w = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31, ws = threadIdx.x >> 5;
   if (w >= nvec) return;                                         // the whole warp leaves together
-  u32* vi = V + ((size_t)w * BT + lane) * WL;
+  u32* V0 = V + (size_t)w * BT * WL;
   for (int j = 0; j < BT; j++) {
-    if (lane == j) {
-      fx_mul(vi, vi, RINV + (size_t)j * WL, 0, WL, LF);
-      for (int k = 0; k < WL; k++) sp[ws][k] = vi[k];
-    }
-    __syncwarp();
-    if (lane > j) {
-      u32 t[WMAX];
-      fx_mul(t, Lt + ((size_t)lane * BT + j) * WL, sp[ws], 0, WL, LF);
-      i64 br = 0;
-      for (int k = 0; k < WL; k++) {
-        const i64 d = (i64)vi[k] - (i64)t[k] + br;
-        vi[k] = (u32)d;
-        br = d >> 32;
-      }
-    }
+    u32* vj = V0 + (size_t)j * WL;
+    wmul<NPL>(vj, RINV + (size_t)j * WL, 0, WL, LF, *ws, vj, ymag, yinfo, yinfo + 1);     // y_j = v_j r_j
+    if (lane > j) fx_rmw_signed(V0 + (size_t)lane * WL, Lt + ((size_t)lane * BT + j) * WL, ymag, yinfo[1], yinfo[0],
+                                WL, LF);
     __syncwarp();
   }
 }
 }  // namespace
 
 namespace {
-// Opt-in shared memory of the tile kernels, set once per process for the largest fast-path tile (WL = FW).
+// Opt-in shared memory of the tile kernels (once per process and instantiation).
+template <class K>
+int smem_attr(K kernel, size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return e == cudaSuccess ? SDPV_OK : sdpv::set_cuda_error(e);
+}
 int smem_attributes() {
   static std::once_flag once;
-  static cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+  static int st = SDPV_OK;
   std::call_once(once, [] {
-    e1 = cudaFuncSetAttribute(chol_tiles_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)chol_smem_bytes(FW));
-    e2 = cudaFuncSetAttribute(trinv_tiles_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)trinv_smem_bytes(FW));
+    int r[4] = {smem_attr(chol_tiles_k<2, false>, chol_smem_bytes<2, false>(FW)),
+                smem_attr(trinv_tiles_k<2, false>, trinv_smem_bytes<2, false>(FW)),
+                smem_attr(chol_tiles_k<3, true>, chol_smem_bytes<3, true>(WMAX)),
+                smem_attr(trinv_tiles_k<3, true>, trinv_smem_bytes<3, true>(WMAX))};
+    for (int q = 0; q < 4; q++)
+      if (r[q] != SDPV_OK) st = r[q];
   });
-  if (e1 != cudaSuccess) return sdpv::set_cuda_error(e1);
-  if (e2 != cudaSuccess) return sdpv::set_cuda_error(e2);
-  return SDPV_OK;
+  return st;
+}
+
+// The triangular inverse: shared-memory slots for WL <= FW (S unused), slots in S (ntiles * 528 * (WL | 1)
+// words, within ntiles * 32 * 32 * WL) above.
+int launch_trinv(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint32_t* S, int64_t ntiles, int WL, int LF,
+                 void* stream) {
+  int st = smem_attributes();
+  if (st != SDPV_OK) return st;
+  if (WL <= FW)
+    trinv_tiles_k<2, false><<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes<2, false>(WL), sdpv::as_stream(stream)>>>(
+        Lt, RINV, X, nullptr, WL, LF);
+  else
+    trinv_tiles_k<3, true><<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes<3, true>(WL), sdpv::as_stream(stream)>>>(
+        Lt, RINV, X, S, WL, LF);
+  return sdpv::launch_status();
 }
 }  // namespace
 
 extern "C" int sdpv_chol_tiles(uint32_t* A, uint32_t* RINV, int64_t ntiles, int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
-  if (WL <= FW) {
-    int st = smem_attributes();
-    if (st != SDPV_OK) return st;
-    chol_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, chol_smem_bytes(WL), sdpv::as_stream(stream)>>>(
+  int st = smem_attributes();
+  if (st != SDPV_OK) return st;
+  if (WL <= FW)
+    chol_tiles_k<2, false><<<(unsigned)ntiles, kThreadsS, chol_smem_bytes<2, false>(WL), sdpv::as_stream(stream)>>>(
         A, RINV, WL, LF, sdpv::device_error_word());
-    return sdpv::launch_status();
-  }
-  chol_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(A, RINV, WL, LF,
-                                                                               sdpv::device_error_word());
+  else
+    chol_tiles_k<3, true><<<(unsigned)ntiles, kThreadsS, chol_smem_bytes<3, true>(WL), sdpv::as_stream(stream)>>>(
+        A, RINV, WL, LF, sdpv::device_error_word());
   return sdpv::launch_status();
 }
 
@@ -883,15 +768,8 @@ extern "C" int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32
                                 int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
-  if (WL <= FW) {                                   // shared-memory kernel: S is not used
-    int st = smem_attributes();
-    if (st != SDPV_OK) return st;
-    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
-        Lt, RINV, X, WL, LF);
-    return sdpv::launch_status();
-  }
-  trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, S, WL, LF);
-  return sdpv::launch_status();
+  if (WL > FW && !S) return SDPV_EINVAL;
+  return launch_trinv(Lt, RINV, X, S, ntiles, WL, LF, stream);
 }
 
 // ---------------------------------------------------------------- allocation-free variant of sdpv_trinv_tiles
@@ -934,13 +812,7 @@ extern "C" int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV
                                         int bt, int WL, int LF, void* stream) {
   if (bt != BT || WL < 2 || WL > WMAX || LF < 2 || LF >= WL || ntiles < 0 || ntiles > 0x7fffffff) return SDPV_EINVAL;
   if (ntiles == 0) return SDPV_OK;
-  if (WL <= FW) {                                   // shared-memory kernel: no scratch, no size limit
-    int st = smem_attributes();
-    if (st != SDPV_OK) return st;
-    trinv_tiles_smem_kernel<<<(unsigned)ntiles, kThreadsS, trinv_smem_bytes(WL), sdpv::as_stream(stream)>>>(
-        Lt, RINV, X, WL, LF);
-    return sdpv::launch_status();
-  }
+  if (WL <= FW) return launch_trinv(Lt, RINV, X, nullptr, ntiles, WL, LF, stream);   // no scratch, no size limit
   if ((uint64_t)ntiles * BT * BT * (uint64_t)WL > SDPV_TRINV_NOALLOC_WORDS) {
     sdpv::set_message("sdpv_trinv_tiles_noalloc: ntiles * 32 * 32 * WL exceeds the fixed scratch of 4 Mi words");
     return SDPV_EINVAL;
@@ -948,8 +820,7 @@ extern "C" int sdpv_trinv_tiles_noalloc(const uint32_t* Lt, const uint32_t* RINV
   uint32_t* scratch = nullptr;
   int st = trinv_scratch_address(&scratch);
   if (st != SDPV_OK) return st;
-  trinv_tiles_kernel<<<(unsigned)ntiles, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, X, scratch, WL, LF);
-  return sdpv::launch_status();
+  return launch_trinv(Lt, RINV, X, scratch, ntiles, WL, LF, stream);
 }
 
 extern "C" int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* V, int64_t nvec, int bt, int WL,
@@ -958,6 +829,11 @@ extern "C" int sdpv_trsv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_
   if (nvec == 0) return SDPV_OK;
   const i64 blocks = (nvec * 32 + kThreads - 1) / kThreads;
   if (blocks > 0x7fffffff) return SDPV_EINVAL;
-  trsv_tiles_kernel<<<(unsigned)blocks, kThreads, 0, sdpv::as_stream(stream)>>>(Lt, RINV, V, nvec, WL, LF);
+  if (WL <= FW)
+    trsv_tiles_k<2><<<(unsigned)blocks, kThreads, trsv_smem_bytes<2>(), sdpv::as_stream(stream)>>>(Lt, RINV, V, nvec, WL,
+                                                                                                     LF);
+  else
+    trsv_tiles_k<3><<<(unsigned)blocks, kThreads, trsv_smem_bytes<3>(), sdpv::as_stream(stream)>>>(Lt, RINV, V, nvec, WL,
+                                                                                                     LF);
   return sdpv::launch_status();
 }

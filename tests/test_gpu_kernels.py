@@ -647,10 +647,11 @@ def test_chol_graph_replay_matches_eager(sb):
 
 
 def test_trsv_tiles_vs_oracle(sb):
-    """sdpv_trsv_tiles (substitution with one factored tile, one warp per vector) against the oracle."""
+    """sdpv_trsv_tiles (substitution with one factored tile, one warp per vector) against the oracle, both
+    words-per-lane instantiations."""
     from sdpvibe_b200 import _lib
     rng = np.random.default_rng(5)
-    for L in (8, 26):
+    for L in (8, 26, 40, 44):                       # WL 68 > 64: three words per lane
         WL, LF = L + 24, L
         W = _spd_tiles(rng, 1, L, False)
         RA, RR = O.chol_tiles(W, 32, WL, LF)
