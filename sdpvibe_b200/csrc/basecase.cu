@@ -198,29 +198,47 @@ __device__ __forceinline__ int load_mag(const u32* src, u32* m, int WL, int& top
   return sign;
 }
 
-// Warp-cooperative truncated product a * b >> F (top t words of each operand when t > 0): one product
-// column per lane, columns kmin .. min(kmax + 2, LF + WL - 1), each a 96-bit exact sum; the column sums are
-// added with their 32- and 64-bit shifts and the carries resolved by chain_carry.  Outputs (any may be
-// null): out = signed result (may alias a or b), omag = magnitude, *osign / *otop (written by lane 0).
+// Warp-cooperative truncated product of magnitudes: out = trunc(x y) (top t words of each operand when t > 0;
+// tops tx, ty): one product column per lane, columns kmin .. min(kmax + 2, LF + WL - 1), each a 96-bit exact
+// sum; the column sums are added with their 32- and 64-bit shifts and the carries resolved by chain_carry.
+// x, y: shared memory (read at words <= their tops); out: 32 NPL words of shared memory, overwritten.
 template <int NPL>
-__device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScratchT<NPL>& s, u32* out, u32* omag,
-                     uint8_t* osign, uint8_t* otop) {
+__device__ void wmul_core(const u32* x, int tx, const u32* y, int ty, int t, int WL, int LF, u32* out) {
   const int lane = threadIdx.x & 31;
-  int ta, tb;
-  const int sa = load_mag<NPL>(a, s.xa, WL, ta);
-  const int sb = load_mag<NPL>(b, s.xb, WL, tb);
-  __syncwarp();
 #pragma unroll
-  for (int c = 0; c < NPL; c++) s.acc[lane + 32 * c] = 0;
-  const int la = t ? max(0, ta - t + 1) : 0, lb = t ? max(0, tb - t + 1) : 0;
-  const int kmin = max(LF - 2, la + lb), kmax = ta + tb;
+  for (int c = 0; c < NPL; c++) out[lane + 32 * c] = 0;
+  const int la = t ? max(0, tx - t + 1) : 0, lb = t ? max(0, ty - t + 1) : 0;
+  const int kmin = max(LF - 2, la + lb), kmax = tx + ty;
   const int ncol = min(kmax + 2, LF + WL - 1) - kmin + 1;
   __syncwarp();
   u32 p_c1 = 0, p_c2a = 0, p_c2b = 0, p_h = 0, cin = 0;          // carried over from the previous 32 columns
   for (int q0 = 0; q0 < ncol; q0 += 32) {
     const int q = q0 + lane, k = kmin + q;
+    // column k = sum of x[i] y[k - i], i0 <= i <= i1: every lane runs the warp's longest column (its own
+    // terms past i1 are zeros), four carry chains, so the loop neither diverges nor waits on one chain
     u32 c0 = 0, c1 = 0, c2 = 0;
-    if (q < ncol && k <= kmax) column96(c0, c1, c2, s.xa, s.xb, k, max(la, k - tb), min(ta, k - lb));
+    {
+      const bool act = q < ncol && k <= kmax;
+      const int i0 = max(la, k - ty), i1 = act ? min(tx, k - lb) : i0 - 1;
+      const int nt = (int)__reduce_max_sync(kFull, (unsigned)max(i1 - i0 + 1, 0));
+      u32 d0 = 0, d1 = 0, d2 = 0, e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
+      for (int j = 0; j < nt; j += 4) {
+        u32 a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int i = i0 + j + u;
+          a[u] = i <= i1 ? x[i] : 0u;
+          b[u] = i <= i1 ? y[k - i] : 0u;
+        }
+        mac96(c0, c1, c2, a[0], b[0]);
+        mac96(d0, d1, d2, a[1], b[1]);
+        mac96(e0, e1, e2, a[2], b[2]);
+        mac96(f0, f1, f2, a[3], b[3]);
+      }
+      add96(d0, d1, d2, f0, f1, f2);
+      add96(c0, c1, c2, e0, e1, e2);
+      add96(c0, c1, c2, d0, d1, d2);
+    }
     u32 c1u = __shfl_up_sync(kFull, c1, 1), c2u = __shfl_up_sync(kFull, c2, 2);
     if (lane == 0) c1u = p_c1;
     if (lane == 0) c2u = p_c2a;
@@ -235,7 +253,7 @@ __device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScra
     u32 cout;
     const u32 cj = chain_carry(e < lo, e == kFull, cin, cout);
     const int w = k - LF;
-    if (q < ncol && w >= 0 && w < WL) s.acc[w] = e + cj;
+    if (q < ncol && w >= 0 && w < WL) out[w] = e + cj;
     p_c1 = n_c1;
     p_c2a = n_c2a;
     p_c2b = n_c2b;
@@ -243,6 +261,20 @@ __device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScra
     cin = cout;
   }
   __syncwarp();
+}
+
+// The truncated product a * b >> F of two's-complement operands (magnitudes multiplied by wmul_core, sign
+// applied last).  Outputs (any may be null): out = signed result (may alias a or b), omag = magnitude,
+// *osign / *otop (written by lane 0).
+template <int NPL>
+__device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScratchT<NPL>& s, u32* out, u32* omag,
+                     uint8_t* osign, uint8_t* otop) {
+  const int lane = threadIdx.x & 31;
+  int ta, tb;
+  const int sa = load_mag<NPL>(a, s.xa, WL, ta);
+  const int sb = load_mag<NPL>(b, s.xb, WL, tb);
+  __syncwarp();
+  wmul_core<NPL>(s.xa, ta, s.xb, tb, t, WL, LF, s.acc);
   u32 m[NPL];
 #pragma unroll
   for (int c = 0; c < NPL; c++) m[c] = lane + 32 * c < WL ? s.acc[lane + 32 * c] : 0u;
@@ -264,6 +296,68 @@ __device__ void wmul(const u32* a, const u32* b, int t, int WL, int LF, WarpScra
       if (lane + 32 * c < WL) out[lane + 32 * c] = m[c];
   }
   __syncwarp();
+}
+
+// ---- register-resident WL-word arithmetic of one warp (word lane + 32 c in v[c], zero at and above WL)
+template <int NPL>
+__device__ __forceinline__ void reg_load(const u32* src, u32 (&v)[NPL], int WL) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < NPL; c++) v[c] = lane + 32 * c < WL ? src[lane + 32 * c] : 0u;
+}
+template <int NPL>
+__device__ __forceinline__ void reg_store(u32* dst, const u32 (&v)[NPL], int WL) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < NPL; c++)
+    if (lane + 32 * c < WL) dst[lane + 32 * c] = v[c];
+}
+// word w of v, in every lane
+template <int NPL>
+__device__ __forceinline__ u32 reg_word(const u32 (&v)[NPL], int w) {
+  u32 r = 0;
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    const u32 x = __shfl_sync(kFull, v[c], w & 31);
+    if (c == (w >> 5)) r = x;
+  }
+  return r;
+}
+// r = a + b or a - b (mod 2^(32 WL)); r may alias a or b
+template <int NPL>
+__device__ __forceinline__ void reg_addsub(u32 (&r)[NPL], const u32 (&a)[NPL], const u32 (&b)[NPL], bool sub, int WL) {
+  const int lane = threadIdx.x & 31;
+  u32 carry = sub ? 1u : 0u;
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    const bool in = lane + 32 * c < WL;
+    const u32 av = in ? a[c] : 0u, bv = in ? (sub ? ~b[c] : b[c]) : 0u;
+    const u64 v = (u64)av + bv;
+    const u32 e = (u32)v;
+    u32 cout;
+    const u32 cj = chain_carry((v >> 32) != 0, e == kFull, carry, cout);
+    r[c] = in ? e + cj : 0u;
+    carry = cout;
+  }
+}
+// arithmetic shift right by one bit (floor of half)
+template <int NPL>
+__device__ __forceinline__ void reg_shr1(u32 (&x)[NPL], int WL) {
+  const int lane = threadIdx.x & 31;
+  u32 up[NPL], first[NPL];
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    up[c] = __shfl_down_sync(kFull, x[c], 1);                     // word w + 1 within the chunk
+    first[c] = __shfl_sync(kFull, x[c], 0);                        // word 32 c
+  }
+#pragma unroll
+  for (int c = 0; c < NPL; c++) {
+    const int w = lane + 32 * c;
+    const u32 nx = lane < 31 ? up[c] : (c + 1 < NPL ? first[c + 1 < NPL ? c + 1 : c] : 0u);
+    if (w < WL - 1) x[c] = (x[c] >> 1) | (nx << 31);
+    else if (w == WL - 1) x[c] = (u32)(((int32_t)x[c]) >> 1);
+    else x[c] = 0u;
+  }
 }
 
 // dst (two's complement, WL words) += trunc(|x| |y|) if add, else -= ; x, y magnitudes with tops tx, ty.
@@ -539,19 +633,81 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
       fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
     }
     __syncwarp();
-    for (int bits = 100;; bits *= 2) {                             // r <- r + r (1 - d r^2) / 2
-      int t = bits / 32 + 2;
-      if (t >= WL) t = 0;
-      wmul<NPL>(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
-      wmul<NPL>(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-      warp_addsub<NPL>(st1, sone, st2, true, WL);
-      wmul<NPL>(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
-      warp_shr1<NPL>(st2, WL);
-      warp_addsub<NPL>(sr, sr, st2, false, WL);
-      if (t == 0) break;
+    u32 D[NPL];
+    reg_load<NPL>(sd, D, WL);
+    const bool dneg = reg_word<NPL>(D, WL - 1) >> 31;
+    bool dnz = false;
+#pragma unroll
+    for (int c = 0; c < NPL; c++) dnz = dnz || __any_sync(kFull, D[c] != 0u);
+    if (!dneg && dnz) {
+      // d > 0: the same truncated products as below, with the operands kept as magnitudes in shared memory
+      // (|r| in sr, d in sd, |1 - d r^2| in ws[0].xa) and the additions, sign changes and halvings done in
+      // registers; r stays positive in practice, its sign is carried all the same
+      const int td = warp_top<NPL>(D, WL);
+      u32 R[NPL], Rt[NPL], P[NPL], S[NPL], O[NPL];
+      reg_load<NPL>(sr, Rt, WL);                                  // r, two's complement
+#pragma unroll
+      for (int c = 0; c < NPL; c++) {
+        O[c] = (lane + 32 * c == LF) ? 1u : 0u;                   // fixed-point 1
+        R[c] = Rt[c];
+      }
+      u32 sR = reg_word<NPL>(Rt, WL - 1) >> 31;
+      if (sR) {
+        warp_negate<NPL>(R, WL);
+        reg_store<NPL>(sr, R, WL);
+        __syncwarp();
+      }
+      int tr = warp_top<NPL>(R, WL);
+      for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
+        int t = bits / 32 + 2;
+        if (t >= WL) t = 0;
+        wmul_core<NPL>(sr, tr, sr, tr, t, WL, LF, st1);           // r^2
+        reg_load<NPL>(st1, P, WL);
+        const int tp = warp_top<NPL>(P, WL);
+        wmul_core<NPL>(st1, tp, sd, td, t, WL, LF, st2);          // d r^2
+        reg_load<NPL>(st2, P, WL);
+        reg_addsub<NPL>(S, O, P, true, WL);                        // 1 - d r^2
+        const u32 sS = reg_word<NPL>(S, WL - 1) >> 31;
+        if (sS) warp_negate<NPL>(S, WL);
+        const int ts = warp_top<NPL>(S, WL);
+        reg_store<NPL>(ws[0].xa, S, WL);
+        __syncwarp();
+        wmul_core<NPL>(sr, tr, ws[0].xa, ts, t, WL, LF, st2);     // |r (1 - d r^2)|
+        reg_load<NPL>(st2, P, WL);
+        if (sR ^ sS) warp_negate<NPL>(P, WL);
+        reg_shr1<NPL>(P, WL);                                      // floor of half
+        reg_addsub<NPL>(Rt, Rt, P, false, WL);
+        sR = reg_word<NPL>(Rt, WL - 1) >> 31;
+#pragma unroll
+        for (int c = 0; c < NPL; c++) R[c] = Rt[c];
+        if (sR) warp_negate<NPL>(R, WL);
+        tr = warp_top<NPL>(R, WL);
+        reg_store<NPL>(sr, R, WL);
+        __syncwarp();
+        if (t == 0) break;
+      }
+      wmul_core<NPL>(sd, td, sr, tr, 0, WL, LF, st1);             // l_kk = d * d^-1/2
+      reg_load<NPL>(st1, P, WL);
+      if (sR) warp_negate<NPL>(P, WL);
+      reg_store<NPL>(akk, P, WL);
+      reg_store<NPL>(sr, Rt, WL);                                  // r, two's complement, for the column
+      reg_store<NPL>(RI + (size_t)k * WL, Rt, WL);
+      __syncwarp();
+    } else {
+      for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
+        int t = bits / 32 + 2;
+        if (t >= WL) t = 0;
+        wmul<NPL>(sr, sr, t, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+        wmul<NPL>(st1, sd, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+        warp_addsub<NPL>(st1, sone, st2, true, WL);
+        wmul<NPL>(sr, st1, t, WL, LF, ws[0], st2, nullptr, nullptr, nullptr);
+        warp_shr1<NPL>(st2, WL);
+        warp_addsub<NPL>(sr, sr, st2, false, WL);
+        if (t == 0) break;
+      }
+      wmul<NPL>(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);   // l_kk = d * d^-1/2
+      for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
     }
-    wmul<NPL>(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);     // l_kk = d * d^-1/2
-    for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
   };
   if (warp == 0) pivot(0);
   __syncthreads();
