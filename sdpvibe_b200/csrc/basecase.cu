@@ -450,6 +450,58 @@ __device__ __forceinline__ void fx_rmw_reg(u32* dst, const u32* x, const u32* y,
   while (cy && w < WL) emit(0);
 }
 
+// fx_rmw with both operands bounded by compile-time tops (|x| top <= LX, |y| top <= LY) and LF fraction words:
+// both in registers, every column sum unrolled over its exact term range (columns LF - 2 .. LX + LY, zero
+// beyond the actual tops), so no multiply-add is predicated away.  The same result as fx_rmw.
+template <int LF_, int LX, int LY>
+__device__ __forceinline__ void fx_rmw_reg2(u32* dst, const u32* x, const u32* y, bool add, int WL) {
+  u32 xr[LX + 1], yr[LY + 1];
+#pragma unroll
+  for (int i = 0; i <= LX; i++) xr[i] = x[i];
+#pragma unroll
+  for (int i = 0; i <= LY; i++) yr[i] = y[i];
+  u32 c0 = 0, c1 = 0, c2 = 0, cy = 0;
+  int w = 0;
+  auto emit = [&](u32 d) {
+    if (w < WL) {
+      const u32 o = dst[w];
+      if (add) {
+        const u64 r = (u64)o + d + cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 32);
+      } else {
+        const u64 r = (u64)o - d - cy;
+        dst[w] = (u32)r;
+        cy = (u32)(r >> 63);
+      }
+      w++;
+    }
+  };
+#pragma unroll
+  for (int k = LF_ - 2; k <= LX + LY; k++) {
+    u32 d0 = 0, d1 = 0, d2 = 0, e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;   // four carry chains
+    const int i0 = k - LY > 0 ? k - LY : 0, i1 = k < LX ? k : LX;
+#pragma unroll
+    for (int i = i0; i <= i1; i++) {
+      const int ch = (i - i0) & 3;
+      if (ch == 0) mac96(c0, c1, c2, xr[i], yr[k - i]);
+      else if (ch == 1) mac96(d0, d1, d2, xr[i], yr[k - i]);
+      else if (ch == 2) mac96(e0, e1, e2, xr[i], yr[k - i]);
+      else mac96(f0, f1, f2, xr[i], yr[k - i]);
+    }
+    add96(d0, d1, d2, f0, f1, f2);
+    add96(c0, c1, c2, e0, e1, e2);
+    add96(c0, c1, c2, d0, d1, d2);
+    if (k >= LF_) emit(c0);
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  emit(c0);                                              // columns LX + LY + 1, + 2: no new terms
+  emit(c1);
+  while (cy && w < WL) emit(0);
+}
+
 // fx_rmw with only the first operand bounded (top <= LFT, kept in registers) and the second read from shared
 // memory (one load per multiply-add instead of two): the triangular inverse's products |l_ij| |x_jk|.
 template <int LFT>
@@ -803,7 +855,11 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_k(const u32* __restrict
       u32* dst = Xm + (size_t)tri(i, k) * WP;
       const u32 *xl = Lcol + (size_t)i * WP, *yx = Xm + (size_t)e * WP;
       const bool add = ls[i] == xs[e];
-      if (LF == 26 && lt[i] <= 26)
+      if (LF == 26 && lt[i] <= 26 && xt[e] <= 30)
+        fx_rmw_reg2<26, 26, 30>(dst, xl, yx, add, WL);
+      else if (LF == 24 && lt[i] <= 24 && xt[e] <= 28)
+        fx_rmw_reg2<24, 24, 28>(dst, xl, yx, add, WL);
+      else if (LF == 26 && lt[i] <= 26)
         fx_rmw_lreg<26>(dst, xl, yx, xt[e], add, WL);
       else if (LF == 24 && lt[i] <= 24)
         fx_rmw_lreg<24>(dst, xl, yx, xt[e], add, WL);
