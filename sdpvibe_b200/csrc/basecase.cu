@@ -767,11 +767,21 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
   // pivot k+1's Newton chain while warps 1.. apply the rest of step k's trailing update.  Every entry gets
   // the same truncated products as without look-ahead (their exact sum is order-free).
   for (int k = 0; k < BT; k++) {
-    for (int i = k + 1 + warp; i < BT; i += kWarpsS) {           // l_ik = a_ik * r_k
-      u32* aik = ent(i, k);
-      wmul<NPL>(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
+    // l_ik = a_ik * r_k: warp 0 takes row k + 1 (its next pivot needs only that row) and goes on without
+    // waiting; warps 1.. take the other rows and wait for the whole column (barrier 1: warp 0 arrives)
+    if (warp == 0) {
+      if (k + 1 < BT) {
+        u32* aik = ent(k + 1, k);
+        wmul<NPL>(aik, sr, 0, WL, LF, ws[0], aik, colmag + (size_t)(k + 1) * WP, colsign + k + 1, coltop + k + 1);
+      }
+      asm volatile("bar.arrive 1, %0;" ::"r"(kThreadsS) : "memory");
+    } else {
+      for (int i = k + 1 + warp; i < BT; i += kWarpsS - 1) {
+        u32* aik = ent(i, k);
+        wmul<NPL>(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
+      }
+      asm volatile("bar.sync 1, %0;" ::"r"(kThreadsS) : "memory");
     }
-    __syncthreads();
     if (k == BT - 1) break;
     if (warp == 0) {
       u32* dn = ent(k + 1, k + 1);                // a_{k+1,k+1} -= l_{k+1,k}^2
