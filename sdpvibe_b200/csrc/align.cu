@@ -163,44 +163,50 @@ __global__ void align_kernel(const int32_t* __restrict__ m, const i64* __restric
   shift_entry32([&](int i) { return (u32)__ldg(m + (i64)i * n + idx); }, L, s, Lout, out + idx, n, err);
 }
 
-// Transpose: tiles of 16 rows x 32 columns staged with all limbs; out is (Lout, nb, C, R).
+// Transpose: tiles of ATR = 8 rows x 32 columns staged with all limbs (about 30 KB at 26 limbs, so seven CTAs
+// share an SM and hide each other's loads); out is (Lout, nb, C, R), written in 32-byte runs (8 rows) per
+// column and limb.  The tiles of one row band run next to each other (column tile fastest in the 1-D grid),
+// so the 32-byte sectors that two column tiles share are read from DRAM once; staged rows are ATP = 36 words
+// apart, which puts the 8 rows x 4 columns that a warp's lanes read at once in distinct banks.
 constexpr int TR = 16, TC = 32;
+constexpr int ATR = 8, ATP = 36;
 __global__ void __launch_bounds__(kThreads) align_t_kernel(const int32_t* __restrict__ m, const i64* __restrict__ e,
                                                            int L, i64 nb, i64 R, i64 C, const i64* __restrict__ target,
                                                            int per_col, int Lout, i64 Rld, int32_t* __restrict__ out,
                                                            unsigned* err) {
-  extern __shared__ u32 sm[];                       // [L][TR][TC + 1] limbs, then [TR][TC] exponents
-  i64* se = reinterpret_cast<i64*>(sm + (size_t)L * TR * (TC + 1) + ((L * TR * (TC + 1)) & 1));
+  extern __shared__ u32 sm[];                       // [L][ATR][ATP] limbs, then [ATR][TC + 1] exponents
+  i64* se = reinterpret_cast<i64*>(sm + (size_t)L * ATR * ATP);
   const i64 n = nb * R * C, no = nb * C * Rld;      // input / output plane sizes
   const i64 b = blockIdx.z;
-  const i64 r0 = (i64)blockIdx.x * TR, c0 = (i64)blockIdx.y * TC;
+  const i64 nct = (C + TC - 1) / TC;
+  const i64 r0 = (i64)(blockIdx.x / nct) * ATR, c0 = (i64)(blockIdx.x % nct) * TC;
   const int tid = threadIdx.x;
-  for (int pos = tid; pos < TR * TC; pos += kThreads) {     // all copies in flight at once
+  for (int pos = tid; pos < ATR * TC; pos += kThreads) {     // all copies in flight at once
     const int rr = pos / TC, cc = pos % TC;
     const i64 r = r0 + rr, c = c0 + cc;
     const bool in = r < R && c < C;
     const int32_t* src = m + (in ? (b * R + r) * C + c : 0);
-    u32* dst = &sm[rr * (TC + 1) + cc];
+    u32* dst = &sm[rr * ATP + cc];
     const u32 nb4 = in ? 4u : 0u;
-    for (int l = 0; l < L; l++, src += n, dst += TR * (TC + 1)) cp_async4(dst, src, nb4);
+    for (int l = 0; l < L; l++, src += n, dst += ATR * ATP) cp_async4(dst, src, nb4);
   }
   cp_async_commit();
-  for (int t = tid; t < TR * TC; t += kThreads) {
+  for (int t = tid; t < ATR * TC; t += kThreads) {
     int rr = t / TC, cc = t % TC;
     i64 r = r0 + rr, c = c0 + cc;
-    se[t] = (r < R && c < C) ? e[(b * R + r) * C + c] : SDPV_EZ;
+    se[rr * (TC + 1) + cc] = (r < R && c < C) ? e[(b * R + r) * C + c] : SDPV_EZ;
   }
   cp_async_wait<0>();
   __syncthreads();
   // thread -> (cc, rr) with rr fastest, so output stores (fast axis = r) are coalesced
-  for (int t = tid; t < TR * TC; t += kThreads) {
-    int rr = t % TR, cc = t / TR;
+  for (int t = tid; t < ATR * TC; t += kThreads) {
+    int rr = t % ATR, cc = t / ATR;
     i64 r = r0 + rr, c = c0 + cc;
     if (r >= R || c >= C) continue;
-    i64 ev = se[rr * TC + cc];
+    i64 ev = se[rr * (TC + 1) + cc];
     i64 s = (ev == SDPV_EZ) ? (1ll << 30) : target[per_col ? b * C + c : b * R + r] - ev;
-    const u32* base = sm + rr * (TC + 1) + cc;
-    shift_entry32([&](int i) { return base[i * TR * (TC + 1)]; }, L, s, Lout, out + (b * C + c) * Rld + r, no, err);
+    const u32* base = sm + rr * ATP + cc;
+    shift_entry32([&](int i) { return base[i * ATR * ATP]; }, L, s, Lout, out + (b * C + c) * Rld + r, no, err);
   }
 }
 
@@ -416,18 +422,19 @@ extern "C" int sdpv_align_t(const int32_t* m, const int64_t* e, int L, int64_t n
   cudaStream_t st = sdpv::as_stream(stream);
   unsigned* err = sdpv::device_error_word();
   {
-    size_t smem = (size_t)L * TR * (TC + 1) * 4 + 8 + TR * TC * 8;
+    size_t smem = (size_t)L * ATR * ATP * 4 + ATR * (TC + 1) * 8;
     static bool attr[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (!attr[dev & 63]) {
       cudaError_t ce = cudaFuncSetAttribute(align_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            64 * TR * (TC + 1) * 4 + 8 + TR * TC * 8);
+                                            64 * ATR * ATP * 4 + ATR * (TC + 1) * 8);
       if (ce != cudaSuccess) return sdpv::set_cuda_error(ce);
       attr[dev & 63] = true;
     }
-    dim3 grid((unsigned)((R + TR - 1) / TR), (unsigned)((C + TC - 1) / TC), (unsigned)nb);
-    if (grid.y > 65535 || (R + TR - 1) / TR > 0x7fffffff) return SDPV_EINVAL;
+    const i64 tiles = ((R + ATR - 1) / ATR) * ((C + TC - 1) / TC);
+    if (tiles > 0x7fffffff) return SDPV_EINVAL;
+    dim3 grid((unsigned)tiles, 1, (unsigned)nb);
     align_t_kernel<<<grid, kThreads, smem, st>>>(m, e, L, nb, R, C, target, per_col, Lout, Rld, out, err);
   }
   return sdpv::launch_status();

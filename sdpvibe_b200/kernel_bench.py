@@ -1,7 +1,7 @@
 """Per-kernel timing of the multiprecision hot path on one GPU (CUDA events, after warm-up).
 
   python -m sdpvibe_b200.kernel_bench --kernel syrk --N 274 --K 7000 --L 27 --reps 20
-  kernels: residues | gemm | syrk | crt | mpfgemm | bgemm (--nb stacked blocks) | cholsolve (batched
+  kernels: residues | align (the Gram chunk's column alignment) | gemm | syrk | crt | mpfgemm | bgemm (--nb stacked blocks) | cholsolve (batched
   Cholesky + solve over uneven blocks) | tiles (--nb 32 x 32 base tiles: factorisation and inverse) |
   solve (mpf.Chol of --nb SPD blocks of size --M, then L^-1 B with B (nb, M, N): per-kernel device time of
   the eager sequence and the time of its CUDA-graph replay)
@@ -175,8 +175,8 @@ def main():
     from . import mpf
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="syrk", choices=("residues", "gemm", "syrk", "crt", "mpfgemm", "cholsolve", "bgemm",
-                                                             "tiles", "solve"))
+    ap.add_argument("--kernel", default="syrk", choices=("residues", "align", "gemm", "syrk", "crt", "mpfgemm", "cholsolve",
+                                                             "bgemm", "tiles", "solve"))
     ap.add_argument("--nb", type=int, default=1, help="bgemm: number of stacked blocks")
     ap.add_argument("--blocks", type=int, default=600, help="cholsolve: number of SPD blocks")
     ap.add_argument("--nmin", type=int, default=8)
@@ -216,6 +216,17 @@ def main():
                 ts = _events(lambda: R.accumulate(Bh, Bl, Ah, Al, acc, unsigned=not a.packed), a.reps, a.warmup)
                 ops = R.n * 8 * a.M * a.N * a.K
             out.update(ms=min(ts), ms_mean=float(np.mean(ts)), tops=ops / (min(ts) * 1e-3) / 1e12)
+    elif a.kernel == "align":
+        # a Gram chunk: K rows x N columns of (L-1)-limb MPF entries, columns rounded to their top - NB and
+        # transposed into L limb planes (sdpv_align_t)
+        La = a.L - 1
+        mm = rng.integers(-(1 << 31), 1 << 31, size=(La, a.K, a.N), dtype=np.int64).astype(np.int32)
+        P = mpf.MPF(torch.from_numpy(mm).to(dev), torch.from_numpy(rng.integers(-8, 9, size=(a.K, a.N))).to(dev))
+        target = (mpf.top_max(P, over_rows=True)[0] - mpf.NBITS(La))[None].contiguous()
+        ld = -(-a.K // 4) * 4
+        ts = _events(lambda: mpf.aligned(P, target, per_col=True, transpose=True, Lout=a.L, ld=ld), a.reps, a.warmup)
+        bytes_ = a.N * a.K * (4 * La + 8 + 4 * a.L)
+        out.update(ms=min(ts), ms_mean=float(np.mean(ts)), gbs=bytes_ / (min(ts) * 1e-3) / 1e9)
     elif a.kernel == "bgemm":
         # batched residue GEMM of nb stacked blocks (M x K) (N x K), as the Cholesky/trsm recursion issues
         X = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.nb * a.M, a.K), dtype=np.int64)
