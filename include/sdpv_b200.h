@@ -222,6 +222,16 @@ int sdpv_trinv_tiles(const uint32_t* Lt, const uint32_t* RINV, uint32_t* X, uint
 /* sdpv_mpf_add that runs only if *pred (a device int32) is nonzero; O may alias A (in-place accumulation).
  * With sdpv_crt_norm_if it lets GramAcc add a flushed partial sum without a host decision
  * (sdpvibe/mpf.py:612-616). */
+/* One Gram chunk's column bookkeeping on the device (GramAcc.add, sdpvibe/mpf.py:556-579): from the chunk's
+ * column tops tp (N), updates the reference exponents E and the running tops Tmax in place, writes the flush
+ * predicate *f (some seen column outgrew E by more than head bits), the flush's CRT exponents rE_old (E - nbits
+ * before the update, 0 for unseen columns), the chunk's alignment targets (E - nbits after it), and adds *f to
+ * *nflush when has_acc.  One launch instead of the elementwise sequence. */
+int sdpv_gram_columns(int64_t N, const int64_t* tp, int64_t* E, int64_t* Tmax, int64_t head, int64_t nbits, int has_acc,
+                      int64_t* rE_old, int64_t* target, int32_t* f, int64_t* nflush, void* stream);
+/* Zeroes nbytes (a multiple of 16, 16-byte aligned) at p when *pred (a device int32) is nonzero: the Gram
+ * accumulator after a flush, decided on the device. */
+int sdpv_zero_if(void* p, int64_t nbytes, const int32_t* pred, void* stream);
 int sdpv_mpf_add_if(int L, int64_t n, const int32_t* A, const int64_t* eA, const int32_t* Bm, const int64_t* eB,
                     int sgn, int32_t* O, int64_t* eO, const int32_t* pred, void* stream);
 

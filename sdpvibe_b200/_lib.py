@@ -34,6 +34,8 @@ _SIGS = {
     "sdpv_mpf_mul": [_I, _L, _P, _P, _P, _P, _I, _P, _P, _P],
     "sdpv_mpf_add": [_I, _L, _P, _P, _P, _P, _I, _P, _P, _P],
     "sdpv_mpf_add_if": [_I, _L, _P, _P, _P, _P, _I, _P, _P, _P, _P],
+    "sdpv_gram_columns": [_L, _P, _P, _P, _L, _L, _I, _P, _P, _P, _P, _P],
+    "sdpv_zero_if": [_P, _L, _P, _P],
     "sdpv_mpf_norm": [_I, _I, _L, _P, _P, _P, _P, _P],
     "sdpv_mpf_from_f64": [_I, _L, _P, _P, _P, _P],
     "sdpv_schur_assemble": [_I, _L, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _P, _P],

@@ -420,9 +420,9 @@ class GramAcc:
     (sdpvibe/mpf.py:536-630).  A column that outgrows its HEAD bits of headroom forces a flush (CRT of
     the partial sum, added in MPF).  Only the lower triangle of the result is defined.
 
-    The flush decision is taken on the device (a predicated CRT and a predicated in-place MPF add instead
-    of a host branch),
-    so ``add`` never waits for the GPU and a whole accumulation can be captured in a CUDA graph; the
+    The flush decision is taken on the device (one bookkeeping kernel per chunk computes the predicate and the
+    exponents; a predicated CRT, a predicated in-place MPF add and a predicated zeroing instead of a host
+    branch), so ``add`` never waits for the GPU and a whole accumulation can be captured in a CUDA graph; the
     arithmetic, and so every bit of the result, is that of the host-branch formulation."""
     HEAD = 28
     OPERAND_ROWS = False       # True: align to operand rows and decompose them (sdpv_align_rows / _residues_rows)
@@ -430,11 +430,15 @@ class GramAcc:
     def __init__(self, N, L, E_ref=None):
         self.N, self.L = N, L
         self.R = ctx(L + 1)
-        self.E = E_ref.clone() if E_ref is not None else torch.full((N,), EZ, dtype=torch.int64, device=dev)
+        self.E = (E_ref.to(torch.int64).contiguous().clone() if E_ref is not None
+                  else torch.full((N,), EZ, dtype=torch.int64, device=dev))
         self.Tmax = torch.full((N,), EZ, dtype=torch.int64, device=dev)
         self.acc = None
         self.part = None                       # sum of the flushed partial sums (zero until the first flush)
         self._nflush = torch.zeros((), dtype=torch.int64, device=dev)
+        self._f = torch.zeros((), dtype=torch.int32, device=dev)          # this chunk's flush predicate
+        self._rE = torch.empty((N,), dtype=torch.int64, device=dev)       # the flush's CRT exponents
+        self._target = torch.empty((1, N), dtype=torch.int64, device=dev)  # the chunk's alignment targets
 
     @property
     def flushes(self):
@@ -444,22 +448,21 @@ class GramAcc:
         """P: MPF (rows, N)."""
         L, N, R = self.L, self.N, self.R
         tp = top_max(P, over_rows=True)[0]                           # column tops (mpf.py:563)
-        live = tp > EZ // 2
-        self.Tmax = torch.maximum(self.Tmax, tp)
-        known = self.E > EZ // 2
-        f = (live & known & (tp > self.E + self.HEAD)).any()         # flush?  (device bool)
-        if self.acc is not None:
-            self._flush_if(f)
-        self.E = torch.where(f & live & (tp > self.E), tp, self.E)
-        known = self.E > EZ // 2
-        self.E = torch.where(live & ~known, tp, self.E)
+        # flush predicate, the flush's CRT exponents (old E), the E / Tmax updates and the alignment targets
+        # (mpf.py:564-575) in one launch; the flush itself runs predicated on the device
+        had_acc = self.acc is not None
+        _lib.call("sdpv_gram_columns", N, _lib.ptr(tp), _lib.ptr(self.E), _lib.ptr(self.Tmax), self.HEAD, NBITS(L),
+                  int(had_acc), _lib.ptr(self._rE), _lib.ptr(self._target), _lib.ptr(self._f),
+                  _lib.ptr(self._nflush), _lib.stream())
+        if had_acc:
+            self._flush_if()
         rows = P.shape[0]
         if self.acc is None:
             # rows padded to a multiple of 8 entries (16 bytes) for the vectorised GEMM epilogue
             self.acc = torch.zeros((R.n, N, -(-N // 8) * 8), dtype=torch.int16, device=dev)
         if not rows:
             return
-        target = (self.E - NBITS(L))[None, :]
+        target = self._target
         if self.OPERAND_ROWS and L + 1 <= 63:
             # columns aligned to E_j - NB in L+1 limbs as operand rows (column j's rows padded to a multiple of
             # 128), decomposed straight from them
@@ -475,24 +478,25 @@ class GramAcc:
             X = aligned(P, target, per_col=True, transpose=True, Lout=L + 1, ld=ld).view(L + 1, N, ld)
             residue_product(R, X, None, self.acc, syrk=True, kvalid=rows)
 
-    def _crt(self, pred=None):
+    def _crt(self, pred=None, rE=None):
         L, N, R = self.L, self.N, self.R
-        rE = torch.where(self.E > EZ // 2, self.E - NBITS(L), torch.zeros_like(self.E))
+        if rE is None:
+            rE = torch.where(self.E > EZ // 2, self.E - NBITS(L), torch.zeros_like(self.E))
         Om, Oe = R.crt_norm(self.acc, self.acc.shape[2], 0, N, N, rE, rE[None, :], L, pred=pred)
         return MPF(Om.view(L, N, N), Oe.view(N, N))
 
-    def _flush_if(self, f):
-        """where f (device bool): part += CRT(acc), acc = 0, one more flush.  part starts at zero, and
+    def _flush_if(self):
+        """where the chunk's flush predicate holds (device int32): part += CRT(acc) at the previous reference
+        exponents, acc = 0 (the flush count was advanced by sdpv_gram_columns).  part starts at zero, and
         0 + q is q itself (q is normalised), so the first flush gives the reference's part = q."""
-        fi = f.to(torch.int32)
-        q = self._crt(pred=fi)
+        fi = self._f
+        q = self._crt(pred=fi, rE=self._rE)
         if self.part is None:
             self.part = zeros((self.N, self.N), self.L)
         n = self.N * self.N
         _lib.call("sdpv_mpf_add_if", self.L, n, _lib.ptr(self.part.m), _lib.ptr(self.part.e), _lib.ptr(q.m),
                   _lib.ptr(q.e), 1, _lib.ptr(self.part.m), _lib.ptr(self.part.e), _lib.ptr(fi), _lib.stream())
-        self.acc.masked_fill_(f, 0)
-        self._nflush += fi
+        _lib.call("sdpv_zero_if", _lib.ptr(self.acc), self.acc.numel() * 2, _lib.ptr(fi), _lib.stream())
 
     def next_reference(self, margin=4):
         return torch.where(self.Tmax > EZ // 2, self.Tmax + margin, self.Tmax)
