@@ -42,7 +42,7 @@ struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
   int16_t stg[128][kStg];                   // epilogue staging of one output tile (coalesced global I/O)
   u64 full[kStages], empty[kStages], acc_full, tmem_empty;
-  u64 nacc_full[2], ntmem_empty[2];          // narrow items: two TMEM buffers
+  u64 nacc_full[2], ntmem_empty[2];          // narrow items: two TMEM buffers, one per epilogue group
   u32 tmem_slot;
   int abort;
   float tminv[kMaxG];                       // this launch's moduli, staged once per CTA
@@ -57,6 +57,17 @@ __device__ __forceinline__ bool epi_sync_or(bool pred) {
       "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, 1, 256, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
       : "=r"(r)
       : "r"((int)pred)
+      : "memory");
+  return r != 0;
+}
+
+// Named barrier 2 + grp over one group of four epilogue warps (narrow items), with the OR of pred.
+__device__ __forceinline__ bool grp_sync_or(int grp, bool pred) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, %2, 128, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((int)pred), "r"(2 + grp)
       : "memory");
   return r != 0;
 }
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(&S.tmem_empty, 8);                // one arrival per epilogue warp
     for (int u = 0; u < 2; u++) {
       mbar_init(&S.nacc_full[u], 1);
-      mbar_init(&S.ntmem_empty[u], 8);
+      mbar_init(&S.ntmem_empty[u], 4);            // one arrival per warp of the item's epilogue group
     }
     S.abort = 0;
     mbar_fence_init();
@@ -415,10 +426,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3, ch = (warp - 2) >> 2, ew = warp - 2;
     const bool vec = ((ldc & 7) == 0) && ((((uintptr_t)acc) & 15) == 0);
     u32 li = 0;
+    // narrow items: two epilogue groups of four warps (group ch takes this CTA's items li with li % 2 == ch, the
+    // TMEM buffer of the same parity), so two items are reduced at once; each warp covers its lane quarter and
+    // all TB columns, in two passes of TB / 2; the group's own named barrier (2 + ch) makes its decisions
+    // uniform
     for (i64 item = blockIdx.x; item < nitems && nmode; item += gridDim.x, li++) {
+      if ((int)(li & 1) != ch) continue;
       // narrow items: TMEM lane = big-side row r, columns = the TB small-side entries; nmode 1: C[r][j]
       // (A is the big side), nmode 2: C[j][r] (B is the big side; a warp's lanes are consecutive r, so each
-      // output row's stores coalesce).  Each thread takes half of the TB columns.
+      // output row's stores coalesce)
       const i64 t = item % tiles, bg = item / tiles;
       const int b = (int)(bg % nb), g = (int)(bg / nb);
       const int gg = g0 + gofs + g;
@@ -442,79 +458,82 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       int16_t* bp = nmode == 1 ? acc + (rowA + r) * ldc : acc + rowA * ldc + col0 + r;
       const i64 js = nmode == 1 ? 1 : ldc;
-      const int j0 = ch * half;
       const bool ok_me = mbar_wait(&S.nacc_full[buf], (li >> 1) & 1, err);
-      const bool fail = epi_sync_or(!ok_me);
+      const bool fail = grp_sync_or(ch, !ok_me);
       if (fail) break;
       tc_fence_after();
-      if (gtab && (q * 32 >= big || j0 >= small)) {       // no valid output in this warp's lanes / columns
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
-        continue;
-      }
-      u32 hh[32], hx[32], ll[32];
-      const u32 base = tmem + buf * 256 + ((u32)(q * 32) << 16) + j0;
-      if (half <= 16) {                                  // TB <= 32: a 16-column load suffices
-        tmem_ld16(base, *reinterpret_cast<u32(*)[16]>(hh));
-        tmem_ld16(base + TB, *reinterpret_cast<u32(*)[16]>(hx));
-        tmem_ld16(base + 2 * TB, *reinterpret_cast<u32(*)[16]>(ll));
-      } else {
-        tmem_ld32(base, hh);
-        tmem_ld32(base + TB, hx);
-        tmem_ld32(base + 2 * TB, ll);
-      }
-      tmem_ld_wait();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
-      if (gtab && nmode == 1 && half == 16 && fresh && u8ops && gtab[8 * t + 4] <= 64) {
-        // grouped items of 32 small-side rows and K <= 64 on unsigned digits: ll < K 127^2 < 2^20 and
-        // hx = hl + lh < 2 K 255 127 < 2^22, so (hh mod m) 2^14 + 128 hx + ll stays below 2^30 and needs one
-        // reduction after hh's; the thread's 16 results of its row leave as two 16-byte stores
-        u32 pk[8];
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-          const int a = (int)hh[u];
-          const int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-          const int v = ra * c14 + (int)hx[u] * 128 + (int)ll[u];
-          int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-          rr += (rr < 0) ? m : 0;
-          rr -= (rr >= m) ? m : 0;
-          if (u & 1)
-            pk[u >> 1] |= ((u32)rr & 0xffffu) << 16;
-          else
-            pk[u >> 1] = (u32)rr & 0xffffu;
-        }
-        if (r < big) {
-          if (j0 + 16 <= small && (ldc & 7) == 0 && (((uintptr_t)acc) & 15) == 0) {
-            uint4* dst = reinterpret_cast<uint4*>(bp + j0);
-            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-          } else {
-            for (int u = 0; u < 16; u++)
-              if (j0 + u < small) bp[j0 + u] = (int16_t)(pk[u >> 1] >> (16 * (u & 1)));
-          }
-        }
-        continue;
-      }
       // grouped items with K <= 64 on unsigned digits: hx < 2 K 255 127 < 2^22, so 128 hx needs no reduction
       // of its own (the sum below stays under 2^30 with an old residue < 2^15)
       const bool small_k = gtab && u8ops && gtab[8 * t + 4] <= 64;
+      const bool fast = gtab && nmode == 1 && half == 16 && fresh && small_k;
+      for (int pass = 0; pass < 2; pass++) {
+        const int j0 = pass * half;
+        const bool skip = gtab && (q * 32 >= big || j0 >= small);    // warp-uniform: no valid output here
+        u32 hh[32], hx[32], ll[32];
+        if (!skip) {
+          const u32 base = tmem + buf * 256 + ((u32)(q * 32) << 16) + j0;
+          if (half <= 16) {                              // TB <= 32: a 16-column load suffices
+            tmem_ld16(base, *reinterpret_cast<u32(*)[16]>(hh));
+            tmem_ld16(base + TB, *reinterpret_cast<u32(*)[16]>(hx));
+            tmem_ld16(base + 2 * TB, *reinterpret_cast<u32(*)[16]>(ll));
+          } else {
+            tmem_ld32(base, hh);
+            tmem_ld32(base + TB, hx);
+            tmem_ld32(base + 2 * TB, ll);
+          }
+          tmem_ld_wait();
+        }
+        if (pass == 1) {                                 // both passes' accumulators read: release the buffer
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&S.ntmem_empty[buf]);
+        }
+        if (skip) continue;
+        if (fast) {
+          // grouped items of 32 small-side rows and K <= 64 on unsigned digits: ll < K 127^2 < 2^20 and
+          // hx = hl + lh < 2 K 255 127 < 2^22, so (hh mod m) 2^14 + 128 hx + ll stays below 2^30 and needs one
+          // reduction after hh's; the thread's 16 results of this pass leave as two 16-byte stores
+          u32 pk[8];
 #pragma unroll
-      for (int u = 0; u < 32; u++) {
-        const int j = j0 + u;
-        if (u >= half) break;
-        int a = (int)hh[u], x = (int)hx[u];
-        int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-        int rx = small_k ? x : x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
-        const bool in = r < big && j < small;
-        const int o = (!fresh && in) ? (int)bp[j * js] : 0;                // old residue (rare: K chunks)
-        int v = ra * c14 + rx * 128 + (int)ll[u] + o;
-        int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-        rr += (rr < 0) ? m : 0;
-        rr -= (rr >= m) ? m : 0;
-        if (in) bp[j * js] = (int16_t)rr;
+          for (int u = 0; u < 16; u++) {
+            const int a = (int)hh[u];
+            const int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+            const int v = ra * c14 + (int)hx[u] * 128 + (int)ll[u];
+            int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+            rr += (rr < 0) ? m : 0;
+            rr -= (rr >= m) ? m : 0;
+            if (u & 1)
+              pk[u >> 1] |= ((u32)rr & 0xffffu) << 16;
+            else
+              pk[u >> 1] = (u32)rr & 0xffffu;
+          }
+          if (r < big) {
+            if (j0 + 16 <= small && (ldc & 7) == 0 && (((uintptr_t)acc) & 15) == 0) {
+              uint4* dst = reinterpret_cast<uint4*>(bp + j0);
+              dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+              dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            } else {
+              for (int u = 0; u < 16; u++)
+                if (j0 + u < small) bp[j0 + u] = (int16_t)(pk[u >> 1] >> (16 * (u & 1)));
+            }
+          }
+          continue;
+        }
+#pragma unroll
+        for (int u = 0; u < 32; u++) {
+          const int j = j0 + u;
+          if (u >= half) break;
+          int a = (int)hh[u], x = (int)hx[u];
+          int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
+          int rx = small_k ? x : x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
+          const bool in = r < big && j < small;
+          const int o = (!fresh && in) ? (int)bp[j * js] : 0;              // old residue (rare: K chunks)
+          int v = ra * c14 + rx * 128 + (int)ll[u] + o;
+          int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
+          rr += (rr < 0) ? m : 0;
+          rr -= (rr >= m) ? m : 0;
+          if (in) bp[j * js] = (int16_t)rr;
+        }
       }
     }
     for (i64 item = blockIdx.x; item < nitems && tailTB; item += gridDim.x, li++) {
