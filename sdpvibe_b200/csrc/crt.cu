@@ -97,17 +97,18 @@ __global__ void __launch_bounds__(kThreads)
     const i64 r = valid ? e / w : 0, jj = valid ? e - (e / w) * w : 0;
     const int16_t* ap = acc + r * N + j0 + jj;
     float ks = 0.f;
-    for (int g32 = 0; g32 < ktc * 128; g32 += 32) {
-      // issue all 32 loads of this group before using any (they are independent)
-      int av[32];
+    for (int gb = 0; gb < ktc * 128; gb += 64) {
+      // the 64 loads of this group of moduli issued before any is used (they are independent): the pre-pass
+      // is bound by memory latency, one per group
+      int av[64];
 #pragma unroll
-      for (int q = 0; q < 32; q++) av[q] = (valid && g32 + q < n) ? (int)__ldcs(ap + (i64)(g32 + q) * ldg) : 0;
+      for (int q = 0; q < 64; q++) av[q] = (valid && gb + q < n) ? (int)__ldcs(ap + (i64)(gb + q) * ldg) : 0;
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < 4; h++) {                              // 16 moduli per 16-byte digit chunk
         u32 ph[4], pl[4];
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-          const int g = g32 + 16 * h + q;
+          const int g = gb + 16 * h + q;
           int y = 0;
           if (valid && g < n) {
             const int m = TB.m[g];
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(kThreads)
           ph[q >> 2] |= (u32)(yh & 255) << (8 * (q & 3));
           pl[q >> 2] |= (u32)(yl & 255) << (8 * (q & 3));
         }
-        const int g16 = g32 + 16 * h;
+        const int g16 = gb + 16 * h;
         int kt = g16 >> 7, chunk = (g16 & 127) >> 4;
         *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
         *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
@@ -167,13 +168,14 @@ __global__ void __launch_bounds__(kThreads)
         for (int j = 0; j < 32; j += 4) {
           int t0 = ch * kDig + c32 + j;
           if (t0 >= E) break;
-          i64 v = carry;
+          // z = 128 Zh + Zl - k Md fits int32: |Zh| <= n 2^14 <= 320 2^14 < 2^23, |Zl| < 2^21, |k Md| < 2^15.
+          // The word's four digits are summed apart from the carry (a tree, independent of the previous
+          // word), so only one 64-bit add per word waits on the carry chain
+          i64 z4[4];
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            // z = 128 Zh + Zl - k Md fits int32: |Zh| <= n 2^14 <= 320 2^14 < 2^23, |Zl| < 2^21, |k Md| < 2^15
-            const int z = 128 * (int)zh[j + u] + (int)zl[j + u] - kq32 * TB.md[t0 + u];
-            v += (i64)z * (i64)(1 << (8 * u));                       // one 32 x 32 -> 64 multiply-add
-          }
+          for (int u = 0; u < 4; u++)
+            z4[u] = (i64)(128 * (int)zh[j + u] + (int)zl[j + u] - kq32 * TB.md[t0 + u]) * (i64)(1 << (8 * u));
+          const i64 v = carry + ((z4[0] + z4[1]) + (z4[2] + z4[3]));
           const u32 wv = (u32)v;
           if (MODE == 0) {
             if (valid) out[(i64)nw * B + e] = (int32_t)wv;
