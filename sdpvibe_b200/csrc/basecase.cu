@@ -222,18 +222,31 @@ __device__ void wmul_core(const u32* x, int tx, const u32* y, int ty, int t, int
       const int i0 = max(la, k - ty), i1 = act ? min(tx, k - lb) : i0 - 1;
       const int nt = (int)__reduce_max_sync(kFull, (unsigned)max(i1 - i0 + 1, 0));
       u32 d0 = 0, d1 = 0, d2 = 0, e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
+      // the next four terms' loads are issued before this four's multiply-adds (software pipelined)
+      u32 a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + u;
+        a[u] = i <= i1 ? x[i] : 0u;
+        b[u] = i <= i1 ? y[k - i] : 0u;
+      }
       for (int j = 0; j < nt; j += 4) {
-        u32 a[4], b[4];
+        u32 an[4], bn[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const int i = i0 + j + u;
-          a[u] = i <= i1 ? x[i] : 0u;
-          b[u] = i <= i1 ? y[k - i] : 0u;
+          const int i = i0 + j + 4 + u;
+          an[u] = i <= i1 ? x[i] : 0u;
+          bn[u] = i <= i1 ? y[k - i] : 0u;
         }
         mac96(c0, c1, c2, a[0], b[0]);
         mac96(d0, d1, d2, a[1], b[1]);
         mac96(e0, e1, e2, a[2], b[2]);
         mac96(f0, f1, f2, a[3], b[3]);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          a[u] = an[u];
+          b[u] = bn[u];
+        }
       }
       add96(d0, d1, d2, f0, f1, f2);
       add96(c0, c1, c2, e0, e1, e2);
@@ -639,7 +652,7 @@ __device__ __forceinline__ void warp_shr1(u32* x, int WL) {              // arit
 __host__ __device__ constexpr int pitch(int WL) { return WL | 1; }
 template <int NPL, bool GLOBAL>
 __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
-  return (size_t)((GLOBAL ? 0 : 528) + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 5 * 32 * NPL * 4 + 64;
+  return (size_t)((GLOBAL ? 0 : 528) + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 6 * 32 * NPL * 4 + 80;
 }
 template <int NPL, bool GLOBAL>
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
@@ -663,9 +676,12 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
   u32* colmag = GLOBAL ? sm : sm + 528 * WP;                     // |l_ik| of the current column
   WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(colmag + 32 * WP);
   u32* nw = reinterpret_cast<u32*>(ws + kWarpsS);
-  u32 *sd = nw, *sr = nw + NWD, *st1 = nw + 2 * NWD, *st2 = nw + 3 * NWD, *sone = nw + 4 * NWD;
-  uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 5 * NWD);
+  // |r| of pivots of alternate parity in rbuf[k & 1]: warp 0 runs pivot k + 1 while the other warps still scale
+  // column k by r_k
+  u32 *sd = nw, *st1 = nw + NWD, *st2 = nw + 2 * NWD, *sone = nw + 3 * NWD, *rbuf = nw + 4 * NWD;
+  uint8_t* colsign = reinterpret_cast<uint8_t*>(nw + 6 * NWD);
   uint8_t* coltop = colsign + 32;
+  int* rinfo = reinterpret_cast<int*>(coltop + 32);               // top and sign of |r| per parity
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
   for (int i = 0; i < BT && !GLOBAL; i++) {
@@ -674,41 +690,58 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
     for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[(w / WL) * WP + w % WL] = src[w];
   }
   __syncthreads();
-  // Pivot k (warp 0): r = d^-1/2 by the Newton schedule, l_kk = d r, r kept in sr and RINV.
+  // Pivot k (warp 0): r = d^-1/2 by the Newton schedule; |r| in rbuf[k & 1] (top, sign in rinfo), r in RINV.
+  // l_kk = d r is formed later by another warp (kkprod), off the chain of pivots.
   auto pivot = [&](int k) {
     u32* akk = ent(k, k);
-    for (int w = lane; w < WL; w += 32) sd[w] = akk[w];
-    for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
-    __syncwarp();
-    if (lane == 0) {
-      if ((sd[WL - 1] >> 31) || (top_word(sd, WL) == 0 && sd[0] == 0)) atomicOr(err, SDPV_ERRBIT_NOTSPD);
-      fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
-    }
-    __syncwarp();
+    u32* sr = rbuf + (k & 1) * NWD;
     u32 D[NPL];
-    reg_load<NPL>(sd, D, WL);
+    reg_load<NPL>(akk, D, WL);
+    reg_store<NPL>(sd, D, WL);
     const bool dneg = reg_word<NPL>(D, WL - 1) >> 31;
     bool dnz = false;
 #pragma unroll
     for (int c = 0; c < NPL; c++) dnz = dnz || __any_sync(kFull, D[c] != 0u);
+    if (lane == 0 && (dneg || !dnz)) atomicOr(err, SDPV_ERRBIT_NOTSPD);
     if (!dneg && dnz) {
       // d > 0: the same truncated products as below, with the operands kept as magnitudes in shared memory
       // (|r| in sr, d in sd, |1 - d r^2| in ws[0].xa) and the additions, sign changes and halvings done in
-      // registers; r stays positive in practice, its sign is carried all the same
+      // registers; r stays positive in practice, its sign is carried all the same.  The first r is
+      // fx_from_double(1 / sqrt(fx_to_double(d))), evaluated by every lane on d's top three words.
       const int td = warp_top<NPL>(D, WL);
+      const u32 x0 = reg_word<NPL>(D, td), x1 = reg_word<NPL>(D, max(td - 1, 0)), x2 = reg_word<NPL>(D, max(td - 2, 0));
+      double dv = (double)x0;
+      if (td >= 1) dv = dv * 4294967296.0 + (double)x1;
+      if (td >= 2) dv = dv * 4294967296.0 + (double)x2;
+      dv = ldexp(dv, 32 * max(td - 2, 0) - 32 * LF);
       u32 R[NPL], Rt[NPL], P[NPL], S[NPL], O[NPL];
-      reg_load<NPL>(sr, Rt, WL);                                  // r, two's complement
+      {
+        int e;
+        const double mf = frexp(1.0 / sqrt(dv), &e);
+        u64 mi = (u64)ldexp(mf, 53);
+        int pos = e - 53 + 32 * LF;
+        if (pos < 0) {
+          mi = (-pos < 64) ? (mi >> (-pos)) : 0ull;
+          pos = 0;
+        }
+        const int li = pos / 32, sh = pos % 32;
+        const u64 lo = mi << sh, hi = sh ? (mi >> (64 - sh)) : 0ull;
+#pragma unroll
+        for (int c = 0; c < NPL; c++) {
+          const int q = lane + 32 * c - li;
+          const u32 wv = q == 0 ? (u32)lo : q == 1 ? (u32)(lo >> 32) : q == 2 ? (u32)hi : q == 3 ? (u32)(hi >> 32) : 0u;
+          Rt[c] = (q >= 0 && lane + 32 * c < WL) ? wv : 0u;
+        }
+      }
 #pragma unroll
       for (int c = 0; c < NPL; c++) {
         O[c] = (lane + 32 * c == LF) ? 1u : 0u;                   // fixed-point 1
         R[c] = Rt[c];
       }
       u32 sR = reg_word<NPL>(Rt, WL - 1) >> 31;
-      if (sR) {
-        warp_negate<NPL>(R, WL);
-        reg_store<NPL>(sr, R, WL);
-        __syncwarp();
-      }
+      if (sR) warp_negate<NPL>(R, WL);
+      reg_store<NPL>(sr, R, WL);
+      __syncwarp();
       int tr = warp_top<NPL>(R, WL);
       for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
         int t = bits / 32 + 2;
@@ -738,14 +771,17 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
         __syncwarp();
         if (t == 0) break;
       }
-      wmul_core<NPL>(sd, td, sr, tr, 0, WL, LF, st1);             // l_kk = d * d^-1/2
-      reg_load<NPL>(st1, P, WL);
-      if (sR) warp_negate<NPL>(P, WL);
-      reg_store<NPL>(akk, P, WL);
-      reg_store<NPL>(sr, Rt, WL);                                  // r, two's complement, for the column
       reg_store<NPL>(RI + (size_t)k * WL, Rt, WL);
+      if (lane == 0) {
+        rinfo[k & 1] = tr;
+        rinfo[2 + (k & 1)] = (int)sR;
+      }
       __syncwarp();
     } else {
+      for (int w = lane; w < WL; w += 32) sone[w] = (w == LF) ? 1u : 0u;
+      __syncwarp();
+      if (lane == 0) fx_from_double(sr, 1.0 / sqrt(fx_to_double(sd, WL, LF)), WL, LF);
+      __syncwarp();
       for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
         int t = bits / 32 + 2;
         if (t >= WL) t = 0;
@@ -757,9 +793,45 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
         warp_addsub<NPL>(sr, sr, st2, false, WL);
         if (t == 0) break;
       }
-      wmul<NPL>(sd, sr, 0, WL, LF, ws[0], akk, nullptr, nullptr, nullptr);   // l_kk = d * d^-1/2
       for (int w = lane; w < WL; w += 32) RI[(size_t)k * WL + w] = sr[w];
+      int tr;
+      const int sg = load_mag<NPL>(sr, st2, WL, tr);              // |r|, then back into sr
+      __syncwarp();
+      for (int w = lane; w < WL; w += 32) sr[w] = st2[w];
+      if (lane == 0) {
+        rinfo[k & 1] = tr;
+        rinfo[2 + (k & 1)] = sg;
+      }
+      __syncwarp();
     }
+  };
+  // a (shared or global memory, may alias out) times r_k given as |r_k| in rbuf with its top and sign: the
+  // truncated product of wmul with the second operand's magnitude already formed
+  auto mul_r = [&](u32* a, int k, u32* out, u32* omag, uint8_t* osign, uint8_t* otop) {
+    WarpScratchT<NPL>& s = ws[warp];
+    int ta;
+    const int sa = load_mag<NPL>(a, s.xa, WL, ta);
+    __syncwarp();
+    wmul_core<NPL>(s.xa, ta, rbuf + (k & 1) * NWD, rinfo[k & 1], 0, WL, LF, s.acc);
+    u32 m[NPL];
+#pragma unroll
+    for (int c = 0; c < NPL; c++) m[c] = lane + 32 * c < WL ? s.acc[lane + 32 * c] : 0u;
+    const int sg = sa ^ rinfo[2 + (k & 1)];
+    if (omag) {
+#pragma unroll
+      for (int c = 0; c < NPL; c++)
+        if (lane + 32 * c < WL) omag[lane + 32 * c] = m[c];
+    }
+    if (otop) {
+      const int tp = warp_top<NPL>(m, WL);
+      if (lane == 0) *otop = (uint8_t)tp;
+    }
+    if (osign && lane == 0) *osign = (uint8_t)sg;
+    if (sg) warp_negate<NPL>(m, WL);
+#pragma unroll
+    for (int c = 0; c < NPL; c++)
+      if (lane + 32 * c < WL) out[lane + 32 * c] = m[c];
+    __syncwarp();
   };
   if (warp == 0) pivot(0);
   __syncthreads();
@@ -768,25 +840,30 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
   // the same truncated products as without look-ahead (their exact sum is order-free).
   for (int k = 0; k < BT; k++) {
     // l_ik = a_ik * r_k: warp 0 takes row k + 1 (its next pivot needs only that row) and goes on without
-    // waiting; warps 1.. take the other rows and wait for the whole column (barrier 1: warp 0 arrives)
+    // waiting; warps 1.. take the other rows and l_kk = d_k r_k (the last warp) and wait for the whole column
+    // (barrier 1: warp 0 arrives)
     if (warp == 0) {
       if (k + 1 < BT) {
         u32* aik = ent(k + 1, k);
-        wmul<NPL>(aik, sr, 0, WL, LF, ws[0], aik, colmag + (size_t)(k + 1) * WP, colsign + k + 1, coltop + k + 1);
+        mul_r(aik, k, aik, colmag + (size_t)(k + 1) * WP, colsign + k + 1, coltop + k + 1);
       }
       asm volatile("bar.arrive 1, %0;" ::"r"(kThreadsS) : "memory");
     } else {
+      if (warp == kWarpsS - 1) {
+        u32* akk = ent(k, k);
+        mul_r(akk, k, akk, nullptr, nullptr, nullptr);
+      }
       for (int i = k + 1 + warp; i < BT; i += kWarpsS - 1) {
         u32* aik = ent(i, k);
-        wmul<NPL>(aik, sr, 0, WL, LF, ws[warp], aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
+        mul_r(aik, k, aik, colmag + (size_t)i * WP, colsign + i, coltop + i);
       }
       asm volatile("bar.sync 1, %0;" ::"r"(kThreadsS) : "memory");
     }
     if (k == BT - 1) break;
     if (warp == 0) {
-      u32* dn = ent(k + 1, k + 1);                // a_{k+1,k+1} -= l_{k+1,k}^2
+      u32* dn = ent(k + 1, k + 1);                // a_{k+1,k+1} -= l_{k+1,k}^2 (a square of magnitudes)
       const u32* lk = colmag + (size_t)(k + 1) * WP;
-      wmul<NPL>(lk, lk, 0, WL, LF, ws[0], st1, nullptr, nullptr, nullptr);
+      wmul_core<NPL>(lk, coltop[k + 1], lk, coltop[k + 1], 0, WL, LF, st1);
       warp_addsub<NPL>(dn, dn, st1, true, WL);
       pivot(k + 1);
     } else {
