@@ -202,7 +202,9 @@ __device__ __forceinline__ int load_mag(const u32* src, u32* m, int WL, int& top
 // tops tx, ty): one product column per lane, columns kmin .. min(kmax + 2, LF + WL - 1), each a 96-bit exact
 // sum; the column sums are added with their 32- and 64-bit shifts and the carries resolved by chain_carry.
 // x, y: shared memory (read at words <= their tops); out: 32 NPL words of shared memory, overwritten.
-template <int NPL>
+// SQ: a square (y = x, ty = tx): each column sums the products x_i x_(k-i), i < k - i, doubles the sum and
+// adds the middle term x_(k/2)^2 (half the multiply-adds, the same exact column sums).
+template <int NPL, bool SQ = false>
 __device__ void wmul_core(const u32* x, int tx, const u32* y, int ty, int t, int WL, int LF, u32* out) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -219,7 +221,8 @@ __device__ void wmul_core(const u32* x, int tx, const u32* y, int ty, int t, int
     u32 c0 = 0, c1 = 0, c2 = 0;
     {
       const bool act = q < ncol && k <= kmax;
-      const int i0 = max(la, k - ty), i1 = act ? min(tx, k - lb) : i0 - 1;
+      const int i0 = max(la, k - ty), i1f = act ? min(tx, k - lb) : i0 - 1;
+      const int i1 = SQ ? min(i1f, (k - 1) >> 1) : i1f;          // SQ: the pairs i < k - i
       const int nt = (int)__reduce_max_sync(kFull, (unsigned)max(i1 - i0 + 1, 0));
       u32 d0 = 0, d1 = 0, d2 = 0, e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
       // the next four terms' loads are issued before this four's multiply-adds (software pipelined)
@@ -251,6 +254,13 @@ __device__ void wmul_core(const u32* x, int tx, const u32* y, int ty, int t, int
       add96(d0, d1, d2, f0, f1, f2);
       add96(c0, c1, c2, e0, e1, e2);
       add96(c0, c1, c2, d0, d1, d2);
+      if (SQ) {
+        c2 = (c2 << 1) | (c1 >> 31);
+        c1 = (c1 << 1) | (c0 >> 31);
+        c0 <<= 1;
+        const int mid = k >> 1;
+        if (!(k & 1) && i0 <= mid && mid <= i1f) mac96(c0, c1, c2, x[mid], x[mid]);
+      }
     }
     u32 c1u = __shfl_up_sync(kFull, c1, 1), c2u = __shfl_up_sync(kFull, c2, 2);
     if (lane == 0) c1u = p_c1;
@@ -656,7 +666,7 @@ __host__ __device__ constexpr size_t chol_smem_bytes(int WL) {
 }
 template <int NPL, bool GLOBAL>
 __host__ __device__ constexpr size_t trinv_smem_bytes(int WL) {
-  return (size_t)((GLOBAL ? 0 : 528) + 32) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 2 * 528 + 64;
+  return (size_t)((GLOBAL ? 0 : 528) + 96) * pitch(WL) * 4 + kWarpsS * sizeof(WarpScratchT<NPL>) + 2 * 528 + 128 + 64;
 }
 
 __device__ __forceinline__ int tri(int i, int j) { return i * (i + 1) / 2 + j; }
@@ -684,16 +694,35 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
   int* rinfo = reinterpret_cast<int*>(coltop + 32);               // top and sign of |r| per parity
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
-  for (int i = 0; i < BT && !GLOBAL; i++) {
-    const u32* src = G + (size_t)i * BT * WL;
-    u32* dst = ent(i, 0);
-    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[(w / WL) * WP + w % WL] = src[w];
-  }
-  __syncthreads();
+  // Row i of the triangle between the tile (global, entry pitch WL) and shared memory (pitch WP), by one warp:
+  // eight entries' loads issued before their stores
+  auto copy_row = [&](int i, bool in) {
+    u32* g = G + (size_t)i * BT * WL;
+    u32* t = ent(i, 0);
+    for (int j0 = 0; j0 <= i; j0 += 8) {
+      u32 v[8][NPL];
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+#pragma unroll
+        for (int c = 0; c < NPL; c++) {
+          const int j = j0 + u, w = lane + 32 * c;
+          v[u][c] = (j <= i && w < WL) ? (in ? g[(size_t)j * WL + w] : t[j * WP + w]) : 0u;
+        }
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+#pragma unroll
+        for (int c = 0; c < NPL; c++) {
+          const int j = j0 + u, w = lane + 32 * c;
+          if (j <= i && w < WL) {
+            if (in) t[j * WP + w] = v[u][c];
+            else g[(size_t)j * WL + w] = v[u][c];
+          }
+        }
+    }
+  };
   // Pivot k (warp 0): r = d^-1/2 by the Newton schedule; |r| in rbuf[k & 1] (top, sign in rinfo), r in RINV.
   // l_kk = d r is formed later by another warp (kkprod), off the chain of pivots.
-  auto pivot = [&](int k) {
-    u32* akk = ent(k, k);
+  auto pivot = [&](int k, const u32* akk) {                      // akk: where d = a_kk is read
     u32* sr = rbuf + (k & 1) * NWD;
     u32 D[NPL];
     reg_load<NPL>(akk, D, WL);
@@ -746,7 +775,7 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
       for (int bits = 100;; bits *= 2) {                           // r <- r + r (1 - d r^2) / 2
         int t = bits / 32 + 2;
         if (t >= WL) t = 0;
-        wmul_core<NPL>(sr, tr, sr, tr, t, WL, LF, st1);           // r^2
+        wmul_core<NPL, true>(sr, tr, sr, tr, t, WL, LF, st1);     // r^2
         reg_load<NPL>(st1, P, WL);
         const int tp = warp_top<NPL>(P, WL);
         wmul_core<NPL>(st1, tp, sd, td, t, WL, LF, st2);          // d r^2
@@ -833,7 +862,10 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
       if (lane + 32 * c < WL) out[lane + 32 * c] = m[c];
     __syncwarp();
   };
-  if (warp == 0) pivot(0);
+  // pivot 0 reads a_00 from the tile itself while warps 1.. copy the triangle into shared memory
+  if (warp == 0) pivot(0, GLOBAL ? ent(0, 0) : G);
+  else if (!GLOBAL)
+    for (int i = warp - 1; i < BT; i += kWarpsS - 1) copy_row(i, true);
   __syncthreads();
   // Step k: column k scaled by r_k; then, with one pivot of look-ahead, warp 0 updates a_{k+1,k+1} and runs
   // pivot k+1's Newton chain while warps 1.. apply the rest of step k's trailing update.  Every entry gets
@@ -863,9 +895,9 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
     if (warp == 0) {
       u32* dn = ent(k + 1, k + 1);                // a_{k+1,k+1} -= l_{k+1,k}^2 (a square of magnitudes)
       const u32* lk = colmag + (size_t)(k + 1) * WP;
-      wmul_core<NPL>(lk, coltop[k + 1], lk, coltop[k + 1], 0, WL, LF, st1);
+      wmul_core<NPL, true>(lk, coltop[k + 1], lk, coltop[k + 1], 0, WL, LF, st1);
       warp_addsub<NPL>(dn, dn, st1, true, WL);
-      pivot(k + 1);
+      pivot(k + 1, dn);
     } else {
       const int m = BT - k - 1, npairs = m * (m + 1) / 2;
       for (int p = 1 + tid - 32; p < npairs; p += kThreadsS - 32) {   // a_ij -= l_ik l_jk, k < j <= i, but (k+1, k+1)
@@ -886,11 +918,9 @@ __global__ void __launch_bounds__(kThreadsS) chol_tiles_k(u32* __restrict__ A, u
     }
     __syncthreads();
   }
-  for (int i = 0; i < BT && !GLOBAL; i++) {
-    u32* dst = G + (size_t)i * BT * WL;
-    const u32* src = ent(i, 0);
-    for (int w = tid; w < (i + 1) * WL; w += kThreadsS) dst[w] = src[(w / WL) * WP + w % WL];
-  }
+  // l_kk of the last pivot was written by the last warp after warp 0 had passed its final barrier
+  __syncthreads();
+  for (int i = warp; i < BT && !GLOBAL; i += kWarpsS) copy_row(BT - 1 - i, false);
 }
 
 // X = L^-1 right-looking: slot (i, k) of Xm first accumulates sum_j l_ij x_jk (two's complement, exact
@@ -905,61 +935,93 @@ __global__ void __launch_bounds__(kThreadsS) trinv_tiles_k(const u32* __restrict
   extern __shared__ __align__(16) u32 sm[];
   const int WP = pitch(WL);
   u32* Xm = GLOBAL ? S + (size_t)blockIdx.x * 528 * WP : sm;     // slots tri(i, k), lower triangle
-  u32* Lcol = GLOBAL ? sm : sm + 528 * WP;                       // |l_ij| of the current column j, by row i
-  WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(Lcol + 32 * WP);
+  // |l_ij| of column j by row i in Lcol + (j & 1) 32 WP (column j + 1 is read from the tile during step j's
+  // products and stored after them); the pivot reciprocals r_i in RIs
+  u32* Lcol = GLOBAL ? sm : sm + 528 * WP;
+  u32* RIs = Lcol + 64 * WP;
+  WarpScratchT<NPL>* ws = reinterpret_cast<WarpScratchT<NPL>*>(RIs + 32 * WP);
   uint8_t* xs = reinterpret_cast<uint8_t*>(ws + kWarpsS);             // signs, tops of finished x
   uint8_t* xt = xs + 528;
-  uint8_t* ls = xt + 528;                                        // signs, tops of the column of L
-  uint8_t* lt = ls + 32;
+  uint8_t* ls = xt + 528;                                        // signs, tops of the columns of L (2 x 32)
+  uint8_t* lt = ls + 64;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const u32* LG = Lt + (size_t)blockIdx.x * BT * BT * WL;
   const u32* RI = RINV + (size_t)blockIdx.x * BT * WL;
   u32* XG = X + (size_t)blockIdx.x * BT * BT * WL;
   for (int e = tid; e < 528 * WP; e += kThreadsS) Xm[e] = 0;
+  for (int i = warp; i < BT; i += kWarpsS)
+    for (int w = lane; w < WL; w += 32) RIs[i * WP + w] = RI[(size_t)i * WL + w];
   __syncthreads();
   for (int i = warp; i < BT; i += kWarpsS) {                     // x_ii = r_i
     int top;
-    const int sg = load_mag<NPL>(RI + (size_t)i * WL, Xm + (size_t)tri(i, i) * WP, WL, top);
+    const int sg = load_mag<NPL>(RIs + i * WP, Xm + (size_t)tri(i, i) * WP, WL, top);
     if (lane == 0) {
       xs[tri(i, i)] = (uint8_t)sg;
       xt[tri(i, i)] = (uint8_t)top;
     }
   }
-  for (int j = 0; j < BT - 1; j++) {
-    for (int i = j + 1 + warp; i < BT; i += kWarpsS) {
-      int top;
-      const int sg = load_mag<NPL>(LG + ((size_t)i * BT + j) * WL, Lcol + (size_t)i * WP, WL, top);
-      if (lane == 0) {
-        ls[i] = (uint8_t)sg;
-        lt[i] = (uint8_t)top;
-      }
+  for (int i = 1 + warp; i < BT; i += kWarpsS) {                 // column 0
+    int top;
+    const int sg = load_mag<NPL>(LG + (size_t)i * BT * WL, Lcol + (size_t)i * WP, WL, top);
+    if (lane == 0) {
+      ls[i] = (uint8_t)sg;
+      lt[i] = (uint8_t)top;
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  for (int j = 0; j < BT - 1; j++) {
+    const u32* Lc = Lcol + (j & 1) * 32 * WP;
+    const uint8_t *lsj = ls + (j & 1) * 32, *ltj = lt + (j & 1) * 32;
+    u32 pf[2][NPL];                                              // column j + 1, rows j + 2 + warp (+ 16)
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int i = j + 2 + warp + q * kWarpsS;
+#pragma unroll
+      for (int c = 0; c < NPL; c++)
+        pf[q][c] = (i < BT && lane + 32 * c < WL) ? LG[((size_t)i * BT + j + 1) * WL + lane + 32 * c] : 0u;
+    }
     const int nk = j + 1, np = (BT - 1 - j) * nk;
     for (int p = tid; p < np; p += kThreadsS) {                  // slot (i, k) += l_ij x_jk
       const int i = j + 1 + p / nk, k = p % nk;
       const int e = tri(j, k);
       u32* dst = Xm + (size_t)tri(i, k) * WP;
-      const u32 *xl = Lcol + (size_t)i * WP, *yx = Xm + (size_t)e * WP;
-      const bool add = ls[i] == xs[e];
-      if (LF == 26 && lt[i] <= 26 && xt[e] <= 30)
+      const u32 *xl = Lc + (size_t)i * WP, *yx = Xm + (size_t)e * WP;
+      const bool add = lsj[i] == xs[e];
+      if (LF == 26 && ltj[i] <= 26 && xt[e] <= 30)
         fx_rmw_reg2<26, 26, 30>(dst, xl, yx, add, WL);
-      else if (LF == 24 && lt[i] <= 24 && xt[e] <= 28)
+      else if (LF == 24 && ltj[i] <= 24 && xt[e] <= 28)
         fx_rmw_reg2<24, 24, 28>(dst, xl, yx, add, WL);
-      else if (LF == 26 && lt[i] <= 26)
+      else if (LF == 26 && ltj[i] <= 26)
         fx_rmw_lreg<26>(dst, xl, yx, xt[e], add, WL);
-      else if (LF == 24 && lt[i] <= 24)
+      else if (LF == 24 && ltj[i] <= 24)
         fx_rmw_lreg<24>(dst, xl, yx, xt[e], add, WL);
       else
-        fx_rmw(dst, xl, lt[i], yx, xt[e], add, WL, LF);
+        fx_rmw(dst, xl, ltj[i], yx, xt[e], add, WL, LF);
     }
     __syncthreads();
     for (int k = warp; k <= j; k += kWarpsS) {                   // x_{j+1,k} = -(sum) r_{j+1}
       const int ei = tri(j + 1, k);
-      wmul<NPL>(Xm + (size_t)ei * WP, RI + (size_t)(j + 1) * WL, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WP,
+      wmul<NPL>(Xm + (size_t)ei * WP, RIs + (j + 1) * WP, 0, WL, LF, ws[warp], nullptr, Xm + (size_t)ei * WP,
            xs + ei, xt + ei);
       if (lane == 0) xs[ei] ^= 1;                                // the negation
       __syncwarp();
+    }
+    {
+      u32* Ln = Lcol + ((j + 1) & 1) * 32 * WP;                  // column j + 1 as magnitudes
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int i = j + 2 + warp + q * kWarpsS;
+        if (i < BT) {
+          const int sg = (int)(reg_word<NPL>(pf[q], WL - 1) >> 31);
+          if (sg) warp_negate<NPL>(pf[q], WL);
+          const int top = warp_top<NPL>(pf[q], WL);
+          reg_store<NPL>(Ln + (size_t)i * WP, pf[q], WL);
+          if (lane == 0) {
+            ls[((j + 1) & 1) * 32 + i] = (uint8_t)sg;
+            lt[((j + 1) & 1) * 32 + i] = (uint8_t)top;
+          }
+        }
+      }
     }
     __syncthreads();
   }
