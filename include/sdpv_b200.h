@@ -55,6 +55,11 @@ const char* sdpv_last_error(void);
  * Replaces RNS.__init__ (sdpvibe/rns.py:166-191) and mpmat.ctx (sdpvibe/mpmat.py:163-166).
  * Tables live on the device that is current at creation. */
 int sdpv_ctx_create(int L, sdpv_ctx** out);
+/* The same with the moduli taken in groups of G (1, 2, 4, 8 or 16; sdpv_ctx_create is G = 16, the
+ * reference's): the least multiple of G primes that meets the bound.  Replaces the G argument of
+ * RNS.__init__ (sdpvibe/rns.py:163-173).  Every G gives the same exact products and CRT values; the
+ * autotuner picks it (SDPV_TUNE_MOD_GROUP) for the library's own contexts. */
+int sdpv_ctx_create_g(int L, int G, sdpv_ctx** out);
 int sdpv_ctx_destroy(sdpv_ctx* ctx);
 /* n moduli, E CRT bytes, W = E/4 words. */
 int sdpv_ctx_query(const sdpv_ctx* ctx, int* n, int* E, int* W);
@@ -91,13 +96,16 @@ int sdpv_mpf_add(int L, int64_t n, const int32_t* A, const int64_t* eA, const in
  * SDPV_TUNE_NARROW_MAX: residue-GEMM narrow items when one side has at most this many rows (0 = never,
  * else a multiple of 16 up to 64; default 64); SDPV_TUNE_PACK_MAX: small blocks packed several to a tile
  * when both sides have at most this many rows (0 = never, multiple of 16 up to 64; default 64);
- * SDPV_TUNE_RES_WARPS: reducer warps of the decomposition kernel (8 or 16; default 8).
+ * SDPV_TUNE_RES_WARPS: reducer warps of the decomposition kernel (8 or 16; default 8);
+ * SDPV_TUNE_MOD_GROUP: the moduli group G of the contexts the Python layer creates for its own products
+ * (1, 2, 4, 8 or 16; default 16; read there, see sdpv_ctx_create_g).
  * No reference counterpart (the reference's launch shapes are fixed). */
 #define SDPV_TUNE_CRT_CTAS 0
 #define SDPV_TUNE_NARROW_MAX 1
 #define SDPV_TUNE_PACK_MAX 2
 #define SDPV_TUNE_RES_WARPS 3
-#define SDPV_TUNE_COUNT 4
+#define SDPV_TUNE_MOD_GROUP 4
+#define SDPV_TUNE_COUNT 5
 int sdpv_tune_set(int knob, int value);
 int sdpv_tune_get(int knob, int* value);
 /* ---------------------------------------------------------------- binary SDP records (El::BigFloat over GMP limbs)

@@ -24,6 +24,7 @@ _SIGS = {
     "sdpv_version": [],
     "sdpv_last_error": [],
     "sdpv_ctx_create": [_I, ctypes.POINTER(_P)],
+    "sdpv_ctx_create_g": [_I, _I, ctypes.POINTER(_P)],
     "sdpv_ctx_destroy": [_P],
     "sdpv_ctx_query": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "sdpv_ctx_moduli": [_P, _P],
@@ -111,7 +112,7 @@ def _apply_tuning(h):
             return
     except (OSError, ValueError, RuntimeError):
         return
-    ids = {"crt_ctas": 0, "narrow_max": 1, "pack_max": 2}
+    ids = {"crt_ctas": 0, "narrow_max": 1, "pack_max": 2, "res_warps": 3, "moduli_group": 4}
     for name, value in table.get("knobs", {}).items():
         if name in ids:
             h.sdpv_tune_set(ids[name], int(value))

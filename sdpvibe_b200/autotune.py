@@ -14,9 +14,18 @@ Knobs and their shapes:
               the c2 buckets (106 x 32 x 32, K 32; 131 x 64 x 32, K 64; 98 x 16 x 16, K 16)
   res_warps   reducer warps of the decomposition kernel: the Gram chunk's residues (274 x 7000 entries,
               L + 1 = 27 limbs, unsigned digits) and the solver's (1000 x 1000, L = 26, API digits)
+  moduli_group  the prime split: the library's own contexts take the least multiple of G primes with
+              M > 4 kmax 2^(2(32 L - 1)) (sdpvibe/rns.py:166-173 with G = 16): at L = 26, 128 / 120 / 116 /
+              113 moduli for G = 16 / 8 / 4 / 1.  Every product is exact whatever the moduli, so the rounded
+              results are the same bits; the work of the decomposition, the residue GEMMs and the CRT
+              scales with the count.  Timed on an mp GEMM (512^3), a grouped Cholesky + solve of 60
+              uneven blocks and a Gram chunk (274 columns, 1750 rows); RNS(L) built by a caller keeps the
+              reference's G = 16 and its residue format.
 
-The prime set and the digit split of the residues are the reference's (they define the API's residue and
-CRT formats), so they are not tuned.
+The digit split of a residue (r = 128 hi + lo, two int8 digits) is fixed by the int8 operands of the tensor
+cores: every split into two digits below 256 has the same products and bounds.  The residue GEMM's 128 x 128
+tile, its 3-stage ring and its single-CTA MMA are fixed by shared memory (three 64 KB stages) and TMEM (384
+accumulator columns per tile); a two-CTA (cta_group::2) variant is not built.
 """
 import argparse
 import json
@@ -30,7 +39,7 @@ from . import _lib
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning_b200.json")
 KNOBS = {"crt_ctas": (0, [1, 2, 3, 4]), "narrow_max": (1, [0, 32, 48, 64]), "pack_max": (2, [0, 32, 64]),
-         "res_warps": (3, [8, 16])}
+         "res_warps": (3, [8, 16]), "moduli_group": (4, [16, 8, 4, 1])}
 
 
 def set_knob(name, value):
@@ -102,6 +111,30 @@ def _rows_case(L, nI, K):
     return lambda: R.residues_rows(Xr, nI, Rp, 0, K)
 
 
+def _mpgemm_case(L, n):
+    from . import mpf
+    A = mpf.from_float(np.random.default_rng(0).standard_normal((n, n)), L)
+    return lambda: mpf.gemm(A, A)
+
+
+def _cholsolve_case(L, nblocks):
+    from . import mpf
+    from .kernel_bench import cholsolve_inputs, cholsolve_buckets
+    pairs = [(A, B) for _, _, A, B in cholsolve_buckets(cholsolve_inputs(nblocks, 8, 160, 8), L)]
+    return lambda: mpf.chol_solve_many(pairs)
+
+
+def _gram_case(L, N, rows):
+    from . import mpf
+    V = mpf.from_float(np.random.default_rng(2).standard_normal((rows, N)), L)
+
+    def run():
+        acc = mpf.GramAcc(N, L)
+        acc.add(V)
+        return acc.result()
+    return run
+
+
 def tune(reps=5, L=26):
     from .mpmat import ctx
     R = ctx(L)
@@ -118,6 +151,7 @@ def tune(reps=5, L=26):
         "pack_max": [_gemm_case(R, 106, 32, 32, 32, rng), _gemm_case(R, 131, 64, 32, 64, rng),
                      _gemm_case(R, 98, 16, 16, 16, rng)],
         "res_warps": [_res_case(27, 274, 7000, True), _res_case(26, 1000, 1000, False), _rows_case(27, 274, 7000)],
+        "moduli_group": [_mpgemm_case(L, 512), _cholsolve_case(L, 60), _gram_case(L, 274, 1750)],
     }
     knobs, timings = {}, {}
     for name, (_, values) in KNOBS.items():

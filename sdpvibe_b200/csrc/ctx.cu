@@ -95,9 +95,12 @@ int upload(T** dst, const std::vector<T>& v) {
 
 }  // namespace
 
-extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) {
-  if (!out || L < 1 || L > 160) return SDPV_EINVAL;
-  const int G = 16;
+extern "C" int sdpv_ctx_create(int L, sdpv_ctx** out) { return sdpv_ctx_create_g(L, 16, out); }
+
+// G: the moduli count is the least multiple of G that meets the bound (the reference uses G = 16); any G
+// gives the same exact products, a smaller one fewer moduli
+extern "C" int sdpv_ctx_create_g(int L, int G, sdpv_ctx** out) {
+  if (!out || L < 1 || L > 160 || G < 1 || G > 16 || (G & (G - 1))) return SDPV_EINVAL;
   // moduli: rns.py:168-173; M > 4 * 2^17 * 2^(2(32L-1)) <=> bitlen(M) >= 64L + 18
   std::vector<int> mods;
   Big M;

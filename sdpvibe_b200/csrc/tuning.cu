@@ -7,10 +7,10 @@
 
 namespace {
 // defaults: CRT CTAs per SM, narrow-item limit of the short side, block-packing limit, decomposition
-// reducer warps
-std::atomic<int> g_knob[SDPV_TUNE_COUNT] = {{3}, {64}, {64}, {8}};
-constexpr int kLo[SDPV_TUNE_COUNT] = {1, 0, 0, 8};
-constexpr int kHi[SDPV_TUNE_COUNT] = {4, 64, 64, 16};
+// reducer warps, moduli group of the Python layer's contexts
+std::atomic<int> g_knob[SDPV_TUNE_COUNT] = {{3}, {64}, {64}, {8}, {16}};
+constexpr int kLo[SDPV_TUNE_COUNT] = {1, 0, 0, 8, 1};
+constexpr int kHi[SDPV_TUNE_COUNT] = {4, 64, 64, 16, 16};
 }  // namespace
 
 namespace sdpv {
@@ -21,6 +21,7 @@ extern "C" int sdpv_tune_set(int knob, int value) {
   if (knob < 0 || knob >= SDPV_TUNE_COUNT || value < kLo[knob] || value > kHi[knob]) return SDPV_EINVAL;
   if ((knob == SDPV_TUNE_NARROW_MAX || knob == SDPV_TUNE_PACK_MAX) && value % 16) return SDPV_EINVAL;
   if (knob == SDPV_TUNE_RES_WARPS && value % 8) return SDPV_EINVAL;
+  if (knob == SDPV_TUNE_MOD_GROUP && (value & (value - 1))) return SDPV_EINVAL;
   g_knob[knob].store(value, std::memory_order_relaxed);
   return SDPV_OK;
 }

@@ -59,6 +59,8 @@ def run(key, fn, inputs):
     replay is a fresh copy."""
     if not ENABLED or torch.cuda.is_current_stream_capturing():
         return fn(inputs)
+    from .mpmat import moduli_group
+    key = (key, moduli_group())                         # a graph holds the contexts it was recorded with
     e = _cache.get(key)
     if e is None:
         result = fn(inputs)                             # eager: also initialises lazy library state

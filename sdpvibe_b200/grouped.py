@@ -411,7 +411,7 @@ def _residue_products(R, g, ws, acc):
     groups within the residue budget), the big side its first RA rows, the small side the rest."""
     rows = g.RA + g.RB
     per_mod = 2 * g.kp * rows
-    GR = R.n if R.n * per_mod <= RES_BUDGET else max(R.G, (RES_BUDGET // per_mod) // R.G * R.G)
+    GR = R.n if R.n * per_mod <= RES_BUDGET else max(16, (RES_BUDGET // per_mod) // 16 * 16)
     small_off = g.RA * g.kp
     for g0 in range(0, R.n, GR):
         G = min(GR, R.n - g0)

@@ -5,8 +5,11 @@ uniform, else an int64 (cols,) tensor): value[i, j] = int(limbs[:, i, j]) * 2**e
 (sdpvibe/mpmat.py:1-8).  gemm_nt computes the exact product with the residue kernels of rns.py and
 rounds every entry once.
 """
+import ctypes
+
 import torch
 
+from . import _lib
 from .rns import RNS, dev
 from .limbops import shift_round, add_same, bitlen_words
 
@@ -175,10 +178,21 @@ def add(A, B, alpha=1, out_exp=None):
 _ctx = {}
 
 
+def moduli_group():
+    """the moduli group G of the library's own contexts (the autotuner's SDPV_TUNE_MOD_GROUP knob; 16, the
+    reference's, unless its table chose another)"""
+    v = ctypes.c_int(16)
+    _lib.check(_lib.lib().sdpv_tune_get(4, ctypes.byref(v)), "sdpv_tune_get")
+    return v.value
+
+
 def ctx(L):
-    key = (L, torch.cuda.current_device())
+    """the RNS context the library's products at L limbs use (sdpvibe/mpmat.py:163-166), one per limb count,
+    device and moduli group"""
+    G = moduli_group()
+    key = (L, torch.cuda.current_device(), G)
     if key not in _ctx:
-        _ctx[key] = RNS(L)
+        _ctx[key] = RNS(L, G=G)
     return _ctx[key]
 
 
@@ -189,7 +203,7 @@ def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False, kvalid=None):
     K = Av.shape[2] if kvalid is None else kvalid
     rows = Av.shape[1] + (0 if syrk else Bv.shape[1])
     per_mod = rows * min(K, KC_MAX) * 2
-    GR = R.n if R.n * per_mod <= RES_BUDGET else max(R.G, (RES_BUDGET // per_mod) // R.G * R.G)
+    GR = R.n if R.n * per_mod <= RES_BUDGET else max(16, (RES_BUDGET // per_mod) // 16 * 16)
     for k0 in range(0, K, KC_MAX):
         kk = min(KC_MAX, K - k0)
         for g0 in range(0, R.n, GR):

@@ -18,15 +18,16 @@ dev = "cuda"
 
 class RNS:
     """Moduli and device tables for products of L-limb integers with inner dimension <= 2^17
-    (sdpvibe/rns.py:163-191)."""
+    (sdpvibe/rns.py:163-191).  G: the moduli count is the least multiple of G primes that meets the bound
+    (the reference's G = 16 by default; 1, 2, 4 and 8 give fewer moduli and the same exact products)."""
 
     KPAD = 16
 
     def __init__(self, L, kmax=1 << 17, G=16):
-        if kmax != 1 << 17 or G != 16:
-            raise ValueError("libsdpv_b200 contexts use kmax = 2^17 and groups of 16 moduli")
+        if kmax != 1 << 17 or G not in (1, 2, 4, 8, 16):
+            raise ValueError("libsdpv_b200 contexts use kmax = 2^17 and groups of 1, 2, 4, 8 or 16 moduli")
         h = ctypes.c_void_p()
-        _lib.call("sdpv_ctx_create", int(L), ctypes.byref(h))
+        _lib.call("sdpv_ctx_create_g", int(L), int(G), ctypes.byref(h))
         self._h = h
         n, E, W = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _lib.call("sdpv_ctx_query", h, ctypes.byref(n), ctypes.byref(E), ctypes.byref(W))
