@@ -97,15 +97,15 @@ def _gemm_case(R, nb, M, N, K, rng):
 
 
 def _res_case(L, rows, K, unsigned):
-    from .mpmat import ctx
-    R = ctx(L)
+    from .mpmat import lib_ctx
+    R = lib_ctx(L)
     X = torch.randint(-(1 << 31), (1 << 31) - 1, (L, rows, K), dtype=torch.int32, device="cuda")
     return lambda: R.residues(X, 0, K, spread=True, unsigned=unsigned)
 
 
 def _rows_case(L, nI, K):
-    from .mpmat import ctx
-    R = ctx(L)
+    from .mpmat import lib_ctx
+    R = lib_ctx(L)
     Rp = -(-K // 128) * 128
     Xr = torch.randint(0, 256, (nI, Rp, 128 if L <= 31 else 256), dtype=torch.uint8, device="cuda")
     return lambda: R.residues_rows(Xr, nI, Rp, 0, K)
@@ -136,8 +136,8 @@ def _gram_case(L, N, rows):
 
 
 def tune(reps=5, L=26):
-    from .mpmat import ctx
-    R = ctx(L)
+    from .mpmat import lib_ctx
+    R = lib_ctx(L)
     rng = np.random.default_rng(0)
     m = torch.tensor(R.mods, dtype=torch.int64, device="cuda")[:, None, None]
     acc_s = (torch.randint(0, 1 << 30, (R.n, 2880, 1000), device="cuda") % m).to(torch.int16)

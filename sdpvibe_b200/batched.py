@@ -10,7 +10,7 @@ import torch
 
 from . import _lib
 from .rns import dev
-from .mpmat import ctx, headroom_bits, residue_product
+from .mpmat import lib_ctx, headroom_bits, residue_product
 from .limbops import shift_round, add_same, bitlen_words
 
 
@@ -84,7 +84,7 @@ def bgemm_nt(A, Bt, out_exp="col", kc=4096, bt_rowexp=None):
     nb2, N, K2 = Bt.shape
     assert nb == nb2 and K == K2
     L = A.L
-    R = ctx(L)
+    R = lib_ctx(L)
     eA = A.exp if isinstance(A.exp, int) else A.exp[:, 0]
     acc = (torch.empty if K else torch.zeros)((R.n, nb * M, N), dtype=torch.int16, device=dev)
     if K:
@@ -108,7 +108,7 @@ def bgemm_nt(A, Bt, out_exp="col", kc=4096, bt_rowexp=None):
 def _bcrt_round(acc, nb, M, N, e_in, out_exp, L):
     """batched.py:200-231: CRT of all nb*M x N entries, then one rounding to a fixed exponent, per
     (block, column) 'col', or per block 'mat' (one extra rounding)."""
-    R = ctx(L)
+    R = lib_ctx(L)
     rows = nb * M
     Wd, bl, _ = R.crt_block(acc, N, 0, N, rows)                   # entries (b*M + i)*N + j
     fixed = isinstance(e_in, int) and isinstance(out_exp, int)

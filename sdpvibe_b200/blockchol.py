@@ -20,7 +20,7 @@ issued is this module's own:
 import torch
 
 from .mpf import MPF, Chol, add, gemm, top_max, aligned, _row_exponents
-from .mpmat import ctx, KC_MAX
+from .mpmat import lib_ctx, KC_MAX
 
 
 def _block(Q, r0, r1, c0, c1):
@@ -47,7 +47,7 @@ class _PanelOperand:
     def __init__(self, A):
         L = A.L
         self.M, K = A.shape
-        self.R = R = ctx(L)
+        self.R = R = lib_ctx(L)
         self.L = L
         self.rexp = _row_exponents(top_max(A, over_rows=False), L)[0]          # (M,)
         Am = aligned(A, self.rexp[None], per_col=False, transpose=False).view(L, self.M, K)

@@ -34,7 +34,7 @@ import torch
 
 from . import _lib
 from .rns import dev
-from .mpmat import ctx
+from .mpmat import lib_ctx
 
 BT = 32
 LI = 24                         # extra words of the base tiles' wide fixed point (sdpvibe/batched.py:243)
@@ -426,7 +426,7 @@ def _residue_products(R, g, ws, acc):
 def _product_wave(g, arenas, L):
     """gather (both sides, one launch), residues (one launch), grouped GEMM, CRT -> (CRT words (W, Rout w),
     bit lengths)"""
-    R = ctx(L)
+    R = lib_ctx(L)
     arr, planes, n, _keep = _ptrs(arenas)
     ws = torch.empty((L, g.RA + g.RB, g.kp), dtype=torch.int32, device=dev)
     _lib.call("sdpv_grp_copy", arr, planes, n, _lib.ptr(ws), ws[0].numel(), L, _lib.ptr(g.desc), g.ndesc, _lib.stream())

@@ -171,7 +171,7 @@ def _cholsolve(a, rng):
 
 
 def main():
-    from .mpmat import ctx
+    from .mpmat import lib_ctx
     from . import mpf
 
     ap = argparse.ArgumentParser()
@@ -192,7 +192,7 @@ def main():
     a = ap.parse_args()
     dev = "cuda"
     rng = np.random.default_rng(0)
-    R = ctx(a.L)
+    R = lib_ctx(a.L)
     out = {"kernel": a.kernel, "L": a.L, "M": a.M, "N": a.N, "K": a.K, "n_mod": R.n}
     if a.kernel in ("residues", "gemm", "syrk"):
         X = torch.from_numpy(rng.integers(-(1 << 31), 1 << 31, size=(a.L, a.N, a.K), dtype=np.int64)

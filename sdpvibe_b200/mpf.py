@@ -16,7 +16,7 @@ import torch
 
 from . import _lib, graphs
 from .limbops import shift_round, bitlen_words
-from .mpmat import ctx, KC_MAX, RES_BUDGET
+from .mpmat import lib_ctx, KC_MAX, RES_BUDGET
 from .rns import dev
 
 EZ = -(1 << 40)                                      # exponent of zero (sdpvibe/mpf.py:21)
@@ -399,7 +399,7 @@ def gemm(A, B, transA=False, transB=False):
     Am = aligned(A, rA, per_col=transA, transpose=transA)          # (L, nb, M, K)
     cB = _row_exponents(top_max(B, over_rows=not transB), L)        # (nb, N)
     Bm = aligned(B, cB, per_col=not transB, transpose=not transB)  # (L, nb, N, K)
-    R = ctx(L)
+    R = lib_ctx(L)
     acc = (torch.empty if K else torch.zeros)((R.n, nb * M, N), dtype=torch.int16, device=dev)
     if K:
         from .mpmat import residue_product
@@ -429,7 +429,7 @@ class GramAcc:
 
     def __init__(self, N, L, E_ref=None):
         self.N, self.L = N, L
-        self.R = ctx(L + 1)
+        self.R = lib_ctx(L + 1)
         self.E = (E_ref.to(torch.int64).contiguous().clone() if E_ref is not None
                   else torch.full((N,), EZ, dtype=torch.int64, device=dev))
         self.Tmax = torch.full((N,), EZ, dtype=torch.int64, device=dev)

@@ -186,14 +186,23 @@ def moduli_group():
     return v.value
 
 
-def ctx(L):
-    """the RNS context the library's products at L limbs use (sdpvibe/mpmat.py:163-166), one per limb count,
-    device and moduli group"""
-    G = moduli_group()
+def _context(L, G):
     key = (L, torch.cuda.current_device(), G)
     if key not in _ctx:
         _ctx[key] = RNS(L, G=G)
     return _ctx[key]
+
+
+def ctx(L):
+    """the RNS context of L-limb products in the reference's format (groups of 16 moduli), one per limb count
+    and device (sdpvibe/mpmat.py:163-166)"""
+    return _context(L, 16)
+
+
+def lib_ctx(L):
+    """the context this library's own products use: the moduli group of the autotuner's table (the results
+    are the same bits for every group; only the residue format, internal to each product, differs)"""
+    return _context(L, moduli_group())
 
 
 def residue_product(R, Av, Bv, acc, nb=1, syrk=False, fresh=False, kvalid=None):
@@ -240,7 +249,7 @@ def gemm_nt(A, Bt, out_exp="col", kc=4096, colblock=None, bt_rowexp=None):
     N, K2 = Bt.shape
     assert K == K2
     L = A.L
-    R = ctx(L)
+    R = lib_ctx(L)
     eA = A.uniform_exp()
     e_in = (eA + bt_rowexp) if bt_rowexp is not None else eA + Bt.uniform_exp()
     acc = (torch.empty if K else torch.zeros)((R.n, M, N), dtype=torch.int16, device=dev)
@@ -265,7 +274,7 @@ def _same_product(R, X, acc):
 def _crt_round(acc, e_in, out_exp, L, colblock=None):
     """sdpvibe/mpmat.py:205-236: CRT, then one rounding to a fixed / per-column ('col') / common
     ('mat', one extra rounding) exponent."""
-    R = ctx(L)
+    R = lib_ctx(L)
     n, M, N = acc.shape
     if colblock is None:
         colblock = max(1, min(N, (1 << 24) // max(M, 1)))

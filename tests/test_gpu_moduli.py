@@ -40,7 +40,7 @@ def test_moduli_group_same_bits(L):
     try:
         for G in (16, 8, 4, 1):
             autotune.set_knob("moduli_group", G)
-            mods[G] = list(mpmat.ctx(L).mods)
+            mods[G] = list(mpmat.lib_ctx(L).mods)
             outs[G], fl[G] = _results(L)
     finally:
         autotune.set_knob("moduli_group", default)
@@ -51,7 +51,8 @@ def test_moduli_group_same_bits(L):
     for G in (8, 4, 1):
         for a, b in zip(outs[16], outs[G]):
             assert torch.equal(a, b)
-    assert list(RNS(L).mods) == want[16]              # the API's context keeps the reference's moduli
+    assert list(RNS(L).mods) == want[16]              # the API's contexts keep the reference's moduli
+    assert list(mpmat.ctx(L).mods) == want[16]
 
 
 def test_moduli_group_knob_range():
