@@ -33,6 +33,7 @@ namespace {
 constexpr int kStages = 3;
 constexpr u32 kSlice = 128 * 128;            // one operand slice: 128 rows x 128 bytes
 constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue warps
+constexpr int kThreadsN = 576;               // narrow items of at most 32 short-side rows: 16 epilogue warps
 constexpr int kCornerKB = 8;                // syrk corner: K blocks of [Thi; Tlo] (8 KB) per ring stage
 
 constexpr int kMaxG = 128;                  // moduli per launch (more are split over launches)
@@ -42,7 +43,7 @@ struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
   int16_t stg[128][kStg];                   // epilogue staging of one output tile (coalesced global I/O)
   u64 full[kStages], empty[kStages], acc_full, tmem_empty;
-  u64 nacc_full[2], ntmem_empty[2];          // narrow items: two TMEM buffers, one per epilogue group
+  u64 nacc_full[4], ntmem_empty[4];          // narrow items: a TMEM buffer per epilogue group (2 or 4)
   u32 tmem_slot;
   int abort;
   float tminv[kMaxG];                       // this launch's moduli, staged once per CTA
@@ -125,7 +126,10 @@ __device__ __forceinline__ void epi_compute(u32 tmem, int q, int ch, int lane, i
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+// NW epilogue warps: 8 (every mode) or 16 (narrow items with TB <= 32 only: four epilogue groups, four TMEM
+// buffers of 128 columns, so four items are reduced at once)
+template <int NW>
+__global__ void __launch_bounds__(64 + 32 * NW, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
@@ -138,6 +142,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   GemmSmem& S = *reinterpret_cast<GemmSmem*>((uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nk = (int)((KC + 127) / 128);
+  constexpr int NT = 64 + 32 * NW;
+  constexpr bool kNarrowOnly = NW == 16;
+  constexpr int NGRP = NW / 4;                  // narrow epilogue groups = narrow TMEM buffers
+  constexpr u32 kNBuf = kNarrowOnly ? 128 : 256; // TMEM columns per narrow buffer (3 TB <= 96 when TB <= 32)
 
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) {
@@ -146,7 +154,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     mbar_init(&S.acc_full, 1);
     mbar_init(&S.tmem_empty, 8);                // one arrival per epilogue warp
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < NGRP; u++) {
       mbar_init(&S.nacc_full[u], 1);
       mbar_init(&S.ntmem_empty[u], 4);            // one arrival per warp of the item's epilogue group
     }
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     tmem_alloc(&S.tmem_slot, 512);
     tmem_relinquish();
   }
-  for (int g = tid; g < G; g += kThreads) {              // moduli < 2^15
+  for (int g = tid; g < G; g += NT) {                    // moduli < 2^15
     S.tmod[g] = (int16_t)mods[g0 + gofs + g];
     S.tc14[g] = (int16_t)c14s[g0 + gofs + g];
     S.tminv[g] = minvs[g0 + gofs + g];
@@ -258,13 +266,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       const u32 idescT = u8ops ? idesc_u8(128, TB) : idesc_i8(128, TB);
       u32 kbg = 0, li = 0;
       for (i64 item = blockIdx.x; item < nitems && !*(volatile int*)&S.abort; item += gridDim.x, li++) {
-        const u32 buf = li & 1;
-        if (li >= 2 && !mbar_wait(&S.ntmem_empty[buf], ((li >> 1) - 1) & 1, err)) {
+        const u32 buf = li % NGRP;
+        if (li >= NGRP && !mbar_wait(&S.ntmem_empty[buf], ((li / NGRP) - 1) & 1, err)) {
           *(volatile int*)&S.abort = 1;
           break;
         }
         tc_fence_after();
-        const u32 tb = tmem + buf * 256;
+        const u32 tb = tmem + buf * kNBuf;
         bool ok = true;
         int nki = nk;
         i64 klen = KC;
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mma_commit(&S.nacc_full[buf]);
       }
-    } else if (lane == 0) {
+    } else if (lane == 0 && !kNarrowOnly) {
       // tail items: N = 2 TB over [Bhi; Blo] (hh | hl at column 0, (hl + lh) | ll at column TB)
       const int TB = tailTB ? tailTB : 128;
       const u32 idesc = u8ops ? idesc_u8(128, 2 * TB) : idesc_i8(128, 2 * TB);
@@ -431,7 +439,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // all TB columns, in two passes of TB / 2; the group's own named barrier (2 + ch) makes its decisions
     // uniform
     for (i64 item = blockIdx.x; item < nitems && nmode; item += gridDim.x, li++) {
-      if ((int)(li & 1) != ch) continue;
+      if ((int)(li % NGRP) != ch) continue;
       // narrow items: TMEM lane = big-side row r, columns = the TB small-side entries; nmode 1: C[r][j]
       // (A is the big side), nmode 2: C[j][r] (B is the big side; a warp's lanes are consecutive r, so each
       // output row's stores coalesce)
@@ -440,7 +448,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int gg = g0 + gofs + g;
       const int m = S.tmod[g], c14 = S.tc14[g];
       const float minv = S.tminv[g];
-      const u32 buf = li & 1;
+      const u32 buf = li % NGRP;
       const int TB = nTB, half = nTB >> 1;
       i64 r = t * 128 + q * 32 + lane;
       i64 big = nmode == 1 ? M : N, small = nmode == 1 ? N : M;
@@ -458,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       int16_t* bp = nmode == 1 ? acc + (rowA + r) * ldc : acc + rowA * ldc + col0 + r;
       const i64 js = nmode == 1 ? 1 : ldc;
-      const bool ok_me = mbar_wait(&S.nacc_full[buf], (li >> 1) & 1, err);
+      const bool ok_me = mbar_wait(&S.nacc_full[buf], (li / NGRP) & 1, err);
       const bool fail = grp_sync_or(ch, !ok_me);
       if (fail) break;
       tc_fence_after();
@@ -471,8 +479,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool skip = gtab && (q * 32 >= big || j0 >= small);    // warp-uniform: no valid output here
         u32 hh[32], hx[32], ll[32];
         if (!skip) {
-          const u32 base = tmem + buf * 256 + ((u32)(q * 32) << 16) + j0;
-          if (half <= 16) {                              // TB <= 32: a 16-column load suffices
+          const u32 base = tmem + buf * kNBuf + ((u32)(q * 32) << 16) + j0;
+          if (kNarrowOnly || half <= 16) {               // TB <= 32: a 16-column load suffices
             tmem_ld16(base, *reinterpret_cast<u32(*)[16]>(hh));
             tmem_ld16(base + TB, *reinterpret_cast<u32(*)[16]>(hx));
             tmem_ld16(base + 2 * TB, *reinterpret_cast<u32(*)[16]>(ll));
@@ -520,7 +528,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           continue;
         }
 #pragma unroll
-        for (int u = 0; u < 32; u++) {
+        for (int u = 0; u < (kNarrowOnly ? 16 : 32); u++) {
           const int j = j0 + u;
           if (u >= half) break;
           int a = (int)hh[u], x = (int)hx[u];
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && tailTB; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && !kNarrowOnly && tailTB; item += gridDim.x, li++) {
       // syrk tail: entry (A row i, tail row j) = Q[nfull + j][i], written transposed into the lower triangle;
       // a warp's lanes are consecutive i, so the accesses of one tail row coalesce
       const i64 t = item % tiles, bg = item / tiles;
@@ -579,7 +587,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (i < M && j < tail && nfull + j >= i) colp[(i64)j * ldc] = (int16_t)r;
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && pack > 1 && !nmode; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && !kNarrowOnly && pack > 1 && !nmode; item += gridDim.x, li++) {
       // packed small blocks: tile rows are the stacked rows of blocks t*pack .. t*pack + nbt - 1, tile
       // columns their stacked B rows; only the diagonal sub-blocks are outputs (staged, coalesced)
       const i64 t = item % tiles;
@@ -630,7 +638,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = lane; j < N; j += 32) dst[j] = S.stg[r][bi * N + j];
       }
     }
-    for (i64 item = blockIdx.x; item < nitems && pack <= 1 && !tailTB && !nmode; item += gridDim.x, li++) {
+    for (i64 item = blockIdx.x; item < nitems && !kNarrowOnly && pack <= 1 && !tailTB && !nmode; item += gridDim.x, li++) {
       const i64 t = item % tiles, bg = item / tiles;
       const int b = (int)(bg % nb), g = (int)(bg / nb);
       int tm, tn;
@@ -807,6 +815,18 @@ int side_stream(int dev, cudaStream_t* s, cudaEvent_t* fork_ev, cudaEvent_t* joi
   return SDPV_OK;
 }
 
+// Dynamic shared memory of both kernel instantiations, set once per process.
+int gemm_attr(size_t smem) {
+  static std::once_flag attr;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr, [&] {
+    attr_err = cudaFuncSetAttribute(rns_gemm_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaFuncSetAttribute(rns_gemm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+  return attr_err == cudaSuccess ? SDPV_OK : sdpv::set_cuda_error(attr_err);
+}
+
 }  // namespace
 
 extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t* Alo, const int8_t* Bhi,
@@ -862,13 +882,9 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
              !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride)) {
     return SDPV_EINVAL;
   }
-  size_t smem = sizeof(GemmSmem) + 1024;
-  static std::once_flag attr;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(attr, [&] {
-    attr_err = cudaFuncSetAttribute(rns_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  });
-  if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
+  const size_t smem = sizeof(GemmSmem) + 1024;
+  const int attr_st = gemm_attr(smem);
+  if (attr_st != SDPV_OK) return attr_st;
   int ntm = (int)((M + 127) / 128), ntn = (int)((N + 127) / 128);
   // syrk whose last row block has at most 32 rows: full lower tiles over the first nfull rows, the tail rows
   // against each full row block inside that row block's diagonal item (its operand slices are in shared
@@ -909,9 +925,17 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       const i64 nitems = ptiles * (pack > 1 ? 1 : nb) * Gl;
       if (nitems == 0) continue;
       const unsigned gx = (unsigned)(nitems < sms ? nitems : sms);  // one resident CTA per SM, items looped
-      rns_gemm_kernel<<<gx, kThreads, smem, part ? side_s : main_s>>>(
-          mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs, Gl, nb, M, N,
-          KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr, sdpv::device_error_word());
+      cudaStream_t ls = part ? side_s : main_s;
+      if (nmode && nTB <= 32)                          // 16 epilogue warps for the short narrow items
+        rns_gemm_kernel<16><<<gx, kThreadsN, smem, ls>>>(
+            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv,
+            c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr,
+            sdpv::device_error_word());
+      else
+        rns_gemm_kernel<8><<<gx, kThreads, smem, ls>>>(
+            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv,
+            c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr,
+            sdpv::device_error_word());
       const int st = sdpv::launch_status();
       if (st != SDPV_OK) return st;
     }
@@ -946,13 +970,9 @@ extern "C" int sdpv_rns_gemm_grouped(const sdpv_ctx* c, const uint8_t* bigHi, co
       !make_map(&mBh, smallHi, KP, small_rows, 1, G, small_stride, TB) ||
       !make_map(&mBl, smallLo, KP, small_rows, 1, G, small_stride, TB))
     return SDPV_EINVAL;
-  size_t smem = sizeof(GemmSmem) + 1024;
-  static std::once_flag attr;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(attr, [&] {
-    attr_err = cudaFuncSetAttribute(rns_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  });
-  if (attr_err != cudaSuccess) return sdpv::set_cuda_error(attr_err);
+  const size_t smem = sizeof(GemmSmem) + 1024;
+  const int attr_st = gemm_attr(smem);
+  if (attr_st != SDPV_OK) return attr_st;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -961,9 +981,14 @@ extern "C" int sdpv_rns_gemm_grouped(const sdpv_ctx* c, const uint8_t* bigHi, co
     const i64 n_all = nitems * Gl;
     const unsigned gx = (unsigned)(n_all < sms ? n_all : sms);
     // M = rows_out: the accumulator planes (one per modulus) hold rows_out rows of ldc entries
-    rns_gemm_kernel<<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-        mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0, gofs,
-        Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
+    if (TB <= 32)
+      rns_gemm_kernel<16><<<gx, kThreadsN, smem, sdpv::as_stream(stream)>>>(
+          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
+          gofs, Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
+    else
+      rns_gemm_kernel<8><<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
+          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
+          gofs, Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
     const int st = sdpv::launch_status();
     if (st != SDPV_OK) return st;
   }
