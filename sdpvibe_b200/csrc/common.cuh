@@ -231,6 +231,18 @@ __device__ __forceinline__ u64 sdesc_sw128(u32 smem_addr) {
   return d;
 }
 
+// The same for K-major rows of rb = 32, 64 or 128 bytes (32-, 64- or 128-byte swizzle; 8-row groups 8 rb
+// bytes apart).
+__device__ __forceinline__ u64 sdesc_sw(u32 smem_addr, int rb) {
+  u64 d = 0;
+  d |= (u64)((smem_addr & 0x3FFFF) >> 4);
+  d |= (u64)1 << 16;
+  d |= (u64)((8 * rb) >> 4) << 32;
+  d |= (u64)1 << 46;
+  d |= (u64)(rb == 32 ? 6 : rb == 64 ? 4 : 2) << 61;
+  return d;
+}
+
 // 32 lanes x 32 consecutive 32-bit columns (this warp's lane quarter) into registers.
 __device__ __forceinline__ void tmem_ld32(u32 taddr, u32 (&r)[32]) {
   asm volatile(

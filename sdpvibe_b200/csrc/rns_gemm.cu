@@ -36,13 +36,14 @@ constexpr int kThreads = 320;                // producer, MMA issuer, 8 epilogue
 constexpr int kThreadsN = 576;               // narrow items of at most 32 short-side rows: 16 epilogue warps
 constexpr int kCornerKB = 8;                // syrk corner: K blocks of [Thi; Tlo] (8 KB) per ring stage
 
+constexpr int kSlots = 16;                  // compact narrow slots in the ring's memory (short K), at most
 constexpr int kMaxG = 128;                  // moduli per launch (more are split over launches)
 constexpr int kStg = 130;                   // staging row pitch (int16): 65 words, conflict-free by row
 
 struct GemmSmem {
   uint8_t stage[kStages][4][kSlice];        // [ah, al, bh, bl], each 1024-aligned
   int16_t stg[128][kStg];                   // epilogue staging of one output tile (coalesced global I/O)
-  u64 full[kStages], empty[kStages], acc_full, tmem_empty;
+  u64 full[kSlots], empty[kSlots], acc_full, tmem_empty;
   u64 nacc_full[4], ntmem_empty[4];          // narrow items: a TMEM buffer per epilogue group (2 or 4)
   u32 tmem_slot;
   int abort;
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
     rns_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                     const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTl, int tailTB,
-                    int nfull, int ftail, int tfirst, int nmode, int nTB, int u8ops,
+                    int nfull, int ftail, int tfirst, int nmode, int nTB, int u8ops, int nrb,
                     int16_t* __restrict__ acc, i64 ldc, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
                     const int32_t* __restrict__ c14s, int g0, int gofs, int G, i64 nb, i64 M, i64 N, i64 KC, int mode, int ntn,
                     i64 tiles, i64 nitems, bool fresh, int pack, const int32_t* __restrict__ gtab,
@@ -146,9 +147,14 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
   constexpr bool kNarrowOnly = NW == 16;
   constexpr int NGRP = NW / 4;                  // narrow epilogue groups = narrow TMEM buffers
   constexpr u32 kNBuf = kNarrowOnly ? 128 : 256; // TMEM columns per narrow buffer (3 TB <= 96 when TB <= 32)
+  // compact narrow slots (16-warp narrow items whose K fits one row of nrb = 32 or 64 bytes): A hi, A lo and
+  // [B hi; B lo] of one item with nrb-byte swizzled rows, NS of them in the ring's memory, one item each
+  const bool compact = kNarrowOnly && nrb > 0;
+  const u32 SB = compact ? (u32)(((256 + 2 * nTB) * nrb + 1023) & ~1023) : 0u;
+  const u32 NS = compact ? min((u32)kSlots, (u32)(kStages * 4 * kSlice) / SB) : (u32)kStages;
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; s++) {
+    for (int s = 0; s < kSlots; s++) {
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], 1);
     }
@@ -226,6 +232,21 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
           }
           continue;
         }
+        if (compact) {                            // one slot: the item's whole K in one row of nrb bytes
+          const u32 s = kbg % NS;
+          if (kbg >= NS && !mbar_wait(&S.empty[s], ((kbg / NS) - 1) & 1, err)) {
+            *(volatile int*)&S.abort = 1;
+            break;
+          }
+          uint8_t* sl = &S.stage[0][0][0] + s * SB;
+          mbar_expect_tx(&S.full[s], (u32)((256 + 2 * nTB) * nrb));
+          tma_load_4d(sl, &mAh, &S.full[s], 0, m0, b, g);
+          tma_load_4d(sl + 128 * nrb, &mAl, &S.full[s], 0, m0, b, g);
+          tma_load_4d(sl + 256 * nrb, &mTh, &S.full[s], 0, n0, b, g);
+          tma_load_4d(sl + (256 + nTB) * nrb, &mTl, &S.full[s], 0, n0, b, g);
+          kbg++;
+          continue;
+        }
         for (int kb = 0; kb < nki; kb++, kbg++) {
           const u32 s = kbg % kStages;
           if (kbg >= kStages && !mbar_wait(&S.empty[s], ((kbg / kStages) - 1) & 1, err)) {
@@ -279,6 +300,32 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
         if (gtab) {
           klen = gtab[8 * (item % tiles) + 4];
           nki = (int)((klen + 127) / 128);
+        }
+        if (compact) {
+          const u32 s = kbg % NS;
+          if (!mbar_wait(&S.full[s], (kbg / NS) & 1, err)) {
+            *(volatile int*)&S.abort = 1;
+            break;
+          }
+          tc_fence_after();
+          const u32 sl = smem_u32(&S.stage[0][0][0]) + s * SB;
+          const u32 bh = sl + 256 * nrb;
+          const u64 dah = sdesc_sw(sl, nrb), dal = sdesc_sw(sl + 128 * nrb, nrb), dbh = sdesc_sw(bh, nrb);
+          for (int ks = 0; ks < (int)((klen + 31) / 32); ks++) {       // klen <= nrb: K steps of 32 bytes
+            const u64 bd = dbh + 2 * ks;
+            if (ks == 0) {
+              mma_i8(tb + 0, dah, bd, idesc, 0u);                                              // hh | hl
+              mma_i8(tb + 2 * TB, dal, sdesc_sw(bh + TB * nrb, nrb), idescT, 0u);              // ll
+              mma_i8(tb + TB, dal, bd, idescT, 1u);                                            // hl += lh
+            } else {
+              mma_i8(tb + 0, dah + 2 * ks, bd, idesc, 1u);
+              mma_i8(tb + TB, dal + 2 * ks, bd, idesc, 1u);
+            }
+          }
+          mma_commit(&S.empty[s]);
+          mma_commit(&S.nacc_full[buf]);
+          kbg++;
+          continue;
         }
         for (int kb = 0; kb < nki; kb++, kbg++) {
           const u32 s = kbg % kStages;
@@ -779,15 +826,20 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
 
 // 4-D int8 map over (K, rows, nb, G) with 128 x 128 boxes and 128-byte swizzle; gstride = bytes between
 // the planes of consecutive moduli (>= K*rows*nb).
-bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G, i64 gstride, int box_rows = 128) {
+// box_x: row bytes of the box (128, or 32 / 64 for compact narrow slots), swizzled by the same width
+bool make_map(CUtensorMap* map, const void* base, i64 K, i64 rows, i64 nb, i64 G, i64 gstride, int box_rows = 128,
+              int box_x = 128) {
   sdpv::EncodeTiledFn fn = sdpv::encode_tiled_fn();
   if (!fn) return false;
   cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nb, (cuuint64_t)G};
   cuuint64_t strides[3] = {(cuuint64_t)K, (cuuint64_t)(K * rows), (cuuint64_t)gstride};
-  cuuint32_t box[4] = {128, (cuuint32_t)box_rows, 1, 1};
+  cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_rows, 1, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUtensorMapSwizzle sw = box_x == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                : box_x == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_128B;
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -870,13 +922,15 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
   }
   CUtensorMap mAh, mAl, mBh, mBl;
   const i64 ra = pack > 1 ? M * nb : M, rb = pack > 1 ? N * nb : N, nbm = pack > 1 ? 1 : nb;
+  // 16-warp narrow items whose K fits a row of 32 or 64 bytes load into compact slots (many items in flight)
+  const int nrb = (nmode && nTB <= 32 && KC <= 64) ? (KC <= 32 ? 32 : 64) : 0, bx = nrb ? nrb : 128;
   if (nmode == 2) {                                    // big side B into the A slots, A as the TB rows
-    if (!make_map(&mAh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mAl, Blo, KC, rb, nbm, G, b_stride) ||
-        !make_map(&mBh, Ahi, KC, ra, nbm, G, a_stride, nTB) || !make_map(&mBl, Alo, KC, ra, nbm, G, a_stride, nTB))
+    if (!make_map(&mAh, Bhi, KC, rb, nbm, G, b_stride, 128, bx) || !make_map(&mAl, Blo, KC, rb, nbm, G, b_stride, 128, bx) ||
+        !make_map(&mBh, Ahi, KC, ra, nbm, G, a_stride, nTB, bx) || !make_map(&mBl, Alo, KC, ra, nbm, G, a_stride, nTB, bx))
       return SDPV_EINVAL;
   } else if (nmode == 1) {
-    if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
-        !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride, nTB) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride, nTB))
+    if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride, 128, bx) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride, 128, bx) ||
+        !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride, nTB, bx) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride, nTB, bx))
       return SDPV_EINVAL;
   } else if (!make_map(&mAh, Ahi, KC, ra, nbm, G, a_stride) || !make_map(&mAl, Alo, KC, ra, nbm, G, a_stride) ||
              !make_map(&mBh, Bhi, KC, rb, nbm, G, b_stride) || !make_map(&mBl, Blo, KC, rb, nbm, G, b_stride)) {
@@ -928,12 +982,12 @@ extern "C" int sdpv_rns_gemm(const sdpv_ctx* c, const int8_t* Ahi, const int8_t*
       cudaStream_t ls = part ? side_s : main_s;
       if (nmode && nTB <= 32)                          // 16 epilogue warps for the short narrow items
         rns_gemm_kernel<16><<<gx, kThreadsN, smem, ls>>>(
-            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv,
+            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, nrb, acc, ldc, c->d.mods, c->d.minv,
             c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr,
             sdpv::device_error_word());
       else
         rns_gemm_kernel<8><<<gx, kThreads, smem, ls>>>(
-            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, acc, ldc, c->d.mods, c->d.minv,
+            mAh, mAl, mBh, mBl, mTh, mTl, tb, nfull, ftail, tfirst, nmode, nTB, u8ops, 0, acc, ldc, c->d.mods, c->d.minv,
             c->d.c14, g0, gofs, Gl, nb, M, N, KC, mode, ntn, ptiles, nitems, fresh, pack, nullptr,
             sdpv::device_error_word());
       const int st = sdpv::launch_status();
@@ -966,9 +1020,11 @@ extern "C" int sdpv_rns_gemm_grouped(const sdpv_ctx* c, const uint8_t* bigHi, co
       (((uintptr_t)bigHi | (uintptr_t)bigLo | (uintptr_t)smallHi | (uintptr_t)smallLo) & 15))
     return SDPV_EINVAL;
   CUtensorMap mAh, mAl, mBh, mBl;
-  if (!make_map(&mAh, bigHi, KP, big_rows, 1, G, big_stride) || !make_map(&mAl, bigLo, KP, big_rows, 1, G, big_stride) ||
-      !make_map(&mBh, smallHi, KP, small_rows, 1, G, small_stride, TB) ||
-      !make_map(&mBl, smallLo, KP, small_rows, 1, G, small_stride, TB))
+  const int nrb = (TB <= 32 && KP <= 64) ? (KP <= 32 ? 32 : 64) : 0, bx = nrb ? nrb : 128;   // compact slots
+  if (!make_map(&mAh, bigHi, KP, big_rows, 1, G, big_stride, 128, bx) ||
+      !make_map(&mAl, bigLo, KP, big_rows, 1, G, big_stride, 128, bx) ||
+      !make_map(&mBh, smallHi, KP, small_rows, 1, G, small_stride, TB, bx) ||
+      !make_map(&mBl, smallLo, KP, small_rows, 1, G, small_stride, TB, bx))
     return SDPV_EINVAL;
   const size_t smem = sizeof(GemmSmem) + 1024;
   const int attr_st = gemm_attr(smem);
@@ -983,11 +1039,11 @@ extern "C" int sdpv_rns_gemm_grouped(const sdpv_ctx* c, const uint8_t* bigHi, co
     // M = rows_out: the accumulator planes (one per modulus) hold rows_out rows of ldc entries
     if (TB <= 32)
       rns_gemm_kernel<16><<<gx, kThreadsN, smem, sdpv::as_stream(stream)>>>(
-          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
+          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, nrb, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
           gofs, Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
     else
       rns_gemm_kernel<8><<<gx, kThreads, smem, sdpv::as_stream(stream)>>>(
-          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
+          mAh, mAl, mBh, mBl, mBh, mBl, 0, 0, 0, 0, out_mode, TB, 1, 0, acc, ldc, c->d.mods, c->d.minv, c->d.c14, g0,
           gofs, Gl, 1, rows_out, TB, KP, 0, 1, nitems, n_all, true, 1, items, sdpv::device_error_word());
     const int st = sdpv::launch_status();
     if (st != SDPV_OK) return st;
