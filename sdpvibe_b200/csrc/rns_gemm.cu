@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
       tc_fence_after();
       // grouped items with K <= 64 on unsigned digits: hx < 2 K 255 127 < 2^22, so 128 hx needs no reduction
       // of its own (the sum below stays under 2^30 with an old residue < 2^15)
-      const bool small_k = gtab && u8ops && gtab[8 * t + 4] <= 64;
+      const bool small_k = u8ops && (gtab ? gtab[8 * t + 4] <= 64 : KC <= 64);
       const bool fast = gtab && nmode == 1 && half == 16 && fresh && small_k;
       for (int pass = 0; pass < 2; pass++) {
         const int j0 = pass * half;
@@ -574,20 +574,23 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
           }
           continue;
         }
+        // this pass's outputs of this thread: u < nval (the row test and the column bound taken once)
+        const int nval = r < big ? (int)(small - j0 < half ? (small - j0 > 0 ? small - j0 : 0) : half) : 0;
+        int16_t* const pj = bp + (i64)j0 * js;
 #pragma unroll
         for (int u = 0; u < (kNarrowOnly ? 16 : 32); u++) {
-          const int j = j0 + u;
           if (u >= half) break;
           int a = (int)hh[u], x = (int)hx[u];
           int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
           int rx = small_k ? x : x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
-          const bool in = r < big && j < small;
-          const int o = (!fresh && in) ? (int)bp[j * js] : 0;              // old residue (rare: K chunks)
+          const bool in = u < nval;
+          const int o = (!fresh && in) ? (int)pj[u * js] : 0;               // old residue (rare: K chunks)
           int v = ra * c14 + rx * 128 + (int)ll[u] + o;
+          // q = v / m rounded to nearest within 1/64 (|v| < 2^31, float rounding of v and of 1/m), so v - q m
+          // lies in (-0.52 m, 0.52 m) and one correction gives the canonical residue
           int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
           rr += (rr < 0) ? m : 0;
-          rr -= (rr >= m) ? m : 0;
-          if (in) bp[j * js] = (int16_t)rr;
+          if (in) pj[u * js] = (int16_t)rr;
         }
       }
     }
