@@ -555,8 +555,7 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
             const int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
             const int v = ra * c14 + (int)hx[u] * 128 + (int)ll[u];
             int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-            rr += (rr < 0) ? m : 0;
-            rr -= (rr >= m) ? m : 0;
+            rr += (rr < 0) ? m : 0;                      // the rounded quotient: one correction (see below)
             if (u & 1)
               pk[u >> 1] |= ((u32)rr & 0xffffu) << 16;
             else
