@@ -575,21 +575,35 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
         }
         // this pass's outputs of this thread: u < nval (the row test and the column bound taken once)
         const int nval = r < big ? (int)(small - j0 < half ? (small - j0 > 0 ? small - j0 : 0) : half) : 0;
-        int16_t* const pj = bp + (i64)j0 * js;
+        // x - (round(x / m) as the float magic number's bits - 0x4B400000) m, with 0x4B400000 m folded into one
+        // constant (arithmetic mod 2^32; the true value is below m in magnitude)
+        const u32 mu = (u32)m, k0 = 0x4B400000u * mu;
+        auto red = [&](int x) -> int {
+          return (int)((u32)x + k0 - (u32)__float_as_int(fmaf((float)x, minv, 12582912.0f)) * mu);
+        };
+        // v - q m with q = v / m rounded to nearest within 1/64 (|v| < 2^31, float rounding of v and of 1/m)
+        // lies in (-0.52 m, 0.52 m): one correction gives the canonical residue
+        int16_t* q = bp + (i64)j0 * js;
+        if (fresh) {
 #pragma unroll
-        for (int u = 0; u < (kNarrowOnly ? 16 : 32); u++) {
-          if (u >= half) break;
-          int a = (int)hh[u], x = (int)hx[u];
-          int ra = a - (__float_as_int(fmaf((float)a, minv, 12582912.0f)) - 0x4B400000) * m;
-          int rx = small_k ? x : x - (__float_as_int(fmaf((float)x, minv, 12582912.0f)) - 0x4B400000) * m;
-          const bool in = u < nval;
-          const int o = (!fresh && in) ? (int)pj[u * js] : 0;               // old residue (rare: K chunks)
-          int v = ra * c14 + rx * 128 + (int)ll[u] + o;
-          // q = v / m rounded to nearest within 1/64 (|v| < 2^31, float rounding of v and of 1/m), so v - q m
-          // lies in (-0.52 m, 0.52 m) and one correction gives the canonical residue
-          int rr = v - (__float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000) * m;
-          rr += (rr < 0) ? m : 0;
-          if (in) pj[u * js] = (int16_t)rr;
+          for (int u = 0; u < (kNarrowOnly ? 16 : 32); u++, q += js) {
+            if (u >= half) break;
+            const int rx = small_k ? (int)hx[u] : red((int)hx[u]);
+            int rr = red(red((int)hh[u]) * c14 + rx * 128 + (int)ll[u]);
+            rr += (rr < 0) ? m : 0;
+            if (u < nval) *q = (int16_t)rr;
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < (kNarrowOnly ? 16 : 32); u++, q += js) {
+            if (u >= half) break;
+            const bool in = u < nval;
+            const int o = in ? (int)*q : 0;                         // old residue (K chunks)
+            const int rx = small_k ? (int)hx[u] : red((int)hx[u]);
+            int rr = red(red((int)hh[u]) * c14 + rx * 128 + (int)ll[u] + o);
+            rr += (rr < 0) ? m : 0;
+            if (in) *q = (int16_t)rr;
+          }
         }
       }
     }
