@@ -19,12 +19,12 @@
 namespace {
 using namespace sdpv;
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 128;              // per 128-entry tile (TPC tiles per CTA: 128 TPC threads)
 constexpr int kDig = 64;                    // digits per MMA chunk (N)
 constexpr u32 kSlice = 128 * 128;
 
 struct CrtSmemHead {
-  u64 bar_ct, bar_mma;
+  u64 bar_ct, bar_mma[2];
   u32 tmem_slot;
   int abort;
 };
@@ -37,9 +37,11 @@ struct CrtTables {
   int md[kEmax];
 };
 
-// Dynamic shared memory: [head (1 KB)] [Yh: ktc slices] [Yl: ktc slices] [Ct: Epad/128 * ktc slices]
-template <int MODE>
-__global__ void __launch_bounds__(kThreads)
+// Dynamic shared memory: [head (8 KB)] per tile [Yh: ktc slices] [Yl: ktc slices], then [Ct: Epad/128 * ktc
+// slices].  TPC tiles per CTA (1 or 2): with 2 the digit table Ct is staged once for two tiles, so two CTAs of
+// 2 x 128 entries fit an SM where three of 128 did (the tables, not the tiles, fill shared memory).
+template <int MODE, int TPC>
+__global__ void __launch_bounds__(kThreads * TPC)
     crt_kernel(const int16_t* __restrict__ acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rows_per_block,
                const int64_t* __restrict__ rowexp, const int64_t* __restrict__ colexp, int L, int n, int E, int W,
                int ktc, int Epad, const int32_t* __restrict__ mods, const float* __restrict__ minvs,
@@ -51,32 +53,32 @@ __global__ void __launch_bounds__(kThreads)
   uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   CrtSmemHead& H = *reinterpret_cast<CrtSmemHead*>(base);
   CrtTables& TB = *reinterpret_cast<CrtTables*>(base + 64);
-  uint8_t* Yh = base + 8192;
+  const int tid = threadIdx.x, warp = tid >> 5, half = tid >> 7, lt = tid & 127;   // tile of the CTA, entry
+  uint8_t* Yh = base + 8192 + (size_t)half * 2 * ktc * kSlice;
   uint8_t* Yl = Yh + (size_t)ktc * kSlice;
-  uint8_t* Ct = Yl + (size_t)ktc * kSlice;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  uint8_t* Ct = base + 8192 + (size_t)TPC * 2 * ktc * kSlice;
   const i64 B = rows * w;
   const i64 ntiles = (B + 127) / 128;
 
   if (tid == 0) {
     mbar_init(&H.bar_ct, 1);
-    mbar_init(&H.bar_mma, 1);
+    for (int h = 0; h < TPC; h++) mbar_init(&H.bar_mma[h], 1);
     H.abort = 0;
     mbar_fence_init();
   }
   if (warp == 0) {
-    tmem_alloc(&H.tmem_slot, 2 * kDig);
+    tmem_alloc(&H.tmem_slot, 2 * kDig * TPC);
     tmem_relinquish();
   }
-  for (int g = tid; g < kNmax; g += kThreads) {
+  for (int g = tid; g < kNmax; g += kThreads * TPC) {
     TB.m[g] = g < n ? mods[g] : 1;
     TB.inv[g] = g < n ? invs[g] : 0;
     TB.minv[g] = g < n ? minvs[g] : 1.f;
   }
-  for (int t = tid; t < kEmax; t += kThreads) TB.md[t] = t < E ? md[t] : 0;
+  for (int t = tid; t < kEmax; t += kThreads * TPC) TB.md[t] = t < E ? md[t] : 0;
   __syncthreads();
   tc_fence_after();
-  const u32 tmem = H.tmem_slot;
+  const u32 tmem = H.tmem_slot + (u32)half * 2 * kDig;              // this tile's Zh, Zl columns
   if (tid == 0) {
     u32 bytes = (u32)(Epad / 128) * ktc * kSlice;
     mbar_expect_tx(&H.bar_ct, bytes);
@@ -90,9 +92,10 @@ __global__ void __launch_bounds__(kThreads)
   u32 phase = 0;
   u32 words[160];
 
-  for (i64 tile = blockIdx.x; tile < ntiles && !H.abort; tile += gridDim.x) {
+  for (i64 tile2 = blockIdx.x; tile2 * TPC < ntiles && !H.abort; tile2 += gridDim.x) {
     // ---- pre-pass: y_i, its int8 digits, k
-    const i64 e = tile * 128 + tid;
+    const i64 tile = tile2 * TPC + half;
+    const i64 e = tile * 128 + lt;
     const bool valid = e < B;
     const i64 r = valid ? e / w : 0, jj = valid ? e - (e / w) * w : 0;
     const int16_t* ap = acc + r * N + j0 + jj;
@@ -128,8 +131,8 @@ __global__ void __launch_bounds__(kThreads)
         }
         const int g16 = gb + 16 * h;
         int kt = g16 >> 7, chunk = (g16 & 127) >> 4;
-        *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-        *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(tid, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        *reinterpret_cast<uint4*>(Yh + kt * kSlice + sw128_off(lt, chunk)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+        *reinterpret_cast<uint4*>(Yl + kt * kSlice + sw128_off(lt, chunk)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
       }
     }
     const i64 kq = (i64)__float2int_rd(ks + 0.5f);
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(kThreads)
     int hz = -1, ho = -1;                              // highest word != 0, != 0xffffffff
     u32 hzv = 0, hov = 0, wtop = 0;
     for (int ch = 0; ch < nchunk; ch++) {
-      if (tid == 0) {
+      if (lt == 0) {                                   // one issuing thread per tile
         tc_fence_after();
         const u32 ctc = smem_u32(Ct) + (u32)((ch * kDig) / 128) * ktc * kSlice + (u32)((ch * kDig) % 128) * 128;
         for (int s = 0; s < ksteps; s++) {
@@ -153,16 +156,16 @@ __global__ void __launch_bounds__(kThreads)
           mma_i8(tmem + 0, sdesc_sw128(smem_u32(Yh) + kt * kSlice + ko), bd, idesc, s ? 1u : 0u);
           mma_i8(tmem + kDig, sdesc_sw128(smem_u32(Yl) + kt * kSlice + ko), bd, idesc, s ? 1u : 0u);
         }
-        mma_commit(&H.bar_mma);
+        mma_commit(&H.bar_mma[half]);
       }
-      if (!mbar_wait(&H.bar_mma, phase, err)) H.abort = 1;
+      if (!mbar_wait(&H.bar_mma[half], phase, err)) H.abort = 1;
       phase ^= 1;
       tc_fence_after();
 #pragma unroll 1
       for (int c32 = 0; c32 < kDig; c32 += 32) {
         u32 zh[32], zl[32];
-        tmem_ld32(tmem + ((u32)(warp * 32) << 16) + c32, zh);
-        tmem_ld32(tmem + ((u32)(warp * 32) << 16) + kDig + c32, zl);
+        tmem_ld32(tmem + ((u32)((warp & 3) * 32) << 16) + c32, zh);
+        tmem_ld32(tmem + ((u32)((warp & 3) * 32) << 16) + kDig + c32, zl);
         tmem_ld_wait();
 #pragma unroll
         for (int j = 0; j < 32; j += 4) {
@@ -220,7 +223,38 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 2 * kDig);
+  if (warp == 0) tmem_dealloc(H.tmem_slot, 2 * kDig * TPC);
+}
+
+template <int MODE, int TPC>
+int launch_crt_t(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i64 w, i64 rows, i64 rpb,
+                 const int64_t* rowexp, const int64_t* colexp, int L, int32_t* out, int64_t* out2, cudaStream_t st,
+                 const int32_t* pred, size_t smem) {
+  const CtxDev& d = c->d;
+  static bool attr_set[64] = {};
+  static size_t attr_val[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63] || attr_val[dev & 63] < smem) {
+    cudaError_t e = cudaFuncSetAttribute(crt_kernel<MODE, TPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    attr_set[dev & 63] = true;
+    attr_val[dev & 63] = smem;
+  }
+  i64 B = rows * w;
+  i64 ntiles = (B + 127) / 128, nunits = (ntiles + TPC - 1) / TPC;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // CTAs per SM: the tuned count for one-tile CTAs; two-tile CTAs as many as shared memory holds (at most 2)
+  i64 per_sm = TPC == 1 ? (i64)sdpv::tune(SDPV_TUNE_CRT_CTAS) : (i64)((228 * 1024) / (smem + 1024));
+  if (per_sm < 1) per_sm = 1;
+  if (TPC == 2 && per_sm > 2) per_sm = 2;
+  i64 gx = per_sm * sms;
+  if (gx > nunits) gx = nunits;
+  crt_kernel<MODE, TPC><<<(unsigned)gx, kThreads * TPC, smem, st>>>(
+      acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, d.n, d.E, d.W, d.ktc, d.Epad, d.mods, d.minv, d.inv, d.md,
+      d.ct, out, out2, pred, device_error_word());
+  return launch_status();
 }
 
 template <int MODE>
@@ -229,28 +263,13 @@ int launch_crt(const sdpv_ctx* c, const int16_t* acc, i64 ldg, i64 N, i64 j0, i6
                const int32_t* pred = nullptr) {
   const CtxDev& d = c->d;
   if (d.n > kNmax || d.E > kEmax) return SDPV_EINVAL;
-  size_t smem = 1024 + 8192 + (size_t)(2 * d.ktc + (d.Epad / 128) * d.ktc) * kSlice;
-  if (smem > 227 * 1024) return SDPV_EINVAL;
-  static bool attr_set[64] = {};
-  static size_t attr_val[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_set[dev & 63] || attr_val[dev & 63] < smem) {
-    cudaError_t e = cudaFuncSetAttribute(crt_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    attr_set[dev & 63] = true;
-    attr_val[dev & 63] = smem;
-  }
-  i64 B = rows * w;
-  i64 ntiles = (B + 127) / 128;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  i64 gx = (i64)sdpv::tune(SDPV_TUNE_CRT_CTAS) * sms;
-  if (gx > ntiles) gx = ntiles;
-  crt_kernel<MODE><<<(unsigned)gx, kThreads, smem, st>>>(acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, d.n, d.E,
-                                                          d.W, d.ktc, d.Epad, d.mods, d.minv, d.inv, d.md, d.ct, out,
-                                                          out2, pred, device_error_word());
-  return launch_status();
+  const size_t tables = (size_t)(d.Epad / 128) * d.ktc * kSlice, tile = (size_t)2 * d.ktc * kSlice;
+  const size_t smem1 = 1024 + 8192 + tile + tables, smem2 = 1024 + 8192 + 2 * tile + tables;
+  // two tiles per CTA when two such CTAs fit an SM (shared memory) and there are tiles for them
+  if (smem2 <= 112 * 1024 && rows * w > 128 * 148)
+    return launch_crt_t<MODE, 2>(c, acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, out, out2, st, pred, smem2);
+  if (smem1 > 227 * 1024) return SDPV_EINVAL;
+  return launch_crt_t<MODE, 1>(c, acc, ldg, N, j0, w, rows, rpb, rowexp, colexp, L, out, out2, st, pred, smem1);
 }
 
 }  // namespace
