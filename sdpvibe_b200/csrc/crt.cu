@@ -4,7 +4,7 @@
 //   y_i = a_i (M/m_i)^-1 mod m_i  (centred),  k = round(sum y_i / m_i),
 //   value = sum_i y_i (M/m_i) - k M = sum_t (Z_t - k Md_t) 256^t,  Z_t = sum_i Ct[t][i] y_i
 // with Ct[t][i] the signed base-256 digits of M/m_i (sdpvibe/rns.py:140-159, 227-245;
-// sdpvibe/limbops.py:85-152).  One CTA handles 128 entries:
+// sdpvibe/limbops.py:85-152).  A CTA handles one or two tiles of 128 entries; each tile goes through:
 //   * pre-pass (one thread per entry): y_i from the int16 accumulator, split y = 128 yh + yl into
 //     two K-major int8 tiles in shared memory, and k;
 //   * digit contraction on the tensor cores, 64 digits at a time: Zh = Yh Ct^T, Zl = Yl Ct^T
