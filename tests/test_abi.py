@@ -42,7 +42,7 @@ def test_tuning_knobs_validated():
     h = _lib.lib()
     v = ctypes.c_int(0)
     for knob, good, bad in ((0, (1, 4), (0, 5)), (1, (0, 32, 64), (8, 80)), (2, (0, 64), (-16, 128)),
-                            (3, (8, 16), (0, 12, 24))):
+                            (3, (8, 16), (0, 12, 24)), (4, (1, 2, 4, 8, 16), (0, 3, 12, 32))):
         assert h.sdpv_tune_get(knob, ctypes.byref(v)) == 0
         old = v.value
         for g in good:
@@ -51,3 +51,14 @@ def test_tuning_knobs_validated():
             assert h.sdpv_tune_set(knob, b) == _lib.EINVAL
         assert h.sdpv_tune_set(knob, old) == 0
     assert h.sdpv_tune_set(3, 1) == _lib.EINVAL
+
+
+def test_context_moduli_group_validated():
+    """sdpv_ctx_create_g refuses moduli groups other than 1, 2, 4, 8, 16 before touching the device"""
+    import ctypes
+    from sdpvibe_b200 import _lib
+    h = _lib.lib()
+    out = ctypes.c_void_p()
+    for G in (0, 3, 6, 32, -1):
+        assert h.sdpv_ctx_create_g(26, G, ctypes.byref(out)) == _lib.EINVAL
+    assert h.sdpv_ctx_create_g(0, 16, ctypes.byref(out)) == _lib.EINVAL
