@@ -75,3 +75,38 @@ def test_unsigned_table_reproduces_the_residue(L):
         sgn = (m - pow(2, 32 * L, m)) % m
         v = [sum(int(b) * t for b, t in zip(row, tab)) + (sgn if ng else 0) for row, ng in zip(by, neg)]
         assert [x % m for x in v] == [int(x) % m for x in ref[g]]
+
+
+def _magic_quotient(v, minv_f32):
+    """the residue GEMM's rounded quotient: __float_as_int(fmaf((float)v, minv, 12582912.0f)) - 0x4B400000,
+    i.e. (float)v (round to nearest even) times the float 1/m, plus 1.5 2^23 with one rounding to a float
+    whose unit is 1 -- computed here exactly with fractions and rounded half to even"""
+    from fractions import Fraction
+    fv = Fraction(float(np.float32(v)))
+    s = fv * Fraction(float(minv_f32))                       # the fma's exact product; the magic adds 1.5 2^23
+    q = s.numerator // s.denominator                         # floor, then round half to even
+    rem = s - q
+    if rem > Fraction(1, 2) or (rem == Fraction(1, 2) and q % 2):
+        q += 1
+    return q
+
+
+@pytest.mark.parametrize("L", [26, 27])
+def test_float_rounded_quotient_needs_one_correction(L):
+    """The narrow residue-GEMM epilogue reduces v (|v| < 2^31) by q = round(v / m) taken from the float
+    estimate above and applies a single correction (add m when negative).  That is exact when v - q m lies in
+    (-m, m/2 + m/64]: checked for every modulus of the context on random v over the whole range, on the
+    multiples of m and their half-way neighbours, and at the range's ends"""
+    rng = np.random.default_rng(L)
+    for m in O.tables(L).m32.astype(np.int64)[::3]:
+        minv = np.float32(1.0 / float(m))
+        k = rng.integers(-((1 << 31) // m), (1 << 31) // m, size=40)
+        v = np.concatenate([rng.integers(-(1 << 31) + 1, 1 << 31, size=120), k * m, k * m + m // 2,
+                            k * m + (m + 1) // 2, k * m - m // 2,
+                            np.array([0, 1, -1, m // 2, -(m // 2), (1 << 31) - 1, -(1 << 31) + 1])])
+        v = v[(v > -(1 << 31)) & (v < (1 << 31))]
+        for x in v.tolist():
+            r = x - _magic_quotient(x, minv) * int(m)
+            assert -int(m) < r <= int(m) // 2 + int(m) // 64
+            r += int(m) if r < 0 else 0
+            assert r == x % int(m)
